@@ -1,0 +1,95 @@
+"""ctypes binding of the C ABI in ``include/ccc_b200.h`` (``libccc_b200.so``).
+
+There is no fallback: if the library is missing or fails to load, every operation raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libccc_b200.so")
+
+# return codes / status bits (mirrors include/ccc_b200.h)
+CCC_OK = 0
+CCC_ST_CAND_OVERFLOW = 1
+CCC_ST_OUT_OVERFLOW = 2
+CCC_ST_STACK_OVERFLOW = 4
+CCC_ST_MALFORMED_TREE = 8
+
+OP_BVH, OP_FIND_COLLISIONS, OP_CONTINUOUS, OP_PROXIMITY, OP_IMPULSES, OP_MINCOL = range(6)
+
+# every symbol the header declares, with (restype, argtypes)
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+SIGNATURES = {
+    "ccc_version": (_I, []),
+    "ccc_error_string": (ctypes.c_char_p, [_I]),
+    "ccc_kernel_launches": (_I64, []),
+    "ccc_timing_begin": (_I, []),
+    "ccc_timing_end": (_I, [_I, _P, _I, _P, _P]),
+    "ccc_workspace_size": (_I64, [_I, _I64, _I64, _I64]),
+    "ccc_read_status": (_I, [_P, _I64, _P, _P]),
+    "ccc_bvh": (_I, [_I, _P, _P, _I64, _I64, _P, _P, _P, _I64, _P]),
+    "ccc_find_collisions": (_I, [_I, _P, _P, _P, _I64, _I64, _D, _I64, _P, _P, _I64, _P]),
+    "ccc_find_collisions_continuous": (_I, [_I, _P, _P, _P, _P, _P, _I64, _I64, _I64, _I64, _P, _P, _P, _I64, _P]),
+    "ccc_find_mincol_cand": (_I, [_I, _P, _P, _P, _P, _I64, _I64, _I64, _P, _P, _I64, _P]),
+    "ccc_find_proximity": (_I, [_I, _P, _P, _P, _I64, _I64, _D, _I64, _P, _P, _I64, _P]),
+    "ccc_compute_impulses": (_I, [_I, _P, _P, _P, _P, _P, _P, _I64, _I64, _I64, _I64, _P, _P, _P, _P, _I64, _P]),
+    "ccc_compute_impulses_from_collisions": (_I, [_I, _P, _P, _I64, _I64, _P, _P, _P, _I64, _P, _P, _P, _P, _I64,
+                                                 _P]),
+}
+
+_lib = None
+
+
+class NativeLibraryError(RuntimeError):
+    pass
+
+
+def lib():
+    """Load libccc_b200.so (raises NativeLibraryError when it is absent)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise NativeLibraryError(
+                f"{LIB_PATH} is not built; run `python -m cccollisions_b200.build` (nvcc, sm_100a)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int, what: str):
+    if rc != CCC_OK:
+        msg = lib().ccc_error_string(rc).decode()
+        raise RuntimeError(f"{what} failed: {msg} (code {rc})")
+
+
+def kernel_launches() -> int:
+    return int(lib().ccc_kernel_launches())
+
+
+def timing_begin():
+    lib().ccc_timing_begin()
+
+
+def timing_end(max_kernels: int = 64):
+    """{kernel name: (total ms, launches)} for the launches since timing_begin()."""
+    name_len = 64
+    names = ctypes.create_string_buffer(max_kernels * name_len)
+    ms = (ctypes.c_float * max_kernels)()
+    cnt = (ctypes.c_int32 * max_kernels)()
+    n = lib().ccc_timing_end(max_kernels, names, name_len, ms, cnt)
+    if n < 0:
+        raise RuntimeError("kernel timing failed")
+    out = {}
+    for i in range(n):
+        nm = names.raw[i * name_len:(i + 1) * name_len].split(b"\0", 1)[0].decode()
+        out[nm] = (float(ms[i]), int(cnt[i]))
+    return out

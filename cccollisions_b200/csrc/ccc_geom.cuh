@@ -1,0 +1,548 @@
+// ccc_geom.cuh — device geometry for the collision pipeline.
+//
+// Every expression keeps the reference's evaluation order (Dolorousrtur/CCCollisions
+// src/figures.cu, src/aabb.cu, src/collisions_continuous.cu, src/collisions_impulses.cu,
+// src/proximity_static.cu).  The library is compiled with -fmad=false so no multiply-add
+// is contracted: results are the plain IEEE-754 float/double results of those expressions.
+#pragma once
+
+#include <stdint.h>
+#include <float.h>
+#include "ccc_libm.h"
+#include "ccc_ddmul.h"
+
+namespace ccc {
+
+template <class T> struct V3 { T x, y, z; };
+template <class T> __device__ __forceinline__ V3<T> mk(T x, T y, T z) { V3<T> r; r.x = x; r.y = y; r.z = z; return r; }
+template <class T> __device__ __forceinline__ V3<T> operator+(V3<T> a, V3<T> b) { return mk<T>(a.x + b.x, a.y + b.y, a.z + b.z); }
+template <class T> __device__ __forceinline__ V3<T> operator-(V3<T> a, V3<T> b) { return mk<T>(a.x - b.x, a.y - b.y, a.z - b.z); }
+template <class T> __device__ __forceinline__ V3<T> operator*(V3<T> a, T s) { return mk<T>(a.x * s, a.y * s, a.z * s); }
+template <class T> __device__ __forceinline__ T dot(V3<T> a, V3<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class T> __device__ __forceinline__ V3<T> cross(V3<T> a, V3<T> b) {
+    return mk<T>(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+template <class T> __device__ __forceinline__ T norm2(V3<T> a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
+__device__ __forceinline__ float fmn(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ float fmx(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double fmn(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ double fmx(double a, double b) { return fmax(a, b); }
+
+template <class T> struct Box { V3<T> lo, hi; };
+template <class T> __device__ __forceinline__ Box<T> merge(const Box<T>& a, const Box<T>& b) {
+    Box<T> r;
+    r.lo = mk<T>(fmn(a.lo.x, b.lo.x), fmn(a.lo.y, b.lo.y), fmn(a.lo.z, b.lo.z));
+    r.hi = mk<T>(fmx(a.hi.x, b.hi.x), fmx(a.hi.y, b.hi.y), fmx(a.hi.z, b.hi.z));
+    return r;
+}
+// checkOverlap (aabb.cu:190-200)
+template <class T> __device__ __forceinline__ bool overlap(const Box<T>& a, const Box<T>& b, T th) {
+    return (a.lo.x <= (b.hi.x + th)) && (a.hi.x >= (b.lo.x - th)) &&
+           (a.lo.y <= (b.hi.y + th)) && (a.hi.y >= (b.lo.y - th)) &&
+           (a.lo.z <= (b.hi.z + th)) && (a.hi.z >= (b.lo.z - th));
+}
+template <class T> __device__ __forceinline__ Box<T> load_box(const T* p) {
+    Box<T> b;
+    b.lo = mk<T>(p[0], p[1], p[2]);
+    b.hi = mk<T>(p[3], p[4], p[5]);
+    return b;
+}
+template <class T> __device__ __forceinline__ void store_box(T* p, const Box<T>& b) {
+    p[0] = b.lo.x; p[1] = b.lo.y; p[2] = b.lo.z; p[3] = b.hi.x; p[4] = b.hi.y; p[5] = b.hi.z;
+}
+
+template <class T> struct Tri { V3<T> v[3]; };
+template <class T> __device__ __forceinline__ Tri<T> load_tri(const T* __restrict__ p, int64_t i) {
+    Tri<T> t;
+    const T* q = p + i * 9;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) t.v[c] = mk<T>(__ldg(q + 3 * c), __ldg(q + 3 * c + 1), __ldg(q + 3 * c + 2));
+    return t;
+}
+// Triangle::ComputeBBox (figures.cu:37-41)
+template <class T> __device__ __forceinline__ Box<T> tri_box(const Tri<T>& t) {
+    Box<T> b;
+    b.lo = mk<T>(fmn(t.v[0].x, fmn(t.v[1].x, t.v[2].x)), fmn(t.v[0].y, fmn(t.v[1].y, t.v[2].y)),
+                 fmn(t.v[0].z, fmn(t.v[1].z, t.v[2].z)));
+    b.hi = mk<T>(fmx(t.v[0].x, fmx(t.v[1].x, t.v[2].x)), fmx(t.v[0].y, fmx(t.v[1].y, t.v[2].y)),
+                 fmx(t.v[0].z, fmx(t.v[1].z, t.v[2].z)));
+    return b;
+}
+
+template <class T> __device__ __forceinline__ bool veq(V3<T> a, V3<T> b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
+// shareVertex (figures.cu:527-544, 578-596): equality of coordinates
+template <class T> __device__ __forceinline__ bool share_vertex(const V3<T>* a, const V3<T>* b) {
+    bool s = false;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) s = s || veq(a[i], b[j]);
+    return s;
+}
+// countSharedVerts (figures.cu:548-576)
+template <class T> __device__ __forceinline__ int count_shared(const Tri<T>& a, const Tri<T>& b) {
+    int c = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        if (veq(a.v[i], b.v[0]) || veq(a.v[i], b.v[1]) || veq(a.v[i], b.v[2])) ++c;
+    return c;
+}
+
+// isect_interval + TriangleTriangleOverlap (figures.cu:378-427)
+template <class T> __device__ __forceinline__ bool axis_overlap(const Tri<T>& a, const Tri<T>& b, V3<T> ax, T th) {
+    T d = dot(ax, a.v[0]);
+    T alo = d, ahi = d;
+    d = dot(ax, a.v[1]); alo = fmn(alo, d); ahi = fmx(ahi, d);
+    d = dot(ax, a.v[2]); alo = fmn(alo, d); ahi = fmx(ahi, d);
+    d = dot(ax, b.v[0]);
+    T blo = d, bhi = d;
+    d = dot(ax, b.v[1]); blo = fmn(blo, d); bhi = fmx(bhi, d);
+    d = dot(ax, b.v[2]); blo = fmn(blo, d); bhi = fmx(bhi, d);
+    return (alo <= bhi + th) && (ahi >= blo - th);
+}
+// TriangleTriangleIsectSepAxis (figures.cu:446-509); the reference ANDs all 17 axes
+// without early exit, which is the same predicate as stopping at the first failure
+template <class T> __device__ __forceinline__ bool sat(const Tri<T>& a, const Tri<T>& b, T th) {
+    V3<T> a0 = a.v[1] - a.v[0], a1 = a.v[2] - a.v[0], a2 = a.v[2] - a.v[1];
+    V3<T> an = cross(a1, a2);
+    V3<T> b0 = b.v[1] - b.v[0], b1 = b.v[2] - b.v[0], b2 = b.v[2] - b.v[1];
+    V3<T> bn = cross(b1, b2);
+    if (!axis_overlap(a, b, an, th)) return false;
+    if (!axis_overlap(a, b, bn, th)) return false;
+    if (!axis_overlap(a, b, cross(a0, b0), th)) return false;
+    if (!axis_overlap(a, b, cross(a0, b1), th)) return false;
+    if (!axis_overlap(a, b, cross(a0, b2), th)) return false;
+    if (!axis_overlap(a, b, cross(a1, b0), th)) return false;
+    if (!axis_overlap(a, b, cross(a1, b1), th)) return false;
+    if (!axis_overlap(a, b, cross(a1, b2), th)) return false;
+    if (!axis_overlap(a, b, cross(a2, b0), th)) return false;
+    if (!axis_overlap(a, b, cross(a2, b1), th)) return false;
+    if (!axis_overlap(a, b, cross(a2, b2), th)) return false;
+    if (!axis_overlap(a, b, cross(an, a0), th)) return false;
+    if (!axis_overlap(a, b, cross(an, a1), th)) return false;
+    if (!axis_overlap(a, b, cross(an, a2), th)) return false;
+    if (!axis_overlap(a, b, cross(an, b0), th)) return false;
+    if (!axis_overlap(a, b, cross(an, b1), th)) return false;
+    if (!axis_overlap(a, b, cross(an, b2), th)) return false;
+    return true;
+}
+
+// ------------------------------------------------------------------ continuous collision
+
+// MovingTriangle (figures.cu:295-366): positions at t = 0 and displacement x1 - x0
+template <class T> struct MTri { V3<T> v[3], dv[3]; };
+template <class T> __device__ __forceinline__ MTri<T> load_mtri(const T* __restrict__ x0, const T* __restrict__ x1, int64_t i) {
+    Tri<T> a = load_tri(x0, i), b = load_tri(x1, i);
+    MTri<T> m;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) { m.v[c] = a.v[c]; m.dv[c] = b.v[c] - a.v[c]; }
+    return m;
+}
+// MovingTriangle::ComputeBBoxVertex (346-351): box of v and v + dv
+template <class T> __device__ __forceinline__ Box<T> mvbox(const MTri<T>& t, int i) {
+    V3<T> a = t.v[i], b = t.v[i] + t.dv[i];
+    Box<T> r;
+    r.lo = mk<T>(fmn(a.x, b.x), fmn(a.y, b.y), fmn(a.z, b.z));
+    r.hi = mk<T>(fmx(a.x, b.x), fmx(a.y, b.y), fmx(a.z, b.z));
+    return r;
+}
+template <class T> __device__ __forceinline__ Box<T> svbox(const Tri<T>& t, int i) {
+    Box<T> r;
+    r.lo = t.v[i];
+    r.hi = t.v[i];
+    return r;
+}
+
+// Point table of the 15 sub-tests (collisions_continuous.cu:36-124): bits per point p:
+// side (first/second triangle of the pair) and corner.  Types 0..8 edge-edge with edges
+// {01, 02, 12}[k/3] and [k%3]; 9..11 face of the first vs vertex k-9 of the second;
+// 12..14 vertex k-12 of the first vs face of the second.
+__device__ __forceinline__ void type_points(int k, int side[4], int corner[4]) {
+    if (k < 9) {
+        int e0 = k / 3, e1 = k - 3 * (k / 3);
+        side[0] = 0; corner[0] = e0 == 2 ? 1 : 0;
+        side[1] = 0; corner[1] = e0 == 0 ? 1 : 2;
+        side[2] = 1; corner[2] = e1 == 2 ? 1 : 0;
+        side[3] = 1; corner[3] = e1 == 0 ? 1 : 2;
+    } else if (k < 12) {
+        side[0] = 0; corner[0] = 0;
+        side[1] = 0; corner[1] = 1;
+        side[2] = 0; corner[2] = 2;
+        side[3] = 1; corner[3] = k - 9;
+    } else {
+        side[0] = 0; corner[0] = k - 12;
+        side[1] = 1; corner[1] = 0;
+        side[2] = 1; corner[2] = 1;
+        side[3] = 1; corner[3] = 2;
+    }
+}
+
+// check_minimal_bbox_overlap (collisions_continuous.cu:234-318): swept sub-boxes, no threshold
+template <class T> __device__ __forceinline__ bool ccd_subbox(const MTri<T>& a, const MTri<T>& b, int k) {
+    int side[4], corner[4];
+    type_points(k, side, corner);
+    Box<T> b0, b1;
+    if (k < 9) {
+        b0 = merge(mvbox(a, corner[0]), mvbox(a, corner[1]));
+        b1 = merge(mvbox(b, corner[2]), mvbox(b, corner[3]));
+    } else if (k < 12) {
+        b0 = merge(merge(mvbox(a, 0), mvbox(a, 1)), mvbox(a, 2));
+        b1 = mvbox(b, k - 9);
+    } else {
+        b0 = mvbox(a, k - 12);
+        b1 = merge(merge(mvbox(b, 0), mvbox(b, 1)), mvbox(b, 2));
+    }
+    return overlap(b0, b1, (T)0);
+}
+
+// all 15 swept sub-box tests as a bit mask; the three per-vertex swept boxes of each
+// triangle are computed once
+template <class T> __device__ __forceinline__ uint32_t ccd_subbox_mask(const MTri<T>& a, const MTri<T>& b) {
+    Box<T> va[3], vb[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) { va[i] = mvbox(a, i); vb[i] = mvbox(b, i); }
+    Box<T> ea[3], eb[3];
+    ea[0] = merge(va[0], va[1]); ea[1] = merge(va[0], va[2]); ea[2] = merge(va[1], va[2]);
+    eb[0] = merge(vb[0], vb[1]); eb[1] = merge(vb[0], vb[2]); eb[2] = merge(vb[1], vb[2]);
+    Box<T> fa = merge(merge(va[0], va[1]), va[2]);
+    Box<T> fb = merge(merge(vb[0], vb[1]), vb[2]);
+    uint32_t m = 0;
+#pragma unroll
+    for (int e0 = 0; e0 < 3; ++e0)
+#pragma unroll
+        for (int e1 = 0; e1 < 3; ++e1)
+            if (overlap(ea[e0], eb[e1], (T)0)) m |= 1u << (3 * e0 + e1);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        if (overlap(fa, vb[i], (T)0)) m |= 1u << (9 + i);
+        if (overlap(va[i], fb, (T)0)) m |= 1u << (12 + i);
+    }
+    return m;
+}
+
+template <class T> struct MTet { V3<T> v[4], dv[4]; };
+template <class T> __device__ __forceinline__ MTet<T> make_tet(const MTri<T>& a, const MTri<T>& b, int k) {
+    int side[4], corner[4];
+    type_points(k, side, corner);
+    MTet<T> t;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const MTri<T>& s = side[i] ? b : a;
+        t.v[i] = s.v[corner[i]];
+        t.dv[i] = s.dv[corner[i]];
+    }
+    return t;
+}
+
+// MovingTetraMatrix::coef3..coef0 (figures.cu:122-293): exact term order, summed from 0
+template <class T> __device__ __forceinline__ void cubic_coeffs(const MTet<T>& t, T c[4]) {
+    V3<T> v0 = t.v[0] - t.v[3], v1 = t.v[1] - t.v[3], v2 = t.v[2] - t.v[3];
+    V3<T> dv0 = t.dv[0] - t.dv[3], dv1 = t.dv[1] - t.dv[3], dv2 = t.dv[2] - t.dv[3];
+    T k3 = 0;
+    k3 += dv2.z * dv1.y * dv0.x;
+    k3 += -dv1.z * dv2.y * dv0.x;
+    k3 += -dv2.z * dv0.y * dv1.x;
+    k3 += dv0.z * dv2.y * dv1.x;
+    k3 += dv1.z * dv0.y * dv2.x;
+    k3 += -dv0.z * dv1.y * dv2.x;
+    T k2 = 0;
+    k2 += v2.z * dv1.y * dv0.x;
+    k2 += dv2.z * v1.y * dv0.x;
+    k2 += dv2.z * dv1.y * v0.x;
+    k2 += -v1.z * dv2.y * dv0.x;
+    k2 += -dv1.z * v2.y * dv0.x;
+    k2 += -dv1.z * dv2.y * v0.x;
+    k2 += -v2.z * dv0.y * dv1.x;
+    k2 += -dv2.z * v0.y * dv1.x;
+    k2 += -dv2.z * dv0.y * v1.x;
+    k2 += v0.z * dv2.y * dv1.x;
+    k2 += dv0.z * v2.y * dv1.x;
+    k2 += dv0.z * dv2.y * v1.x;
+    k2 += v1.z * dv0.y * dv2.x;
+    k2 += dv1.z * v0.y * dv2.x;
+    k2 += dv1.z * dv0.y * v2.x;
+    k2 += -v0.z * dv1.y * dv2.x;
+    k2 += -dv0.z * v1.y * dv2.x;
+    k2 += -dv0.z * dv1.y * v2.x;
+    T k1 = 0;
+    k1 += v2.z * v1.y * dv0.x;
+    k1 += v2.z * dv1.y * v0.x;
+    k1 += dv2.z * v1.y * v0.x;
+    k1 += -v1.z * v2.y * dv0.x;
+    k1 += -v1.z * dv2.y * v0.x;
+    k1 += -dv1.z * v2.y * v0.x;
+    k1 += -v2.z * v0.y * dv1.x;
+    k1 += -v2.z * dv0.y * v1.x;
+    k1 += -dv2.z * v0.y * v1.x;
+    k1 += v0.z * v2.y * dv1.x;
+    k1 += v0.z * dv2.y * v1.x;
+    k1 += dv0.z * v2.y * v1.x;
+    k1 += v1.z * v0.y * dv2.x;
+    k1 += v1.z * dv0.y * v2.x;
+    k1 += dv1.z * v0.y * v2.x;
+    k1 += -v0.z * v1.y * dv2.x;
+    k1 += -v0.z * dv1.y * v2.x;
+    k1 += -dv0.z * v1.y * v2.x;
+    T k0 = 0;
+    k0 += v2.z * v1.y * v0.x;
+    k0 += -v1.z * v2.y * v0.x;
+    k0 += -v2.z * v0.y * v1.x;
+    k0 += v0.z * v2.y * v1.x;
+    k0 += v1.z * v0.y * v2.x;
+    k0 += -v0.z * v1.y * v2.x;
+    c[0] = k3; c[1] = k2; c[2] = k1; c[3] = k0;
+}
+
+#define CCC_EPS 1e-16   // EPSILON (flags.h:36-38)
+
+// add_root (collisions_continuous.cu:448-464): the root arrives converted to T
+template <class T> __device__ __forceinline__ void add_root(T r[3], T x, int& nr) {
+    if (x < -CCC_EPS || x > 1 + CCC_EPS) return;
+    if (nr < 3) r[nr] = x;
+    nr++;
+}
+
+// solveCubic with computeG / computeH (collisions_continuous.cu:472-613); roots start at -1.
+template <class T> __device__ __noinline__ void solve_cubic(double a, double b, double c, double d, T r[3]) {
+    r[0] = r[1] = r[2] = (T)-1;
+    int nr = 0;
+    if (a == 0 && b == 0) {
+        return;     // linear case: the reference never stores its root
+    } else if (fabs(a) < CCC_EPS) {
+        double D = c * c - 4.0 * b * d;
+        if (D >= 0) {
+            D = ccc_sqrt(D);
+            double x1 = (-c + D) / (2.0 * b);
+            double x2 = (-c - D) / (2.0 * b);
+            add_root<T>(r, (T)x1, nr);
+            add_root<T>(r, (T)x2, nr);
+        }
+    } else {
+        double f = ((3.0 * c / a) - ((b * b) / (a * a))) / 3.0;
+        double b3 = 2 * ccc_cube_hi(b);
+        double a2dd[2];
+        ccc_sq_dd(a, a2dd);
+        double a2 = a2dd[0];
+        double a3c[2];
+        ccc_certmul_r2(a2dd, 2, a, a3c);
+        double a3 = a3c[0];
+        double p1 = b3 / a3;
+        double p2 = (b * c * 9) / a2;
+        double p3 = 27.0 * d / a;
+        double g = (p1 - p2 + p3) / 27.0;
+        double f3 = ccc_cube_hi(f);
+        double h = g * g / 4.0 + f3 / 27.0;
+        if (f == 0 && g == 0 && h == 0) {
+            float k = (float)(d / a);
+            double x1;
+            if (k >= 0) x1 = (double)(ccc_cbrtf(k) * -1);
+            else x1 = (double)ccc_cbrtf(-k);
+            add_root<T>(r, (T)x1, nr);
+        } else if (h <= 0) {
+            double i = ccc_sqrt(((g * g) / 4.0) - h);
+            double j = ccc_cbrt(i);
+            double k = ccc_acos(-(g / (2 * i)));
+            double L = j * -1;
+            double M = ccc_cos(k / 3.0);
+            double N = ccc_sqrt(3.0) * ccc_sin(k / 3.0);
+            double P = (b / (3.0 * a)) * -1;
+            double x1 = 2 * j * ccc_cos(k / 3.0) - (b / (3.0 * a));
+            double x2 = L * (M + N) + P;
+            double x3 = L * (M - N) + P;
+            add_root<T>(r, (T)x1, nr);
+            add_root<T>(r, (T)x2, nr);
+            add_root<T>(r, (T)x3, nr);
+        } else {
+            double R = -(g / 2.0) + ccc_sqrt(h);
+            double S, U;
+            if (R >= 0) S = ccc_cbrt(R);
+            else S = -ccc_cbrt(-R);
+            double V = -(g / 2.0) - ccc_sqrt(h);
+            if (V >= 0) U = ccc_cbrt(V);
+            else U = -ccc_cbrt(-V);
+            double x1 = (S + U) - (b / (3.0 * a));
+            add_root<T>(r, (T)x1, nr);
+        }
+    }
+}
+
+// is_inside (collisions_continuous.cu:615-637)
+template <class T> __device__ __forceinline__ bool is_inside(V3<T> v0, V3<T> v1, V3<T> v2, V3<T> vt) {
+    V3<T> e1 = v0 - v1, e2 = v2 - v1, ep = vt - v1;
+    T d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2), d20 = dot(ep, e1), d21 = dot(ep, e2);
+    T denom = d00 * d11 - d01 * d01;
+    T v = (d11 * d20 - d01 * d21) / denom;
+    T w = (d00 * d21 - d01 * d20) / denom;
+    T u = 1 - v - w;
+    if (v < 0 || v > 1) return false;
+    if (w < 0 || w > 1) return false;
+    if (u < 0 || u > 1) return false;
+    return true;
+}
+
+template <class T> __device__ __forceinline__ V3<T> at_time(const MTet<T>& t, int i, T root) { return t.v[i] + t.dv[i] * root; }
+
+// filterCollisions (collisions_continuous.cu:640-684)
+template <class T> __device__ __forceinline__ bool ccd_filter(const MTet<T>& tet, int k, T root) {
+    if (root < -(T)CCC_EPS) return false;
+    V3<T> p0 = at_time(tet, 0, root), p1 = at_time(tet, 1, root), p2 = at_time(tet, 2, root), p3 = at_time(tet, 3, root);
+    if (k < 9) {
+        V3<T> da = p1 - p0, db = p3 - p2, dc = p2 - p0;
+        T s = dot(cross(dc, db), cross(da, db)) / norm2(cross(da, db));
+        T p = dot(cross(dc, da), cross(da, db)) / norm2(cross(da, db));
+        if (s < 0 || s > 1 || p < 0 || p > 1) return false;
+        return true;
+    } else if (k < 12) {
+        return is_inside(p0, p1, p2, p3);
+    }
+    return is_inside(p1, p2, p3, p0);
+}
+
+// ------------------------------------------------------------------ impulses
+
+#define CCC_THICKNESS 2e-3   // collisions_impulses.cu:12-14
+
+template <class T> __device__ __forceinline__ V3<T> vnormalize(V3<T> a) {
+    T n = a.x * a.x + a.y * a.y + a.z * a.z;
+    T inv = (T)1 / (T)ccc_sqrt((double)n);
+    return a * inv;
+}
+
+template <class T> struct Contact { V3<T> n; T vn, m0, m1; };
+
+// compute_coeficients_and_directions and helpers (collisions_impulses.cu:162-543)
+template <class T> __device__ __forceinline__ Contact<T> contact(const MTet<T>& tet, int k, T root, const T q[4]) {
+    Contact<T> ct;
+    V3<T> th[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) th[i] = at_time(tet, i, root);
+    if (k < 9) {
+        V3<T> da = th[1] - th[0], db = th[3] - th[2], dc = th[2] - th[0];
+        T denom = norm2(cross(da, db));
+        T s, t;
+        if (fabs((double)denom) < 1e-15) { s = (T)0.5; t = (T)0.5; }
+        else {
+            s = dot(cross(dc, db), cross(da, db)) / norm2(cross(da, db));
+            t = dot(cross(dc, da), cross(da, db)) / norm2(cross(da, db));
+        }
+        const V3<T>* v = tet.v;
+        const V3<T>* dv = tet.dv;
+        V3<T> p0 = v[0] + (v[1] - v[0]) * s;
+        V3<T> p1 = v[2] + (v[3] - v[2]) * t;
+        V3<T> dp0 = dv[0] + (dv[1] - dv[0]) * s;
+        V3<T> dp1 = dv[2] + (dv[3] - dv[2]) * t;
+        V3<T> c0 = v[0] + dv[0] * root, c1 = v[1] + dv[1] * root, c2 = v[2] + dv[2] * root;
+        V3<T> nd = vnormalize(cross(c1 - c0, c2 - c0));
+        if (dot(p1 - p0, nd) < 0) nd = nd * (T)-1;
+        ct.n = nd;
+        ct.vn = dot(dp1 - dp0, nd);
+        ct.m0 = q[0] * (1 - s) + q[1] * s;
+        ct.m1 = q[2] * (1 - t) + q[3] * t;
+        return ct;
+    }
+    bool inv = k >= 12;
+    int f0 = inv ? 1 : 0, f1 = inv ? 2 : 1, f2 = inv ? 3 : 2, fv = inv ? 0 : 3;
+    V3<T> e1 = th[f0] - th[f1], e2 = th[f2] - th[f1], ep = th[fv] - th[f1];
+    T d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2), d20 = dot(ep, e1), d21 = dot(ep, e2);
+    T denom = d00 * d11 - d01 * d01;
+    T u, w, vv;
+    if (fabs((double)denom) < 1e-15) { u = (T)(1. / 3.); w = (T)(1. / 3.); }
+    else {
+        u = (d11 * d20 - d01 * d21) / denom;
+        w = (d00 * d21 - d01 * d20) / denom;
+    }
+    vv = 1 - u - w;
+    const V3<T>* v = tet.v;
+    const V3<T>* dv = tet.dv;
+    V3<T> pt = v[f0] * u + v[f1] * vv + v[f2] * w;
+    V3<T> dpt = dv[f0] * u + dv[f1] * vv + dv[f2] * w;
+    V3<T> c0 = v[f0] + dv[f0] * root, c1 = v[f1] + dv[f1] * root, c2 = v[f2] + dv[f2] * root;
+    V3<T> nd = vnormalize(cross(c1 - c0, c2 - c0));
+    if (dot(v[fv] - pt, nd) < 0) nd = nd * (T)-1;
+    ct.vn = dot(dv[fv] - dpt, nd);
+    if (inv) nd = nd * (T)-1;
+    ct.n = nd;
+    if (inv) {
+        ct.m0 = q[0];
+        ct.m1 = q[1] * u + q[2] * vv + q[3] * w;
+    } else {
+        ct.m0 = q[0] * u + q[1] * vv + q[2] * w;
+        ct.m1 = q[3];
+    }
+    return ct;
+}
+
+// ------------------------------------------------------------------ proximity
+
+template <class T> __device__ __forceinline__ bool prox_subbox(const Tri<T>& a, const Tri<T>& b, int k, T th) {
+    int side[4], corner[4];
+    type_points(k, side, corner);
+    Box<T> b0, b1;
+    if (k < 9) {
+        b0 = merge(svbox(a, corner[0]), svbox(a, corner[1]));
+        b1 = merge(svbox(b, corner[2]), svbox(b, corner[3]));
+    } else if (k < 12) {
+        b0 = tri_box(a);
+        b1 = svbox(b, k - 9);
+    } else {
+        b0 = svbox(a, k - 12);
+        b1 = tri_box(b);
+    }
+    return overlap(b0, b1, th);
+}
+
+// vec_sq_diff returns float (utils.cu:57-61); the distance is sqrt in float
+template <class T> __device__ __forceinline__ float sq_diff_f(V3<T> a, V3<T> b) { V3<T> d = a - b; return (float)dot(d, d); }
+
+template <class T> __device__ __forceinline__ void pt_seg(V3<T> p, V3<T> a, V3<T> b, T dc[3], bool set_s, T second) {
+    V3<T> ab = b - a, ap = p - a;
+    T t = dot(ap, ab) / dot(ab, ab);
+    if (t < (T)0.0) t = (T)0.0;
+    if (t > (T)1.0) t = (T)1.0;
+    V3<T> c = mk<T>(a.x + t * ab.x, a.y + t * ab.y, a.z + t * ab.z);
+    T nd = (T)__fsqrt_rn(sq_diff_f(p, c));
+    if (nd < dc[0]) {
+        dc[0] = nd;
+        if (set_s) { dc[1] = t; dc[2] = second; }
+        else { dc[2] = t; dc[1] = second; }
+    }
+}
+
+// compute_distance_edge_edge / compute_distance_triangle_node (proximity_static.cu:205-433)
+template <class T> __device__ __forceinline__ T prox_distance(const Tri<T>& a, const Tri<T>& b, int k) {
+    int side[4], corner[4];
+    type_points(k, side, corner);
+    V3<T> v[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) v[p] = (side[p] ? b : a).v[corner[p]];
+    if (k < 9) {
+        V3<T> da = v[1] - v[0], db = v[3] - v[2], dc = v[2] - v[0];
+        T s = dot(cross(dc, db), cross(da, db)) / norm2(cross(da, db));
+        T t = dot(cross(dc, da), cross(da, db)) / norm2(cross(da, db));
+        if (s != s || t != t) {
+            T d3[3] = {(T)FLT_MAX, (T)-1., (T)-1.};
+            pt_seg(v[0], v[2], v[3], d3, false, (T)0.);
+            pt_seg(v[1], v[2], v[3], d3, false, (T)1.);
+            pt_seg(v[2], v[0], v[1], d3, true, (T)0.);
+            pt_seg(v[3], v[0], v[1], d3, true, (T)1.);
+            s = d3[1];
+            t = d3[2];
+        }
+        bool sv = (s >= 0 && s <= 1), tv = (t >= 0 && t <= 1);
+        if (!sv || !tv) return (T)-1;
+        return (T)__fsqrt_rn(sq_diff_f(v[0] + da * s, v[2] + db * t));
+    }
+    int f0 = k < 12 ? 0 : 1, f1 = k < 12 ? 1 : 2, f2 = k < 12 ? 2 : 3, fv = k < 12 ? 3 : 0;
+    V3<T> e1 = v[f0] - v[f1], e2 = v[f2] - v[f1], ep = v[fv] - v[f1];
+    T d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2), d20 = dot(ep, e1), d21 = dot(ep, e2);
+    T denom = d00 * d11 - d01 * d01;
+    T u = (d11 * d20 - d01 * d21) / denom;
+    T w = (d00 * d21 - d01 * d20) / denom;
+    T vv = 1 - w - u;
+    bool ok = (vv >= 0 && vv <= 1) && (w >= 0 && w <= 1) && (u >= 0 && u <= 1);
+    if (!ok) return (T)-1;
+    V3<T> pt = v[f0] * u + v[f1] * vv + v[f2] * w;
+    return (T)__fsqrt_rn(sq_diff_f(v[fv], pt));
+}
+
+}  // namespace ccc

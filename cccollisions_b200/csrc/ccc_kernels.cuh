@@ -1,0 +1,566 @@
+// ccc_kernels.cuh — sm_100a kernels of the collision pipeline.
+//
+// Meshes are processed as a "forest": M meshes concatenated, mesh m owning triangles
+// [moff[m], moff[m+1]).  The exported tree tensors use the reference layout per mesh
+// (src/build_bvh.cu:309-378): rows 0..F-2 internal nodes, rows F-1..2F-2 leaves in sorted
+// position order, bboxes row = (min xyz, max xyz), tree row = (parent, left, right, tri id),
+// -1 for "none".  Mesh m's rows start at 2*moff[m] - m.
+//
+// Traversal works on a compact copy of the internal nodes (TNode, 64 B): both child boxes
+// rounded outward to fp32 plus child references, so one node visit is four 16-byte loads.
+#pragma once
+
+#include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
+#include "ccc_geom.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace ccc {
+
+enum StatusBits {
+    ST_CAND_OVERFLOW = 1,     // more candidate pairs than max_candidates_per_triangle * F
+    ST_OUT_OVERFLOW = 2,      // more result rows than the output tensor holds
+    ST_STACK_OVERFLOW = 4,    // traversal deeper than the 64-entry stack
+    ST_MALFORMED_TREE = 8,    // child / parent index out of range or a cycle in the tree
+};
+
+// Workspace header (int32 words) shared by all operations.
+struct WsHeader {
+    int status;
+    int cand_count;
+    int pad[14];
+};
+
+struct __align__(16) TNode {
+    float4 a;   // left  lo.x lo.y lo.z hi.x
+    float4 b;   // left  hi.y hi.z | right lo.x lo.y
+    float4 c;   // right lo.z hi.x hi.y hi.z
+    int4 d;     // left ref, right ref, left aux, right aux
+};
+// ref >= 0: internal node (mesh-local index); ref < 0: leaf at position ~ref.
+// aux: internal child -> rightmost leaf position of its subtree; leaf child -> triangle id.
+
+static constexpr int TRAV_THREADS = 128;
+static constexpr int STACK_DEPTH = 64;        // STACK_SIZE (flags.h:26-29)
+static constexpr int NARROW_THREADS = 128;
+
+// mesh containing element g where base(m) = off[m] - m * shift (shift 0: triangles,
+// shift 1: internal nodes); off has M + 1 entries
+__device__ __forceinline__ int find_mesh(const int* __restrict__ off, int M, long long g, int shift) {
+    int lo = 0, hi = M - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        long long b = (long long)__ldg(off + mid) - (long long)mid * shift;
+        if (b <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------------------------------
+// uniform mesh offsets for the reference API (B meshes of F triangles)
+__global__ void k_uniform_offsets(int* moff, int M, int F) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i <= M) moff[i] = i * F;
+}
+
+// ---------------------------------------------------------------------------------------
+// Build (reference order): leaf boxes, Karras topology, bottom-up box refit.
+// The reference's scene box is reduced from AABB() = (-MAX, +MAX) (aabb.cu:114-122,
+// build_bvh.cu:243-244), which makes every Morton code 0; with all keys equal the stable
+// sort keeps the input order, so leaf position p holds triangle p and the Karras prefix
+// delta(i, j) reduces to 32 + clz(i ^ j).
+
+// leaf rows: box of triangle p (swept over t0/t1 for motion), tree row (parent set later,
+// -1, -1, p)
+template <class T>
+__global__ void k_leaf_rows(const T* __restrict__ x0, const T* __restrict__ x1, const int* __restrict__ moff, int M,
+                            int total, T* __restrict__ bboxes, long long* __restrict__ tree) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    int m = find_mesh(moff, M, g, 0);
+    int F = moff[m + 1] - moff[m];
+    int p = g - moff[m];
+    long long row = 2LL * moff[m] - m + (F - 1) + p;
+    Box<T> b = tri_box(load_tri(x0, g));
+    if (x1) b = merge(b, tri_box(load_tri(x1, g)));      // MergeTriBoundingBoxes (452-460)
+    store_box(bboxes + row * 6, b);
+    tree[row * 4 + 1] = -1;
+    tree[row * 4 + 2] = -1;
+    tree[row * 4 + 3] = p;
+}
+
+// delta for all-equal keys and identity ids (LongestCommonPrefix, bvh.cu:65-89)
+__device__ __forceinline__ int delta_id(int i, int j, int n) {
+    if (j < 0 || j > n - 1) return -1;
+    return 32 + __clz(i ^ j);
+}
+
+// BuildRadixTree (build_bvh.cu:74-143) for identity order.  The split search is the
+// standard Karras one (steps ceil(l/2), ceil(l/4), ..., 1), which reaches the same split
+// as the reference's loop.
+__global__ void k_karras_identity(const int* __restrict__ moff, int M, int total_internal, long long* __restrict__ tree) {
+    int gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= total_internal) return;
+    int m = find_mesh(moff, M, gi, 1);
+    int n = moff[m + 1] - moff[m];
+    int i = gi - (moff[m] - m);
+    long long base = 2LL * moff[m] - m;
+    int dnext = delta_id(i, i + 1, n), dlast = delta_id(i, i - 1, n);
+    int d = (dnext - dlast >= 0) ? 1 : -1;
+    int dmin = delta_id(i, i - d, n);
+    int lmax = 2;
+    while (delta_id(i, i + lmax * d, n) > dmin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2)
+        if (delta_id(i, i + (l + t) * d, n) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = delta_id(i, j, n);
+    int s = 0;
+    for (int div = 2;; div *= 2) {
+        int t = (l + div - 1) / div;
+        if (delta_id(i, i + (s + t) * d, n) > dnode) s += t;
+        if (t <= 1) break;
+    }
+    int split = i + s * d + min(d, 0);
+    long long lc = (min(i, j) == split) ? (long long)(n - 1 + split) : (long long)split;
+    long long rc = (max(i, j) == split + 1) ? (long long)(n - 1 + split + 1) : (long long)(split + 1);
+    tree[(base + i) * 4 + 1] = lc;
+    tree[(base + i) * 4 + 2] = rc;
+    tree[(base + i) * 4 + 3] = -1;
+    tree[(base + lc) * 4 + 0] = i;
+    tree[(base + rc) * 4 + 0] = i;
+    if (i == 0) tree[base * 4 + 0] = -1;
+}
+
+// CreateHierarchy (build_bvh.cu:145-209): each leaf climbs; the second thread to reach a
+// node writes the union of its children's boxes and continues.
+template <class T>
+__global__ void k_refit(const int* __restrict__ moff, int M, int total, T* bboxes, const long long* __restrict__ tree,
+                        int* __restrict__ visits, int* status) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    int m = find_mesh(moff, M, g, 0);
+    int n = moff[m + 1] - moff[m];
+    if (n < 2) return;
+    int p = g - moff[m];
+    long long base = 2LL * moff[m] - m;
+    int* vis = visits + (moff[m] - m);
+    long long node = tree[(base + n - 1 + p) * 4 + 0];
+    for (int guard = 0; guard < n; ++guard) {
+        if (node < 0 || node >= n - 1) { atomicOr(status, ST_MALFORMED_TREE); return; }
+        __threadfence();
+        if (atomicAdd(vis + node, 1) == 0) return;
+        long long lc = tree[(base + node) * 4 + 1], rc = tree[(base + node) * 4 + 2];
+        const T* lb = bboxes + (base + lc) * 6;
+        const T* rb = bboxes + (base + rc) * 6;
+        Box<T> L, R;
+        L.lo = mk<T>(__ldcg(lb + 0), __ldcg(lb + 1), __ldcg(lb + 2));
+        L.hi = mk<T>(__ldcg(lb + 3), __ldcg(lb + 4), __ldcg(lb + 5));
+        R.lo = mk<T>(__ldcg(rb + 0), __ldcg(rb + 1), __ldcg(rb + 2));
+        R.hi = mk<T>(__ldcg(rb + 3), __ldcg(rb + 4), __ldcg(rb + 5));
+        store_box(bboxes + (base + node) * 6, merge(L, R));
+        if (node == 0) return;
+        node = tree[(base + node) * 4 + 0];
+    }
+    atomicOr(status, ST_MALFORMED_TREE);
+}
+
+// ---------------------------------------------------------------------------------------
+// Import of exported tensors into traversal nodes (build_bvh_from_array_tree 667-705 and
+// set_rightmost_nodes 707-743).
+
+template <class T> __device__ __forceinline__ void box_to_f32(const T* p, float lo[3], float hi[3]) {
+    if (sizeof(T) == 4) {
+        for (int c = 0; c < 3; ++c) { lo[c] = (float)p[c]; hi[c] = (float)p[3 + c]; }
+    } else {
+        for (int c = 0; c < 3; ++c) {
+            lo[c] = __double2float_rd((double)p[c]);
+            hi[c] = __double2float_ru((double)p[3 + c]);
+        }
+    }
+}
+
+template <class T>
+__global__ void k_import_nodes(const int* __restrict__ moff, int M, int total_internal, const T* __restrict__ bboxes,
+                               const long long* __restrict__ tree, TNode* __restrict__ nodes, int* status) {
+    int gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= total_internal) return;
+    int m = find_mesh(moff, M, gi, 1);
+    int n = moff[m + 1] - moff[m];
+    int k = gi - (moff[m] - m);
+    long long base = 2LL * moff[m] - m;
+    long long ch[2] = {tree[(base + k) * 4 + 1], tree[(base + k) * 4 + 2]};
+    float lo[2][3], hi[2][3];
+    int ref[2], aux[2];
+    for (int s = 0; s < 2; ++s) {
+        long long c = ch[s];
+        if (c <= 0 || c >= 2LL * n - 1) {
+            atomicOr(status, ST_MALFORMED_TREE);
+            c = 2LL * n - 2;     // keep the record pointing at a valid leaf
+        }
+        box_to_f32<T>(bboxes + (base + c) * 6, lo[s], hi[s]);
+        if (c >= n - 1) {
+            ref[s] = ~(int)(c - (n - 1));
+            long long id = tree[(base + c) * 4 + 3];
+            if (id < 0 || id >= n) {
+                atomicOr(status, ST_MALFORMED_TREE);
+                id = 0;
+            }
+            aux[s] = (int)id;
+        } else {
+            ref[s] = (int)c;
+            aux[s] = -1;
+        }
+    }
+    TNode t;
+    t.a = make_float4(lo[0][0], lo[0][1], lo[0][2], hi[0][0]);
+    t.b = make_float4(hi[0][1], hi[0][2], lo[1][0], lo[1][1]);
+    t.c = make_float4(lo[1][2], hi[1][0], hi[1][1], hi[1][2]);
+    t.d = make_int4(ref[0], ref[1], aux[0], aux[1]);
+    nodes[gi] = t;
+}
+
+// rightmost leaf position of every internal subtree, written into the parent's aux slot
+__global__ void k_import_rightmost(const int* __restrict__ moff, int M, int total, const long long* __restrict__ tree,
+                                   TNode* nodes, int* __restrict__ visits, int* __restrict__ rmk, int* status) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    int m = find_mesh(moff, M, g, 0);
+    int n = moff[m + 1] - moff[m];
+    if (n < 2) return;
+    int p = g - moff[m];
+    long long base = 2LL * moff[m] - m;
+    int ioff = moff[m] - m;
+    long long node = tree[(base + n - 1 + p) * 4 + 0];
+    for (int guard = 0; guard < n; ++guard) {
+        if (node < 0 || node >= n - 1) { atomicOr(status, ST_MALFORMED_TREE); return; }
+        __threadfence();
+        if (atomicAdd(visits + ioff + node, 1) == 0) return;
+        int4 d = nodes[ioff + node].d;
+        int rl = d.x < 0 ? ~d.x : __ldcg(rmk + ioff + d.x);
+        int rr = d.y < 0 ? ~d.y : __ldcg(rmk + ioff + d.y);
+        int r = max(rl, rr);
+        rmk[ioff + node] = r;
+        long long par = tree[(base + node) * 4 + 0];
+        if (par >= 0 && par < n - 1) {
+            int4 pd = nodes[ioff + par].d;
+            if (pd.x == (int)node) nodes[ioff + par].d.z = r;
+            else nodes[ioff + par].d.w = r;
+        }
+        if (node == 0) return;
+        node = par;
+    }
+    atomicOr(status, ST_MALFORMED_TREE);
+}
+
+// ---------------------------------------------------------------------------------------
+// Traversal (traverseBVH, collisions_static.cu:10-103; traverseBVHPartial,
+// collisions_continuous.cu:127-230).  One thread per query leaf, an explicit stack in
+// shared memory, fp32 child-box tests with outward rounding, then the exact
+// reference-precision leaf test for every fp32 hit.  Emits global triangle indices.
+
+__device__ __forceinline__ float nudge_down(float x) { return nextafterf(x, -INFINITY); }
+__device__ __forceinline__ float nudge_up(float x) { return nextafterf(x, INFINITY); }
+
+template <class T, bool MASKED, bool EXACT_F32>
+__global__ void __launch_bounds__(TRAV_THREADS)
+k_traverse(const TNode* __restrict__ nodes, const T* __restrict__ bboxes, const long long* __restrict__ tree,
+           const int* __restrict__ moff, int M, int total, const uint8_t* __restrict__ mask, T th,
+           int2* __restrict__ cand, int cand_cap, WsHeader* hdr) {
+    __shared__ int stack[STACK_DEPTH][TRAV_THREADS];
+    const int tid = threadIdx.x;
+    int g = blockIdx.x * blockDim.x + tid;
+    if (g >= total) return;
+    if (MASKED && !mask[g]) return;
+    int m = find_mesh(moff, M, g, 0);
+    int n = moff[m + 1] - moff[m];
+    if (n < 2) return;
+    int p = g - moff[m];
+    long long base = 2LL * moff[m] - m;
+    const TNode* nd = nodes + (moff[m] - m);
+    long long qrow = base + n - 1 + p;
+    Box<T> q = load_box(bboxes + qrow * 6);
+    long long qid64 = tree[qrow * 4 + 3];
+    if (qid64 < 0 || qid64 >= n) {
+        atomicOr(&hdr->status, ST_MALFORMED_TREE);
+        return;
+    }
+    int qid = (int)qid64;
+    // conservative fp32 query box: threshold folded in, rounded outward, nudged one more ulp
+    float qlo[3], qhi[3];
+    {
+        T lo[3] = {q.lo.x, q.lo.y, q.lo.z}, hi[3] = {q.hi.x, q.hi.y, q.hi.z};
+        for (int c = 0; c < 3; ++c) {
+            if (EXACT_F32) {
+                qlo[c] = (float)lo[c];
+                qhi[c] = (float)hi[c];
+            } else {
+                qlo[c] = nudge_down(__double2float_rd((double)lo[c] - (double)th));
+                qhi[c] = nudge_up(__double2float_ru((double)hi[c] + (double)th));
+            }
+        }
+    }
+    int sp = 0;
+    int node = 0;
+    const int limit = 4 * n + 64;
+    for (int it = 0;; ++it) {
+        if (it > limit) { atomicOr(&hdr->status, ST_MALFORMED_TREE); break; }
+        const float4* np = reinterpret_cast<const float4*>(nd + node);
+        float4 A = __ldg(np + 0), B = __ldg(np + 1), C = __ldg(np + 2);
+        int4 D = __ldg(reinterpret_cast<const int4*>(np + 3));
+        bool ol = (qlo[0] <= A.w) && (qhi[0] >= A.x) && (qlo[1] <= B.x) && (qhi[1] >= A.y) && (qlo[2] <= B.y) &&
+                  (qhi[2] >= A.z);
+        bool orr = (qlo[0] <= C.y) && (qhi[0] >= B.z) && (qlo[1] <= C.z) && (qhi[1] >= B.w) && (qlo[2] <= C.w) &&
+                   (qhi[2] >= C.x);
+        if (!MASKED) {
+            int rml = D.x < 0 ? ~D.x : D.z;
+            int rmr = D.y < 0 ? ~D.y : D.w;
+            if (p >= rml) ol = false;
+            if (p >= rmr) orr = false;
+        }
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            int ref = s ? D.y : D.x;
+            bool hit = (s ? orr : ol) && ref < 0;
+            if (hit) {
+                int cpos = ~ref;
+                int cid = s ? D.w : D.z;
+                if (MASKED && mask[moff[m] + cid] && !(qid < cid)) hit = false;
+                if (hit && !EXACT_F32) {
+                    Box<T> cb = load_box(bboxes + (base + n - 1 + cpos) * 6);
+                    hit = overlap(q, cb, th);
+                }
+                if (hit) {
+                    cg::coalesced_group grp = cg::coalesced_threads();
+                    int slot = 0;
+                    if (grp.thread_rank() == 0) slot = atomicAdd(&hdr->cand_count, (int)grp.size());
+                    slot = grp.shfl(slot, 0) + grp.thread_rank();
+                    if (slot < cand_cap) cand[slot] = make_int2(moff[m] + min(qid, cid), moff[m] + max(qid, cid));
+                }
+            }
+        }
+        bool tl = ol && D.x >= 0, tr = orr && D.y >= 0;
+        if (!tl && !tr) {
+            if (sp == 0) break;
+            node = stack[--sp][tid];
+        } else {
+            node = tl ? D.x : D.y;
+            if (tl && tr) {
+                if (sp >= STACK_DEPTH) { atomicOr(&hdr->status, ST_STACK_OVERFLOW); break; }
+                stack[sp++][tid] = D.y;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Narrow phases.  Grid-stride over the candidate buffer; the count is read on the device.
+
+// per-mesh append of one row; returns the row index within the mesh region or -1 when full
+__device__ __forceinline__ long long append_row(int* mesh_counters, int m, long long cap, int* status) {
+    cg::coalesced_group act = cg::coalesced_threads();
+    cg::coalesced_group grp = cg::labeled_partition(act, m);
+    int slot = 0;
+    if (grp.thread_rank() == 0) slot = atomicAdd(mesh_counters + m, (int)grp.size());
+    slot = grp.shfl(slot, 0) + grp.thread_rank();
+    if ((long long)slot >= cap) {
+        atomicOr(status, ST_OUT_OVERFLOW);
+        return -1;
+    }
+    return slot;
+}
+
+// find_collisions: SAT + shared-vertex count (collisions_static.cu:123-159)
+template <class T>
+__global__ void __launch_bounds__(NARROW_THREADS)
+k_static_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ tri,
+                const int* __restrict__ moff, int M, T th, long long* __restrict__ rows, int max_per_tri,
+                int* __restrict__ mesh_counters) {
+    int n = min(hdr->cand_count, cand_cap);
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        int2 pr = cand[c];
+        Tri<T> a = load_tri(tri, pr.x), b = load_tri(tri, pr.y);
+        bool keep = sat(a, b, th) && !(count_shared(a, b) > 0);
+        if (keep) {
+            int m = find_mesh(moff, M, pr.x, 0);
+            long long cap = (long long)(moff[m + 1] - moff[m]) * max_per_tri;
+            long long r = append_row(mesh_counters, m, cap, &hdr->status);
+            if (r >= 0) {
+                long long o = (long long)moff[m] * max_per_tri + r;
+                rows[o * 2 + 0] = pr.x - moff[m];
+                rows[o * 2 + 1] = pr.y - moff[m];
+            }
+        }
+    }
+}
+
+enum CcdMode { CCD_ROWS = 0, CCD_IMPULSES = 1, CCD_MINCOL = 2 };
+
+// continuous narrow phase (collisions_continuous.cu:14-765, collisions_impulses.cu:24-1067)
+template <class T, int MODE>
+__global__ void __launch_bounds__(NARROW_THREADS)
+k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ x0,
+             const T* __restrict__ x1, const int* __restrict__ moff, int M, long long* __restrict__ rows,
+             T* __restrict__ times, int max_per_tri, int* __restrict__ mesh_counters, const T* __restrict__ masses,
+             T* __restrict__ dv_out, T* __restrict__ dx_out, int* __restrict__ cnt_out) {
+    int n = min(hdr->cand_count, cand_cap);
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        int2 pr = cand[c];
+        MTri<T> a = load_mtri(x0, x1, pr.x), b = load_mtri(x0, x1, pr.y);
+        if (share_vertex(a.v, b.v)) continue;
+        uint32_t bits = ccd_subbox_mask(a, b);
+        while (bits) {
+            int k = __ffs(bits) - 1;
+            bits &= bits - 1;
+            if (MODE == CCD_MINCOL) {
+                int m = find_mesh(moff, M, pr.x, 0);
+                long long cap = (long long)(moff[m + 1] - moff[m]) * max_per_tri;
+                long long r = append_row(mesh_counters, m, cap, &hdr->status);
+                if (r >= 0) {
+                    long long o = (long long)moff[m] * max_per_tri + r;
+                    rows[o * 3 + 0] = pr.x - moff[m];
+                    rows[o * 3 + 1] = pr.y - moff[m];
+                    rows[o * 3 + 2] = k;
+                }
+                continue;
+            }
+            MTet<T> tet = make_tet(a, b, k);
+            T cf[4];
+            cubic_coeffs(tet, cf);
+            T rr[3];
+            solve_cubic<T>((double)cf[0], (double)cf[1], (double)cf[2], (double)cf[3], rr);
+#pragma unroll 1
+            for (int s = 0; s < 3; ++s) {
+                T root = rr[s];
+                if (!(root >= 0 && root <= 1)) continue;
+                if (!ccd_filter(tet, k, root)) continue;
+                if (MODE == CCD_ROWS) {
+                    int m = find_mesh(moff, M, pr.x, 0);
+                    long long cap = (long long)(moff[m + 1] - moff[m]) * max_per_tri;
+                    long long r = append_row(mesh_counters, m, cap, &hdr->status);
+                    if (r >= 0) {
+                        long long o = (long long)moff[m] * max_per_tri + r;
+                        rows[o * 3 + 0] = pr.x - moff[m];
+                        rows[o * 3 + 1] = pr.y - moff[m];
+                        rows[o * 3 + 2] = k;
+                        times[o] = root;
+                    }
+                } else {
+                    int side[4], corner[4];
+                    type_points(k, side, corner);
+                    T q[4];
+#pragma unroll
+                    for (int pt = 0; pt < 4; ++pt) q[pt] = masses[(long long)(side[pt] ? pr.y : pr.x) * 3 + corner[pt]];
+                    Contact<T> ct = contact(tet, k, root, q);
+                    // extrapolate_impulses (936-1067) + extrapolate_impulses_dv (609-933)
+                    T offset;
+                    if (fabs((double)ct.vn) < 1e-15) offset = (T)0.1;
+                    else offset = (T)((2 * CCC_THICKNESS) / (double)(-ct.vn));
+                    offset = (T)fmin(fmax((double)offset, 0.), 1.);
+                    T msum = ct.m0 + ct.m1;
+                    T mf0, mf1;
+                    if (fabs((double)msum) < 1e-15) { mf0 = (T)0.5; mf1 = (T)0.5; }
+                    else { mf0 = ct.m0 / msum; mf1 = 1 - mf0; }
+                    T mag0 = ct.vn * mf1;
+                    T mag1 = -ct.vn * mf0;
+                    T ro = (T)fmax((double)(root - offset), 0.);
+#pragma unroll
+                    for (int pt = 0; pt < 4; ++pt) {
+                        T mag = (k < 9) ? (pt < 2 ? mag0 : mag1) : (k < 12 ? (pt < 3 ? mag0 : mag1) : (pt < 1 ? mag0 : mag1));
+                        V3<T> imp = ct.n * mag;
+                        V3<T> nv = tet.dv[pt] + imp;
+                        V3<T> idx = (nv - tet.dv[pt]) * (1 - ro);
+                        long long tri = side[pt] ? pr.y : pr.x;
+                        T* d = dv_out + tri * 9 + corner[pt] * 3;
+                        atomicAdd(d + 0, imp.x); atomicAdd(d + 1, imp.y); atomicAdd(d + 2, imp.z);
+                        T* x = dx_out + tri * 9 + corner[pt] * 3;
+                        atomicAdd(x + 0, idx.x); atomicAdd(x + 1, idx.y); atomicAdd(x + 2, idx.z);
+                        atomicAdd(cnt_out + tri * 3 + corner[pt], 1);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// proximity (proximity_static.cu:11-508)
+template <class T>
+__global__ void __launch_bounds__(NARROW_THREADS)
+k_prox_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ tri,
+              const int* __restrict__ moff, int M, T th, long long* __restrict__ rows, int max_per_tri,
+              int* __restrict__ mesh_counters) {
+    int n = min(hdr->cand_count, cand_cap);
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        int2 pr = cand[c];
+        Tri<T> a = load_tri(tri, pr.x), b = load_tri(tri, pr.y);
+        if (share_vertex(a.v, b.v)) continue;
+        for (int k = 0; k < 15; ++k) {
+            if (!prox_subbox(a, b, k, th)) continue;
+            T d = prox_distance(a, b, k);
+            if (!(d <= th && d >= 0)) continue;
+            int m = find_mesh(moff, M, pr.x, 0);
+            long long cap = (long long)(moff[m + 1] - moff[m]) * max_per_tri;
+            long long r = append_row(mesh_counters, m, cap, &hdr->status);
+            if (r >= 0) {
+                long long o = (long long)moff[m] * max_per_tri + r;
+                rows[o * 3 + 0] = pr.x - moff[m];
+                rows[o * 3 + 1] = pr.y - moff[m];
+                rows[o * 3 + 2] = k;
+            }
+        }
+    }
+}
+
+// compute_impulses_from_collisions (collisions_impulses.cu:1738-1880) on caller rows.
+// Rows with an index outside [0, F) or a type outside [0, 15) are skipped (the reference
+// reads out of bounds on its -1 padding rows).
+template <class T>
+__global__ void __launch_bounds__(NARROW_THREADS)
+k_impulses_from_rows(const long long* __restrict__ rows, const T* __restrict__ roots, int B, long long N, int F,
+                     const T* __restrict__ x0, const T* __restrict__ x1, const T* __restrict__ masses,
+                     T* __restrict__ dv_out, T* __restrict__ dx_out, int* __restrict__ cnt_out, WsHeader* hdr) {
+    long long total = (long long)B * N;
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < total;
+         r += (long long)gridDim.x * blockDim.x) {
+        long long b = r / N;
+        long long i = rows[r * 3 + 0], j = rows[r * 3 + 1], kk = rows[r * 3 + 2];
+        if (i < 0 || j < 0 || i >= F || j >= F || kk < 0 || kk >= 15) continue;
+        int k = (int)kk;
+        long long gi = b * F + i, gj = b * F + j;
+        T root = roots[r];
+        MTri<T> a = load_mtri(x0, x1, gi), bb = load_mtri(x0, x1, gj);
+        MTet<T> tet = make_tet(a, bb, k);
+        int side[4], corner[4];
+        type_points(k, side, corner);
+        T q[4];
+        for (int pt = 0; pt < 4; ++pt) q[pt] = masses[(side[pt] ? gj : gi) * 3 + corner[pt]];
+        Contact<T> ct = contact(tet, k, root, q);
+        T offset;
+        if (fabs((double)ct.vn) < 1e-15) offset = (T)0.1;
+        else offset = (T)((2 * CCC_THICKNESS) / (double)(-ct.vn));
+        offset = (T)fmin(fmax((double)offset, 0.), 1.);
+        T msum = ct.m0 + ct.m1;
+        T mf0, mf1;
+        if (fabs((double)msum) < 1e-15) { mf0 = (T)0.5; mf1 = (T)0.5; }
+        else { mf0 = ct.m0 / msum; mf1 = 1 - mf0; }
+        T mag0 = ct.vn * mf1;
+        T mag1 = -ct.vn * mf0;
+        T ro = (T)fmax((double)(root - offset), 0.);
+        for (int pt = 0; pt < 4; ++pt) {
+            T mag = (k < 9) ? (pt < 2 ? mag0 : mag1) : (k < 12 ? (pt < 3 ? mag0 : mag1) : (pt < 1 ? mag0 : mag1));
+            V3<T> imp = ct.n * mag;
+            V3<T> nv = tet.dv[pt] + imp;
+            V3<T> idx = (nv - tet.dv[pt]) * (1 - ro);
+            long long tri = side[pt] ? gj : gi;
+            T* d = dv_out + tri * 9 + corner[pt] * 3;
+            atomicAdd(d + 0, imp.x); atomicAdd(d + 1, imp.y); atomicAdd(d + 2, imp.z);
+            T* x = dx_out + tri * 9 + corner[pt] * 3;
+            atomicAdd(x + 0, idx.x); atomicAdd(x + 1, idx.y); atomicAdd(x + 2, idx.z);
+            atomicAdd(cnt_out + tri * 3 + corner[pt], 1);
+        }
+    }
+}
+
+}  // namespace ccc

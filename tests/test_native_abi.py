@@ -1,0 +1,73 @@
+"""The C ABI library builds, loads without a GPU and exports every declared symbol."""
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+
+def _declared_functions():
+    src = open(os.path.join(ROOT, "include", "ccc_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(ccc_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_the_reference_entry_points():
+    names = _declared_functions()
+    for n in ("ccc_bvh", "ccc_find_collisions", "ccc_find_collisions_continuous", "ccc_find_proximity",
+              "ccc_find_mincol_cand", "ccc_compute_impulses", "ccc_compute_impulses_from_collisions",
+              "ccc_workspace_size", "ccc_read_status"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol(native_lib):
+    from cccollisions_b200 import _native
+    for name in _declared_functions():
+        assert hasattr(native_lib, name), name
+        assert name in _native.SIGNATURES, name
+
+
+def test_pure_host_calls(native_lib):
+    from cccollisions_b200 import _native as N
+    assert native_lib.ccc_version() >= 1
+    assert native_lib.ccc_error_string(N.CCC_OK) == b"ok"
+    for op in range(6):
+        a = native_lib.ccc_workspace_size(op, 1, 1000, 16)
+        b = native_lib.ccc_workspace_size(op, 2, 1000, 16)
+        assert 0 < a <= b
+    assert native_lib.ccc_workspace_size(0, 1, 1, 16) == -1      # F >= 2 is required
+    # argument errors are reported before any device work (no GPU touched)
+    rc = native_lib.ccc_bvh(7, None, None, 1, 10, None, None, None, 0, None)
+    assert rc == 1
+    rc = native_lib.ccc_find_collisions(0, None, None, None, 1, 1, 0.0, 16, None, None, 0, None)
+    assert rc == 1
+
+
+def test_api_mirrors_reference_signatures():
+    import inspect
+    import cccollisions_b200 as C
+    sig = lambda f: list(inspect.signature(f).parameters.items())
+    p = sig(C.find_collisions)
+    assert [k for k, _ in p] == ["bboxes", "tree", "triangles", "threshold", "max_collisions"]
+    assert p[3][1].default == 0.0 and p[4][1].default == 16
+    p = sig(C.find_collisions_continuous)
+    assert [k for k, _ in p] == ["bboxes", "tree", "triangles", "triangles_next", "max_candidates_per_triangle",
+                                 "max_collisions_per_triangle"]
+    p = sig(C.compute_impulses_partial)
+    assert [k for k, _ in p][:6] == ["bboxes", "tree", "triangles", "triangles_next", "triangles_mass",
+                                     "triangles_to_check"]
+    assert [k for k, _ in sig(C.find_proximity)] == ["bboxes", "tree", "triangles", "threshold",
+                                                    "max_candidates_per_triangle"]
+    assert [k for k, _ in sig(C.compute_impulses_from_collisions)] == ["collisions", "roots", "triangles",
+                                                                      "triangles_next", "triangles_mass"]
+    with pytest.raises(NotImplementedError):
+        C.find_triangle_edge_collisions(None, None, None)
+
+
+def test_api_rejects_cpu_tensors():
+    import torch
+    import cccollisions_b200 as C
+    t = torch.zeros((1, 4, 3, 3))
+    with pytest.raises(RuntimeError, match="CUDA"):
+        C.bvh(t)

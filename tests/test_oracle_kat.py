@@ -1,0 +1,310 @@
+"""Known-answer and brute-force pins of the CPU oracle (no GPU needed).
+
+The reference ships no tests or golden vectors, so the oracle's restatement is pinned by
+hand-derived values: Morton interleaving, the Karras topology over all-equal keys, the
+reference's unbounded-scene-box quirk, each branch of the cubic solver, analytic times of
+impact, the separating-axis test on known configurations, CAMPARY products against exact
+rational arithmetic, and O(F^2) brute force for candidate pairs.
+"""
+import math
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+from conftest import random_mesh_soup
+
+
+# ----------------------------------------------------------------------------- primitives
+
+def test_morton_known_values(oracle):
+    # expandBits interleaves x*4 + y*2 + z over 10 bits per axis (bvh.cu:29-62)
+    assert oracle.morton(0.0, 0.0, 0.0) == 0
+    assert oracle.morton(1.0, 1.0, 1.0) == (1 << 30) - 1        # clamps to 1023 on each axis
+    # x = 1/1024 -> cell 1 -> bit 2
+    assert oracle.morton(1.0 / 1024, 0.0, 0.0) == 4
+    assert oracle.morton(0.0, 1.0 / 1024, 0.0) == 2
+    assert oracle.morton(0.0, 0.0, 1.0 / 1024) == 1
+    assert oracle.morton(2.0 / 1024, 0.0, 0.0) == 32
+    # negative and NaN clamp to 0 (fmax semantics)
+    assert oracle.morton(-5.0, float("nan"), 0.0) == 0
+    assert oracle.morton(0.5, 0.5, 0.5, single=True) == oracle.morton(0.5, 0.5, 0.5)
+
+
+def test_karras_identity_topology_n8(oracle):
+    # all-equal keys with ids 0..7: delta(i, j) = 32 + clz(i ^ j), i.e. the radix tree of
+    # the indices
+    tri = np.zeros((8, 3, 3), dtype=np.float64)
+    tri[:, :, 0] = np.arange(8)[:, None] + np.array([0.0, 0.5, 0.0])
+    tri[:, 2, 1] = 1.0
+    bb, tr = oracle.bvh(tri)
+    expect = np.array([[-1, 3, 4, -1], [3, 7, 8, -1], [3, 9, 10, -1], [0, 1, 2, -1], [0, 5, 6, -1],
+                       [4, 11, 12, -1], [4, 13, 14, -1]])
+    assert (tr[:7] == expect).all()
+    assert (tr[7:, 0] == [1, 1, 2, 2, 5, 5, 6, 6]).all()
+    assert (tr[7:, 1:3] == -1).all()
+    assert (tr[7:, 3] == np.arange(8)).all()
+    # internal boxes are unions of their children
+    for k in range(7):
+        l, r = tr[k, 1], tr[k, 2]
+        assert (bb[k, :3] == np.minimum(bb[l, :3], bb[r, :3])).all()
+        assert (bb[k, 3:] == np.maximum(bb[l, 3:], bb[r, 3:])).all()
+
+
+def test_reference_scene_box_gives_zero_codes(oracle):
+    # AABB() is (-MAX, +MAX) (aabb.cu:114-122) and seeds the scene-box reduction
+    # (build_bvh.cu:243), so every normalised centroid is 0 and every code is 0
+    x0, x1, _ = random_mesh_soup(3)
+    _, _, codes = oracle.bvh(x0, return_codes=True)
+    assert (codes == 0).all()
+    _, _, codes_m = oracle.bvh(x0, x1, return_codes=True)
+    assert (codes_m == 0).all()
+    _, _, codes32 = oracle.bvh(x0.astype(np.float32), return_codes=True)
+    assert (codes32 == 0).all()
+    # a bounded scene box gives real codes
+    _, _, codes_s = oracle.bvh(x0, spatial=True, return_codes=True)
+    assert len(np.unique(codes_s)) > 10
+
+
+def _ulp(x):
+    return math.ulp(x)
+
+
+def test_cbrt_within_one_ulp(oracle):
+    g = np.random.default_rng(5)
+    xs = list(np.exp(g.uniform(-700, 700, 3000))) + [1e-310, 5e-324, 8.0, 27.0, 1.0, 0.001, 1e-16]
+    for x in xs:
+        y = oracle.cbrt(float(x))
+        if x == 8.0:
+            assert y == 2.0
+        if x == 27.0:
+            assert y == 3.0
+        fx = Fraction(float(x))
+        # correctly rounded c satisfies (c - ulp/2)^3 <= x <= (c + ulp/2)^3; accept 1 ulp
+        u = Fraction(_ulp(y))
+        lo = Fraction(y) - u
+        hi = Fraction(y) + u
+        assert lo ** 3 <= fx <= hi ** 3, x
+        assert oracle.cbrt(-float(x)) == -y
+
+
+def test_trig_within_two_ulp(oracle):
+    g = np.random.default_rng(7)
+    for x in g.uniform(-1.0, 1.0, 4000):
+        a = oracle.acos(float(x))
+        assert abs(a - math.acos(x)) <= 2 * _ulp(math.acos(x)), x
+    for x in list(g.uniform(0.0, math.pi / 3, 4000)) + [0.0, 1e-300, 1.0471975511965976]:
+        c, s = oracle.cos(float(x)), oracle.sin(float(x))
+        assert abs(c - math.cos(x)) <= 2 * _ulp(math.cos(x)), x
+        assert abs(s - math.sin(x)) <= 2 * max(_ulp(math.sin(x)), 5e-324), x
+    assert oracle.acos(1.0) == 0.0
+    assert abs(oracle.acos(-1.0) - math.pi) <= _ulp(math.pi)
+    assert math.isnan(oracle.acos(1.5))
+
+
+def test_certmul_matches_exact_products(oracle):
+    # certifiedMul<1,1,2> gives an exact 2-term expansion of a double product
+    # (multiplication.h:132-184); <2,1,2> rounds a 3-term exact product to 2 terms
+    g = np.random.default_rng(11)
+    for _ in range(3000):
+        b = float(g.uniform(-1, 1) * 10.0 ** g.integers(-12, 3))
+        r = oracle.certmul(b, b)
+        assert Fraction(r[0]) + Fraction(r[1]) == Fraction(b) * Fraction(b)
+        assert r[0] == b * b
+        c = oracle.certmul(r, b)
+        exact = Fraction(b) ** 3
+        approx = Fraction(c[0]) + Fraction(c[1])
+        if exact != 0:
+            assert abs(approx - exact) <= abs(exact) * Fraction(1, 2 ** 100)
+        # leading term within one ulp of the correctly rounded cube
+        assert abs(c[0] - float(exact)) <= _ulp(float(exact)) if exact != 0 else c[0] == 0
+
+
+# ----------------------------------------------------------------------------- cubic solver
+
+def test_solve_cubic_branches(oracle):
+    # linear (a == b == 0): the reference never stores the root
+    assert (oracle.solve_cubic(0.0, 0.0, 1.0, -0.5) == -1).all()
+    # quadratic (|a| < 1e-16): (t - 0.25)(t - 0.75) = t^2 - t + 0.1875
+    r = oracle.solve_cubic(1e-18, 1.0, -1.0, 0.1875)
+    assert sorted(r[:2]) == pytest.approx([0.25, 0.75], abs=1e-15) and r[2] == -1
+    # three real roots: (t - 0.1)(t - 0.5)(t - 0.9)
+    a, b, c, d = 1.0, -1.5, 0.59, -0.045
+    r = oracle.solve_cubic(a, b, c, d)
+    assert sorted(r) == pytest.approx([0.1, 0.5, 0.9], abs=1e-12)
+    # one real root (h > 0): (t - 0.3)(t^2 + 1)
+    r = oracle.solve_cubic(1.0, -0.3, 1.0, -0.3)
+    assert r[0] == pytest.approx(0.3, abs=1e-14) and (r[1:] == -1).all()
+    # roots outside [-eps, 1 + eps] are dropped: (t - 2)(t - 3)(t - 4)
+    assert (oracle.solve_cubic(1.0, -9.0, 26.0, -24.0) == -1).all()
+    # triple root (f == g == h == 0): (t - 0.5)^3 -> d / a = -0.125, root from float cbrt
+    r = oracle.solve_cubic(1.0, -1.5, 0.75, -0.125)
+    assert r[0] == pytest.approx(0.5, abs=1e-6)
+
+
+def _tet(v, dv):
+    return np.concatenate([np.asarray(v, float).ravel(), np.asarray(dv, float).ravel()])
+
+
+def test_cubic_coeffs_vertex_face_analytic(oracle):
+    # face z = 0 (points 0..2), vertex at z = 1 moving -2 per step: det linear in t with
+    # root 0.5; the cubic's coefficients are those of det(v - v3 + t (dv - dv3))
+    v = [[0, 0, 0], [1, 0, 0], [0, 1, 0], [0.2, 0.2, 1.0]]
+    dv = [[0, 0, 0], [0, 0, 0], [0, 0, 0], [0, 0, -2.0]]
+    c = oracle.cubic_coeffs(_tet(v, dv))
+    m = lambda t: np.array(v[:3]) - np.array(v[3]) + t * (np.array(dv[:3]) - np.array(dv[3]))
+    for t in (0.0, 0.3, 1.0, -2.0):
+        assert c[0] * t ** 3 + c[1] * t ** 2 + c[2] * t + c[3] == pytest.approx(np.linalg.det(m(t)), abs=1e-12)
+
+
+# ----------------------------------------------------------------------------- CCD known answers
+
+def _soup(*tris):
+    return np.ascontiguousarray(np.array(tris, dtype=np.float64))
+
+
+def test_ccd_vertex_face_time_of_impact(oracle):
+    # face of triangle 0 stays in z = 0 but grows (v1, v2 move outward in the plane);
+    # triangle 1's vertex 0 goes from z = 0.4 to z = -0.6: det(t) ~ (0.4 - t)(1 + t/2)^2,
+    # a genuine cubic with the impact at t = 0.4 (inside the face)
+    t0 = [[0, 0, 0], [1, 0, 0], [0, 1, 0]]
+    t0n = [[0, 0, 0], [1.5, 0, 0], [0, 1.5, 0]]
+    t1 = [[0.2, 0.2, 0.4], [2.0, 2.0, 0.4], [2.0, 3.0, 0.4]]
+    t1n = [[0.2, 0.2, -0.6], [2.0, 2.0, 0.4], [2.0, 3.0, 0.4]]
+    x0 = _soup(t0, t1)
+    x1 = _soup(t0n, t1n)
+    bb, tr = oracle.bvh(x0, x1)
+    rows, times = oracle.ccd(bb, tr, x0, x1)
+    vf = [t for r, t in zip(rows.tolist(), times.tolist()) if tuple(r) == (0, 1, 9)]
+    assert len(vf) == 1 and abs(vf[0] - 0.4) < 1e-12
+
+
+def test_ccd_rigid_translation_is_dropped(oracle):
+    # a static face and a vertex translating through it make the coplanarity polynomial
+    # linear (a == b == 0); the reference computes -d/c into a local and never stores it
+    # (collisions_continuous.cu:532-536), so no row is reported
+    t0 = [[0, 0, 0], [1, 0, 0], [0, 1, 0]]
+    t1 = [[0.2, 0.2, 0.4], [2.0, 2.0, 0.4], [2.0, 3.0, 0.4]]
+    t1n = [[0.2, 0.2, -0.6], [2.0, 2.0, -0.6], [2.0, 3.0, -0.6]]
+    x0 = _soup(t0, t1)
+    x1 = _soup(t0, t1n)
+    bb, tr = oracle.bvh(x0, x1)
+    rows, _ = oracle.ccd(bb, tr, x0, x1)
+    assert len(rows) == 0
+    # the sub-test itself is a candidate
+    assert (0, 1, 9) in set(map(tuple, oracle.mincol_cand(bb, tr, x0, x1).tolist()))
+
+
+def test_ccd_edge_edge_crossing(oracle):
+    # edge (0,1) of triangle 0 along x at z = 0 (static); edge (0,1) of triangle 1 along y
+    # at z = 0.2 moving down 0.4 while stretching -> crossing at t = 0.5 at both midpoints
+    t0 = [[-1, 0, 0], [1, 0, 0], [0, -3, -5]]
+    t1 = [[0, -1, 0.2], [0, 1, 0.2], [3, 0, 5]]
+    t1n = [[0, -1.5, -0.2], [0, 1.5, -0.2], [3, 0, 5]]
+    x0 = _soup(t0, t1)
+    x1 = _soup(t0, t1n)
+    bb, tr = oracle.bvh(x0, x1)
+    rows, times = oracle.ccd(bb, tr, x0, x1)
+    ee = [t for r, t in zip(rows.tolist(), times.tolist()) if tuple(r) == (0, 1, 0)]
+    assert len(ee) == 1 and abs(ee[0] - 0.5) < 1e-12
+
+
+def test_ccd_shared_vertex_rejected(oracle):
+    # triangles sharing a vertex (exact coordinates) never produce sub-tests
+    t0 = [[0, 0, 0], [1, 0, 0], [0, 1, 0]]
+    t1 = [[0, 0, 0], [0.3, 0.3, 0.5], [0.3, -0.2, -0.5]]
+    x0 = _soup(t0, t1)
+    x1 = x0.copy()
+    x1[1, 1:, 2] *= -1
+    bb, tr = oracle.bvh(x0, x1)
+    rows, _ = oracle.ccd(bb, tr, x0, x1)
+    assert len(rows) == 0
+    assert len(oracle.mincol_cand(bb, tr, x0, x1)) == 0
+
+
+# ----------------------------------------------------------------------------- static SAT
+
+def test_sat_known_configurations(oracle):
+    a = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], dtype=np.float64)
+    pierce = np.array([[0.2, 0.2, -1], [0.3, 0.2, 1], [0.2, 0.3, 1]], dtype=np.float64)
+    above = pierce + [0, 0, 3.0]
+    assert oracle.sat(a, pierce)
+    assert not oracle.sat(a, above)
+    assert oracle.sat(a, above, threshold=2.5)     # the threshold widens every interval
+    # coplanar overlapping and coplanar disjoint
+    assert oracle.sat(a, a + [0.1, 0.1, 0])
+    assert not oracle.sat(a, a + [2.0, 0, 0])
+    assert oracle.sat(a.astype(np.float32), pierce.astype(np.float32))
+
+
+# ----------------------------------------------------------------------------- brute force
+
+def _brute_pairs(bb, tr, th=0.0):
+    n = (bb.shape[0] + 1) // 2
+    lo, hi, ids = bb[n - 1:, :3], bb[n - 1:, 3:], tr[n - 1:, 3]
+    out = set()
+    for p in range(n):
+        ok = np.all((lo[p] <= hi + th) & (hi[p] >= lo - th), axis=1)
+        for q in np.nonzero(ok)[0]:
+            if q > p:
+                out.add((min(ids[p], ids[q]), max(ids[p], ids[q])))
+    return out
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_candidates_equal_brute_force(oracle, seed, dtype):
+    x0, x1, _ = random_mesh_soup(seed, dtype=dtype)
+    for motion in (False, True):
+        bb, tr = oracle.bvh(x0, x1 if motion else None)
+        for th in (0.0, 0.01):
+            c = oracle.candidates(bb, tr, threshold=th)
+            assert len(c) == len(set(map(tuple, c.tolist())))
+            assert set(map(tuple, c.tolist())) == _brute_pairs(bb, tr, dtype(th))
+    # the spatial (Morton) build gives the same candidate set
+    bbs, trs = oracle.bvh(x0, x1, spatial=True)
+    bbr, trr = oracle.bvh(x0, x1)
+    assert set(map(tuple, oracle.candidates(bbs, trs).tolist())) == set(map(tuple, oracle.candidates(bbr, trr).tolist()))
+
+
+def test_partial_mask_semantics(oracle):
+    x0, x1, _ = random_mesh_soup(4)
+    bb, tr = oracle.bvh(x0, x1)
+    n = x0.shape[0]
+    full = set(map(tuple, oracle.candidates(bb, tr).tolist()))
+    allm = np.ones(n, dtype=np.uint8)
+    c = oracle.candidates(bb, tr, mask=allm)
+    # all triangles checked: each overlapping pair once (query id < other id)
+    assert sorted(map(tuple, c.tolist())) == sorted(full)
+    none = np.zeros(n, dtype=np.uint8)
+    assert len(oracle.candidates(bb, tr, mask=none)) == 0
+    g = np.random.default_rng(0)
+    m = (g.random(n) < 0.3).astype(np.uint8)
+    cm = oracle.candidates(bb, tr, mask=m)
+    # a pair appears iff one of its triangles is checked; pairs with both checked once,
+    # pairs with one checked once (identity leaf order: position == id)
+    expect = sorted(p for p in full if m[p[0]] or m[p[1]])
+    assert sorted(map(tuple, cm.tolist())) == expect
+
+
+def test_ccd_multithreaded_equals_single(oracle):
+    x0, x1, _ = random_mesh_soup(6, nx=12, ny=12)
+    bb, tr = oracle.bvh(x0, x1)
+    r1, t1 = oracle.ccd(bb, tr, x0, x1, nthreads=1)
+    r4, t4 = oracle.ccd(bb, tr, x0, x1, nthreads=4)
+    assert oracle.row_multiset(r1, t1) == oracle.row_multiset(r4, t4)
+    assert len(r1) > 0
+
+
+def test_impulses_from_rows_match_full(oracle):
+    x0, x1, m = random_mesh_soup(8)
+    bb, tr = oracle.bvh(x0, x1)
+    rows, times = oracle.ccd(bb, tr, x0, x1)
+    dv, dx, cnt, nc = oracle.impulses(bb, tr, x0, x1, m)
+    dv2, dx2, cnt2 = oracle.impulses_from_rows(x0, x1, m, rows, times)
+    assert nc == len(rows) > 0
+    assert (cnt == cnt2).all()
+    assert np.allclose(dv, dv2, rtol=1e-12, atol=1e-15)
+    assert np.allclose(dx, dx2, rtol=1e-12, atol=1e-15)
+    # every contact touches exactly four corners
+    assert cnt.sum() == 4 * nc
