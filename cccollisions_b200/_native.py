@@ -28,6 +28,7 @@ SIGNATURES = {
     "ccc_version": (_I, []),
     "ccc_error_string": (ctypes.c_char_p, [_I]),
     "ccc_kernel_launches": (_I64, []),
+    "ccc_debug_math": (_I, [_I, _P, _P, _I64, _P]),
     "ccc_timing_begin": (_I, []),
     "ccc_timing_end": (_I, [_I, _P, _I, _P, _P]),
     "ccc_workspace_size": (_I64, [_I, _I64, _I64, _I64]),

@@ -299,6 +299,15 @@ int ccc_version(void) { return 1; }
 
 int64_t ccc_kernel_launches(void) { return g_launches; }
 
+int ccc_debug_math(int op, const double* in, double* out, int64_t n, void* stream) {
+    if (op < 0 || op > 11 || n < 0 || (n > 0 && (!in || !out)) || n >= ((int64_t)1 << 31)) return CCC_ERR_INVALID_ARG;
+    if (n == 0) return CCC_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    CCC_LAUNCH("k_debug_math", s, k_debug_math<<<grid_for(n, 128), 128, 0, s>>>(op, in, out, (int)n));
+    CCC_LAUNCH_CHECK();
+    return CCC_OK;
+}
+
 int ccc_timing_begin(void) {
     g_timing = true;
     g_ntimed = 0;

@@ -24,82 +24,109 @@ CCC_HD double ccc_fma(double a, double b, double c) {
 #endif
 }
 
+// Values are passed and returned by value (no pointers into locals), which keeps the
+// device code straightforward.
+struct ccc_dd {
+    double hi, lo;
+};
+
 // s = fl(a + b) and the exact error b - (s - a); valid when |a| >= |b|
-CCC_HD double ccc_fast_two_sum(double a, double b, double* err) {
-    double s = a + b;
-    double z = s - a;
-    *err = b - z;
-    return s;
+CCC_HD ccc_dd ccc_fast_two_sum(double a, double b) {
+    ccc_dd r;
+    r.hi = a + b;
+    double z = r.hi - a;
+    r.lo = b - z;
+    return r;
 }
 
-// r[0..1] = expansion (x[0] (+ x[1] when k == 2)) * y, bins of 45 bits, 4 live bins.
-CCC_HD void ccc_certmul_r2(const double* x, int k, double y, double* r) {
+// (x0 (+ x1 when k == 2)) * y rounded to a 2-term expansion: bins of 45 bits, 4 live bins.
+CCC_HD ccc_dd ccc_certmul(double x0, double x1, int k, double y) {
     const int BIN = 45;
-    const int NB = 4;                      // 2*53/45 + 2
-    double bins[NB + 2], bias[NB + 2];
-    int ex0 = ccc_frexp_exp(x[0]);
-    int ex1 = (k > 1) ? ccc_frexp_exp(x[1]) : 0;
+    double b0, b1, b2, b3, b4, b5;           // bins (6 slots, the last two spill targets)
+    double s0, s1, s2, s3;                   // biases of the live bins
+    int ex0 = ccc_frexp_exp(x0);
+    int ex1 = (k > 1) ? ccc_frexp_exp(x1) : 0;
     int ey = ccc_frexp_exp(y);
     int e0 = ex0 + ey;
-    bias[0] = ccc_ldexp(1.5, e0 - BIN + 52);
-    bins[0] = bias[0];
     const double step = ccc_pow2i(-BIN);
-    for (int i = 1; i < NB + 2; ++i) {
-        bias[i] = bias[i - 1] * step;
-        bins[i] = bias[i];
-    }
+    s0 = ccc_ldexp(1.5, e0 - BIN + 52);
+    s1 = s0 * step;
+    s2 = s1 * step;
+    s3 = s2 * step;
+    double s4 = s3 * step;
+    double s5 = s4 * step;
+    b0 = s0; b1 = s1; b2 = s2; b3 = s3; b4 = s4; b5 = s5;
     for (int i = 0; i < k; ++i) {
-        double xi = x[i];
+        double xi = i == 0 ? x0 : x1;
         // a zero partial product leaves every bin unchanged
         if (xi == 0.0 || y == 0.0) continue;
         int l = e0 - ((i == 0 ? ex0 : ex1) + ey);
         int sh = l / BIN;
         l = l - sh * BIN;
-        if (sh < 0 || sh >= NB - 1) continue;
+        if (sh < 0 || sh >= 3) continue;
         double p = xi * y;
         double e = ccc_fma(xi, y, -p);
+        // the bins touched are sh .. sh+3; work on a window w0..w3 and write it back
+        double w0 = sh == 0 ? b0 : (sh == 1 ? b1 : b2);
+        double w1 = sh == 0 ? b1 : (sh == 1 ? b2 : b3);
+        double w2 = sh == 0 ? b2 : (sh == 1 ? b3 : b4);
+        double w3 = sh == 0 ? b3 : (sh == 1 ? b4 : b5);
+        ccc_dd t;
         if (l < 30) {
-            bins[sh] = ccc_fast_two_sum(bins[sh], p, &p);
-            bins[sh + 1] = bins[sh + 1] + p;
-            bins[sh + 1] = ccc_fast_two_sum(bins[sh + 1], e, &e);
-            bins[sh + 2] = bins[sh + 2] + e;
+            t = ccc_fast_two_sum(w0, p); w0 = t.hi; p = t.lo;
+            w1 = w1 + p;
+            t = ccc_fast_two_sum(w1, e); w1 = t.hi; e = t.lo;
+            w2 = w2 + e;
         } else if (l < 37) {
-            bins[sh] = ccc_fast_two_sum(bins[sh], p, &p);
-            bins[sh + 1] = bins[sh + 1] + p;
-            bins[sh + 1] = ccc_fast_two_sum(bins[sh + 1], e, &e);
-            bins[sh + 2] = ccc_fast_two_sum(bins[sh + 2], e, &e);
-            bins[sh + 3] = bins[sh + 3] + e;
+            t = ccc_fast_two_sum(w0, p); w0 = t.hi; p = t.lo;
+            w1 = w1 + p;
+            t = ccc_fast_two_sum(w1, e); w1 = t.hi; e = t.lo;
+            t = ccc_fast_two_sum(w2, e); w2 = t.hi; e = t.lo;
+            w3 = w3 + e;
         } else {
-            bins[sh] = ccc_fast_two_sum(bins[sh], p, &p);
-            bins[sh + 1] = ccc_fast_two_sum(bins[sh + 1], p, &p);
-            bins[sh + 2] = bins[sh + 2] + p;
-            bins[sh + 2] = ccc_fast_two_sum(bins[sh + 2], e, &e);
-            bins[sh + 3] = bins[sh + 3] + e;
+            t = ccc_fast_two_sum(w0, p); w0 = t.hi; p = t.lo;
+            t = ccc_fast_two_sum(w1, p); w1 = t.hi; p = t.lo;
+            w2 = w2 + p;
+            t = ccc_fast_two_sum(w2, e); w2 = t.hi; e = t.lo;
+            w3 = w3 + e;
         }
+        if (sh == 0) { b0 = w0; b1 = w1; b2 = w2; b3 = w3; }
+        else if (sh == 1) { b1 = w0; b2 = w1; b3 = w2; b4 = w3; }
+        else { b2 = w0; b3 = w1; b4 = w2; b5 = w3; }
     }
-    for (int i = 0; i < NB; ++i) bins[i] = bins[i] + (-bias[i]);
+    b0 = b0 + (-s0);
+    b1 = b1 + (-s1);
+    b2 = b2 + (-s2);
+    b3 = b3 + (-s3);
     // VecSumErrBranch: carry a running sum, emit a term whenever its error is non-zero
+    double r0 = 0.0, r1 = 0.0;
     int out = 0;
-    double carry = bins[0];
-    for (int i = 1; i < NB && out < 2; ++i) {
-        double err;
-        double s = ccc_fast_two_sum(carry, bins[i], &err);
-        r[out] = s;
-        carry = err;
-        if (carry == 0.0) carry = s;
+    double carry = b0;
+    for (int i = 1; i < 4 && out < 2; ++i) {
+        double bi = i == 1 ? b1 : (i == 2 ? b2 : b3);
+        ccc_dd t = ccc_fast_two_sum(carry, bi);
+        if (out == 0) r0 = t.hi;
+        else r1 = t.hi;
+        carry = t.lo;
+        if (carry == 0.0) carry = t.hi;
         else ++out;
     }
-    if (out < 2 && carry != 0.0) r[out++] = carry;
-    for (int i = out; i < 2; ++i) r[i] = 0.0;
+    if (out < 2 && carry != 0.0) {
+        if (out == 0) r0 = carry;
+        else r1 = carry;
+        ++out;
+    }
+    if (out < 1) r0 = 0.0;
+    if (out < 2) r1 = 0.0;
+    ccc_dd r;
+    r.hi = r0;
+    r.lo = r1;
+    return r;
 }
 
 // Leading terms the solver uses: x^2 (as a 2-term expansion) and x^3 = (x^2) * x.
-CCC_HD void ccc_sq_dd(double x, double* r2) {
-    ccc_certmul_r2(&x, 1, x, r2);
-}
+CCC_HD ccc_dd ccc_sq_dd(double x) { return ccc_certmul(x, 0.0, 1, x); }
 CCC_HD double ccc_cube_hi(double x) {
-    double s[2], c[2];
-    ccc_certmul_r2(&x, 1, x, s);
-    ccc_certmul_r2(s, 2, x, c);
-    return c[0];
+    ccc_dd s = ccc_sq_dd(x);
+    return ccc_certmul(s.hi, s.lo, 2, x).hi;
 }

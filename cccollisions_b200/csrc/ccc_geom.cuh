@@ -320,12 +320,9 @@ template <class T> __device__ __noinline__ void solve_cubic(double a, double b, 
     } else {
         double f = ((3.0 * c / a) - ((b * b) / (a * a))) / 3.0;
         double b3 = 2 * ccc_cube_hi(b);
-        double a2dd[2];
-        ccc_sq_dd(a, a2dd);
-        double a2 = a2dd[0];
-        double a3c[2];
-        ccc_certmul_r2(a2dd, 2, a, a3c);
-        double a3 = a3c[0];
+        ccc_dd a2dd = ccc_sq_dd(a);
+        double a2 = a2dd.hi;
+        double a3 = ccc_certmul(a2dd.hi, a2dd.lo, 2, a).hi;
         double p1 = b3 / a3;
         double p2 = (b * c * 9) / a2;
         double p3 = 27.0 * d / a;

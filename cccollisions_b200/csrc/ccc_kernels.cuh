@@ -338,6 +338,7 @@ k_traverse(const TNode* __restrict__ nodes, const T* __restrict__ bboxes, const 
                     if (grp.thread_rank() == 0) slot = atomicAdd(&hdr->cand_count, (int)grp.size());
                     slot = grp.shfl(slot, 0) + grp.thread_rank();
                     if (slot < cand_cap) cand[slot] = make_int2(moff[m] + min(qid, cid), moff[m] + max(qid, cid));
+                    else atomicOr(&hdr->status, ST_CAND_OVERFLOW);
                 }
             }
         }
@@ -560,6 +561,49 @@ k_impulses_from_rows(const long long* __restrict__ rows, const T* __restrict__ r
             atomicAdd(x + 0, idx.x); atomicAdd(x + 1, idx.y); atomicAdd(x + 2, idx.z);
             atomicAdd(cnt_out + tri * 3 + corner[pt], 1);
         }
+    }
+}
+
+// Element-wise evaluation of the solver's arithmetic building blocks, for tests that compare
+// them bit for bit with the CPU oracle and against CUDA's own elementary functions.
+// op 0 cbrt, 1 acos, 2 cos, 3 sin, 4 certified product (in: x0, x1, k, y; out: r0, r1),
+// 5 solve_cubic (in: a, b, c, d; out: three roots), 6 CUDA cbrt, 7 CUDA acos, 8 CUDA cos,
+// 9 CUDA sin.  in has 4 doubles per element, out 3.
+__global__ void k_debug_math(int op, const double* __restrict__ in, double* __restrict__ out, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double* a = in + 4 * i;
+    double* o = out + 3 * i;
+    o[0] = o[1] = o[2] = 0.0;
+    switch (op) {
+        case 0: o[0] = ccc_cbrt(a[0]); break;
+        case 1: o[0] = ccc_acos(a[0]); break;
+        case 2: o[0] = ccc_cos(a[0]); break;
+        case 3: o[0] = ccc_sin(a[0]); break;
+        case 4: {
+            ccc_dd d = ccc_certmul(a[0], a[1], (int)a[2], a[3]);
+            o[0] = d.hi;
+            o[1] = d.lo;
+            break;
+        }
+        case 5: solve_cubic<double>(a[0], a[1], a[2], a[3], o); break;
+        case 6: o[0] = cbrt(a[0]); break;
+        case 7: o[0] = acos(a[0]); break;
+        case 8: o[0] = cos(a[0]); break;
+        case 9: o[0] = sin(a[0]); break;
+        case 10: case 11: {
+            double A = a[0], Bc = a[1], Cc = a[2], Dc = a[3];
+            double f = ((3.0 * Cc / A) - ((Bc * Bc) / (A * A))) / 3.0;
+            double b3 = 2 * ccc_cube_hi(Bc);
+            ccc_dd a2dd = ccc_sq_dd(A);
+            double a3 = ccc_certmul(a2dd.hi, a2dd.lo, 2, A).hi;
+            double g = (b3 / a3 - (Bc * Cc * 9) / a2dd.hi + 27.0 * Dc / A) / 27.0;
+            double h = g * g / 4.0 + ccc_cube_hi(f) / 27.0;
+            if (op == 10) { o[0] = f; o[1] = g; o[2] = h; }
+            else { o[0] = b3; o[1] = a2dd.hi; o[2] = a3; }
+            break;
+        }
+        default: break;
     }
 }
 

@@ -133,6 +133,30 @@ def impulse_fold(seed: int = 0, n: int = 256, dtype=np.float64):
     return x0, x1, masses
 
 
+def jittered_fold(seed: int, nx: int = 8, ny: int = 8, noise: float = 0.02, drop: float = 0.05,
+                  dtype=np.float64, fold: bool = True):
+    """Small jittered grid folded over itself with a random displacement: (x0, x1, masses).
+
+    Each soup is (F, 3, 3) built from an indexed mesh, so neighbouring triangles share
+    vertices exactly (the reference detects shared vertices by coordinate equality).
+    masses (F, 3) are per-corner, uniform in [0.5, 2].
+    """
+    g = rng(seed)
+    v, f = grid(nx, ny)
+    v[:, 2] = g.normal(0, noise, v.shape[0])
+    if fold:
+        m = v[:, 0] > 0.5
+        v[m, 0] = 1.0 - v[m, 0]
+        v[m, 2] += 0.01
+    v1 = v.copy()
+    v1[:, 2] -= drop
+    v1 += g.normal(0, noise, v.shape)
+    x0 = soup(v, f).astype(dtype)
+    x1 = soup(v1, f).astype(dtype)
+    masses = g.uniform(0.5, 2.0, (x0.shape[0], 3)).astype(dtype)
+    return x0, x1, masses
+
+
 def grid_for_count(g, tris: int):
     """nx, ny with aspect U[0.5, 2] and 2 (nx-1)(ny-1) close to 'tris'."""
     aspect = g.uniform(0.5, 2.0)

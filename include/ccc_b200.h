@@ -59,6 +59,14 @@ int64_t ccc_kernel_launches(void);
 int ccc_timing_begin(void);
 int ccc_timing_end(int max_kernels, char* names, int name_len, float* total_ms, int32_t* count);
 
+/* Test hook (no counterpart in the reference): evaluates the continuous-collision solver's
+ * arithmetic element-wise on the device so tests can compare it with the CPU oracle.
+ * op: 0 cbrt, 1 acos, 2 cos, 3 sin (the library's own), 4 certified product
+ * (in x0, x1, k, y -> out r0, r1), 5 cubic solve (in a, b, c, d -> out three roots,
+ * -1 = none), 6..9 CUDA's cbrt, acos, cos, sin.  in: n x 4 doubles, out: n x 3 doubles
+ * (device pointers). */
+int ccc_debug_math(int op, const double* in, double* out, int64_t n, void* stream);
+
 /* Bytes of device scratch an operation needs for B meshes of F triangles with the given
  * per-triangle candidate capacity (ignored by CCC_OP_BVH). */
 int64_t ccc_workspace_size(int op, int64_t B, int64_t F, int64_t max_candidates_per_triangle);

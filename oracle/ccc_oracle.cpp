@@ -616,12 +616,9 @@ template <class T> static void solve_cubic(double a, double b, double c, double 
         double f = ((3.0 * c / a) - ((b * b) / (a * a))) / 3.0;
         // computeG
         double b3 = 2 * ccc_cube_hi(b);
-        double a2dd[2];
-        ccc_sq_dd(a, a2dd);
-        double a2 = a2dd[0];
-        double a3c[2];
-        ccc_certmul_r2(a2dd, 2, a, a3c);
-        double a3 = a3c[0];
+        ccc_dd a2dd = ccc_sq_dd(a);
+        double a2 = a2dd.hi;
+        double a3 = ccc_certmul(a2dd.hi, a2dd.lo, 2, a).hi;
         double p1 = b3 / a3;
         double p2 = (b * c * 9) / a2;
         double p3 = 27.0 * d / a;
@@ -1165,7 +1162,11 @@ ORC_API int orc_solve_cubic(double a, double b, double c, double d, double* root
 }
 ORC_API uint32_t orc_morton(double x, double y, double z) { return morton3d<double>(x, y, z); }
 ORC_API uint32_t orc_morton_f(float x, float y, float z) { return morton3d<float>(x, y, z); }
-ORC_API void orc_certmul(const double* x, int k, double y, double* r) { ccc_certmul_r2(x, k, y, r); }
+ORC_API void orc_certmul(const double* x, int k, double y, double* r) {
+    ccc_dd d = ccc_certmul(x[0], k > 1 ? x[1] : 0.0, k, y);
+    r[0] = d.hi;
+    r[1] = d.lo;
+}
 ORC_API double orc_cbrt(double x) { return ccc_cbrt(x); }
 ORC_API double orc_acos(double x) { return ccc_acos(x); }
 ORC_API double orc_cos(double x) { return ccc_cos(x); }

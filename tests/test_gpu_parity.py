@@ -55,10 +55,17 @@ def _assert_same_rows_times(got_rows, got_times, exp_rows, exp_times):
 
 
 def _impulse_close(a, b):
+    """dv / dx agreement: 1e-6 relative for float64.  Contacts are summed per corner with
+    atomics in any order, so in float32 the bound is float32 summation error: 1e-5
+    relative plus 1e-6 of the largest magnitude."""
+    single = np.asarray(b).dtype == np.float32
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     scale = np.abs(b).max(initial=0.0)
-    tol = IMPULSE_RTOL * np.abs(b) + 1e-12 * max(scale, 1e-30)
+    if single:
+        tol = 1e-5 * np.abs(b) + 1e-6 * max(scale, 1e-30)
+    else:
+        tol = IMPULSE_RTOL * np.abs(b) + 1e-12 * max(scale, 1e-30)
     bad = ~(np.abs(a - b) <= tol)
     both_nan = np.isnan(a) & np.isnan(b)
     bad &= ~both_nan
@@ -127,7 +134,10 @@ def test_find_collisions_batch_random(cuda, oracle, dtype):
     import cccollisions_b200 as C
     xs = np.stack([random_mesh_soup(s, nx=10, ny=10, dtype=dtype)[0] for s in (11, 12, 13)])
     bb, tr = C.bvh(_t(xs, cuda))
-    out = C.find_collisions(bb, tr, _t(xs, cuda), 0.005, 8).cpu().numpy()
+    F, mc = xs.shape[1], 32
+    for b in range(3):    # stay within the candidate capacity (the reference wraps around beyond it)
+        assert len(oracle.candidates(bb[b].cpu().numpy(), tr[b].cpu().numpy(), threshold=0.005)) <= F * mc
+    out = C.find_collisions(bb, tr, _t(xs, cuda), 0.005, mc).cpu().numpy()
     for b in range(3):
         n = _valid_prefix(out[b])
         exp = oracle.find_collisions(bb[b].cpu().numpy(), tr[b].cpu().numpy(), xs[b], threshold=0.005)
@@ -246,7 +256,8 @@ def test_compute_impulses_fold_full_size(cuda, oracle):
     x0, x1, m = W.impulse_fold()
     X0, X1, Mt = _t(x0, cuda), _t(x1, cuda), _t(m, cuda)
     bb, tr = C.bvh_motion(X0, X1)
-    dv, dx, cnt = C.compute_impulses(bb, tr, X0, X1, Mt)
+    # 21.3 candidates per triangle: the reference's default of 16 would wrap around
+    dv, dx, cnt = C.compute_impulses(bb, tr, X0, X1, Mt, 32, 16)
     edv, edx, ecnt, nc = oracle.impulses(bb[0].cpu().numpy(), tr[0].cpu().numpy(), x0[0], x1[0], m[0], nthreads=0)
     assert nc > 1000
     assert (cnt[0].cpu().numpy() == ecnt).all()
