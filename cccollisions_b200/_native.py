@@ -12,6 +12,7 @@ LIB_PATH = os.path.join(_HERE, "libccc_b200.so")
 
 # return codes / status bits (mirrors include/ccc_b200.h)
 CCC_OK = 0
+CCC_ERR_TOO_LARGE = 4
 CCC_ST_CAND_OVERFLOW = 1
 CCC_ST_OUT_OVERFLOW = 2
 CCC_ST_STACK_OVERFLOW = 4
@@ -39,6 +40,8 @@ SIGNATURES = {
     "ccc_find_mincol_cand": (_I, [_I, _P, _P, _P, _P, _I64, _I64, _I64, _P, _P, _I64, _P]),
     "ccc_find_proximity": (_I, [_I, _P, _P, _P, _I64, _I64, _D, _I64, _P, _P, _I64, _P]),
     "ccc_compute_impulses": (_I, [_I, _P, _P, _P, _P, _P, _P, _I64, _I64, _I64, _I64, _P, _P, _P, _P, _I64, _P]),
+    "ccc_static_scratch_bytes": (_I64, []),
+    "ccc_find_collisions_continuous_static": (_I, [_I, _P, _P, _P, _P, _P, _I64, _I64, _I64, _I64, _P, _P, _P]),
     "ccc_compute_impulses_from_collisions": (_I, [_I, _P, _P, _I64, _I64, _P, _P, _P, _I64, _P, _P, _P, _P, _I64,
                                                  _P]),
 }

@@ -7,6 +7,8 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <atomic>
+
 #include "../../include/ccc_b200.h"
 #include "ccc_kernels.cuh"
 
@@ -344,6 +346,7 @@ const char* ccc_error_string(int code) {
         case CCC_ERR_INVALID_ARG: return "invalid argument";
         case CCC_ERR_WORKSPACE: return "workspace too small";
         case CCC_ERR_CUDA: return "CUDA launch error";
+        case CCC_ERR_TOO_LARGE: return "problem larger than the fixed scratch of the no-allocation entry point";
         default: return "unknown error";
     }
 }
@@ -464,6 +467,50 @@ int ccc_compute_impulses_from_collisions(int dtype, const int64_t* collisions, c
                                               counter, ws, ws_bytes, s)
                       : from_rows_impl<double>(collisions, roots, B, N, triangles, triangles_next, masses, F, dv, dx,
                                                counter, ws, ws_bytes, s);
+}
+
+// ---------------------------------------------------------------------------------------
+// Continuous collisions without any caller-provided or library-allocated scratch.
+//
+// Some callers cannot allocate device memory at all: plugins running inside a host
+// framework that owns every byte of the GPU through its own pool, or real-time step loops
+// whose policy forbids allocations after start-up.  For them the scratch of
+// ccc_find_collisions_continuous lives in a fixed file-scope device array of
+// CCC_STATIC_SCRATCH_BYTES, which every GPU that loads this library holds until the
+// process exits.  The array's name is only a host-side stand-in in host code, so its
+// device address is looked up once per device with cudaGetSymbolAddress (on the first
+// call on that device, which should therefore come before any stream capture).  Every
+// call shares the array: calls whose work overlaps on the GPU (different streams or
+// threads without ordering) race on it.  Each call clears the parts that must start at
+// zero; the rest is fully rewritten before it is read.
+
+#define CCC_STATIC_SCRATCH_BYTES (64ll << 20)
+
+static __device__ __align__(256) unsigned char g_ccc_static_scratch[CCC_STATIC_SCRATCH_BYTES];
+static std::atomic<void*> g_ccc_static_addr[64];
+
+int64_t ccc_static_scratch_bytes(void) { return CCC_STATIC_SCRATCH_BYTES; }
+
+int ccc_find_collisions_continuous_static(int dtype, const void* bboxes, const int64_t* tree, const void* triangles,
+                                          const void* triangles_next, const uint8_t* mask, int64_t B, int64_t F,
+                                          int64_t maxc, int64_t maxcol, int64_t* out_rows, void* out_times,
+                                          void* stream) {
+    int rc = check_common(dtype, B, F);
+    if (rc) return rc;
+    if (maxc < 1 || maxcol < 1) return CCC_ERR_INVALID_ARG;
+    int64_t need = layout(B, F, maxc, true).end;
+    if (need > CCC_STATIC_SCRATCH_BYTES) return CCC_ERR_TOO_LARGE;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return CCC_ERR_CUDA;
+    void* base = g_ccc_static_addr[dev].load();
+    if (base == nullptr) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_ccc_static_scratch) != cudaSuccess || p == nullptr) return CCC_ERR_CUDA;
+        g_ccc_static_addr[dev].store(p);
+        base = p;
+    }
+    return ccc_find_collisions_continuous(dtype, bboxes, tree, triangles, triangles_next, mask, B, F, maxc, maxcol,
+                                          out_rows, out_times, base, CCC_STATIC_SCRATCH_BYTES, stream);
 }
 
 }  // extern "C"

@@ -32,6 +32,7 @@ extern "C" {
 #define CCC_ERR_INVALID_ARG 1
 #define CCC_ERR_WORKSPACE 2
 #define CCC_ERR_CUDA 3
+#define CCC_ERR_TOO_LARGE 4
 
 /* status word bits (device side, read with ccc_read_status) */
 #define CCC_ST_CAND_OVERFLOW 1   /* more candidate pairs than F * max_candidates_per_triangle */
@@ -130,6 +131,23 @@ int ccc_compute_impulses_from_collisions(int dtype, const int64_t* collisions, c
                                          int64_t N, const void* triangles, const void* triangles_next,
                                          const void* masses, int64_t F, void* dv, void* dx, int32_t* counter,
                                          void* ws, int64_t ws_bytes, void* stream);
+
+/* find_collisions_continuous without any scratch allocation — no counterpart in the
+ * reference.  For callers that cannot allocate device memory (a plugin inside a host
+ * framework that owns the GPU's memory through its own pool, or a real-time step loop that
+ * forbids allocations): the same computation and outputs as ccc_find_collisions_continuous,
+ * with its scratch in a fixed device array of ccc_static_scratch_bytes() bytes (64 MiB)
+ * that every GPU loading this library holds until exit.  Problems whose scratch
+ * (ccc_workspace_size(CCC_OP_CONTINUOUS, B, F, max_candidates_per_triangle)) exceeds it
+ * return CCC_ERR_TOO_LARGE before any device work.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress); make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race.  Outputs as for
+ * ccc_find_collisions_continuous (pre-filled with -1 by the caller). */
+int64_t ccc_static_scratch_bytes(void);
+int ccc_find_collisions_continuous_static(int dtype, const void* bboxes, const int64_t* tree, const void* triangles,
+                                          const void* triangles_next, const uint8_t* mask, int64_t B, int64_t F,
+                                          int64_t max_candidates_per_triangle, int64_t max_collisions_per_triangle,
+                                          int64_t* out_rows, void* out_times, void* stream);
 
 #ifdef __cplusplus
 }
