@@ -16,14 +16,6 @@
 
 #include "ccc_libm.h"
 
-CCC_HD double ccc_fma(double a, double b, double c) {
-#if defined(__CUDA_ARCH__)
-    return __fma_rn(a, b, c);
-#else
-    return fma(a, b, c);
-#endif
-}
-
 // Values are passed and returned by value (no pointers into locals), which keeps the
 // device code straightforward.
 struct ccc_dd {
@@ -40,7 +32,7 @@ CCC_HD ccc_dd ccc_fast_two_sum(double a, double b) {
 }
 
 // (x0 (+ x1 when k == 2)) * y rounded to a 2-term expansion: bins of 45 bits, 4 live bins.
-CCC_HD ccc_dd ccc_certmul(double x0, double x1, int k, double y) {
+CCC_HD_CALL ccc_dd ccc_certmul(double x0, double x1, int k, double y) {
     const int BIN = 45;
     double b0, b1, b2, b3, b4, b5;           // bins (6 slots, the last two spill targets)
     double s0, s1, s2, s3;                   // biases of the live bins

@@ -220,7 +220,56 @@ template <class T> __device__ __forceinline__ uint32_t ccd_subbox_mask(const MTr
     return m;
 }
 
+// The same table packed into constants, so a runtime type k selects points without
+// indexing local arrays: side(k, p) = bit 4k + p of CCD_SIDE_TABLE, corner(k, p) = the
+// 2-bit field 8 (k % 8) + 2p of CCD_CORNER_TABLE[k / 8].
+constexpr int ccd_side_of(int k, int p) { return k < 9 ? (p >= 2) : (k < 12 ? (p == 3) : (p >= 1)); }
+constexpr int ccd_corner_of(int k, int p) {
+    return k < 9 ? (p == 0 ? (k / 3 == 2 ? 1 : 0) : p == 1 ? (k / 3 == 0 ? 1 : 2)
+                    : p == 2 ? (k % 3 == 2 ? 1 : 0) : (k % 3 == 0 ? 1 : 2))
+         : k < 12 ? (p < 3 ? p : k - 9)
+                  : (p == 0 ? k - 12 : p - 1);
+}
+constexpr unsigned long long ccd_side_table() {
+    unsigned long long t = 0;
+    for (int k = 0; k < 15; ++k)
+        for (int p = 0; p < 4; ++p) t |= (unsigned long long)ccd_side_of(k, p) << (4 * k + p);
+    return t;
+}
+constexpr unsigned long long ccd_corner_table(int half) {
+    unsigned long long t = 0;
+    for (int k = 8 * half; k < 15 && k < 8 * half + 8; ++k)
+        for (int p = 0; p < 4; ++p) t |= (unsigned long long)ccd_corner_of(k, p) << (8 * (k - 8 * half) + 2 * p);
+    return t;
+}
+constexpr unsigned long long CCD_SIDE_TABLE = ccd_side_table();
+constexpr unsigned long long CCD_CORNER_TABLE0 = ccd_corner_table(0);
+constexpr unsigned long long CCD_CORNER_TABLE1 = ccd_corner_table(1);
+__device__ __forceinline__ int tet_side(int k, int p) { return (int)((CCD_SIDE_TABLE >> (4 * k + p)) & 1ull); }
+__device__ __forceinline__ int tet_corner(int k, int p) {
+    unsigned long long t = k < 8 ? CCD_CORNER_TABLE0 : CCD_CORNER_TABLE1;
+    return (int)((t >> (8 * (k & 7) + 2 * p)) & 3ull);
+}
+
 template <class T> struct MTet { V3<T> v[4], dv[4]; };
+
+// tetrahedron of sub-test k read straight from the two soups: the four points at t = 0 and
+// their displacements x1 - x0 (make_tetrahedron, collisions_continuous.cu:36-124)
+template <class T>
+__device__ __forceinline__ MTet<T> load_tet(const T* __restrict__ x0, const T* __restrict__ x1, long long gi,
+                                            long long gj, int k) {
+    MTet<T> t;
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        long long o = (tet_side(k, p) ? gj : gi) * 9 + tet_corner(k, p) * 3;
+        V3<T> a = mk<T>(__ldg(x0 + o), __ldg(x0 + o + 1), __ldg(x0 + o + 2));
+        V3<T> b = mk<T>(__ldg(x1 + o), __ldg(x1 + o + 1), __ldg(x1 + o + 2));
+        t.v[p] = a;
+        t.dv[p] = b - a;
+    }
+    return t;
+}
+
 template <class T> __device__ __forceinline__ MTet<T> make_tet(const MTri<T>& a, const MTri<T>& b, int k) {
     int side[4], corner[4];
     type_points(k, side, corner);
@@ -407,14 +456,16 @@ template <class T> __device__ __forceinline__ V3<T> vnormalize(V3<T> a) {
 
 template <class T> struct Contact { V3<T> n; T vn, m0, m1; };
 
-// compute_coeficients_and_directions and helpers (collisions_impulses.cu:162-543)
+// compute_coeficients_and_directions and helpers (collisions_impulses.cu:162-543).
+// q holds the masses of the four tetrahedron points.  For vertex-face types the points
+// are first put in (face 0, face 1, face 2, vertex) order with selects: types 9..11 are
+// already in that order, types 12..14 have the vertex first.
 template <class T> __device__ __forceinline__ Contact<T> contact(const MTet<T>& tet, int k, T root, const T q[4]) {
     Contact<T> ct;
-    V3<T> th[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) th[i] = at_time(tet, i, root);
     if (k < 9) {
-        V3<T> da = th[1] - th[0], db = th[3] - th[2], dc = th[2] - th[0];
+        V3<T> th0 = at_time(tet, 0, root), th1 = at_time(tet, 1, root), th2 = at_time(tet, 2, root),
+              th3 = at_time(tet, 3, root);
+        V3<T> da = th1 - th0, db = th3 - th2, dc = th2 - th0;
         T denom = norm2(cross(da, db));
         T s, t;
         if (fabs((double)denom) < 1e-15) { s = (T)0.5; t = (T)0.5; }
@@ -437,9 +488,14 @@ template <class T> __device__ __forceinline__ Contact<T> contact(const MTet<T>& 
         ct.m1 = q[2] * (1 - t) + q[3] * t;
         return ct;
     }
-    bool inv = k >= 12;
-    int f0 = inv ? 1 : 0, f1 = inv ? 2 : 1, f2 = inv ? 3 : 2, fv = inv ? 0 : 3;
-    V3<T> e1 = th[f0] - th[f1], e2 = th[f2] - th[f1], ep = th[fv] - th[f1];
+    const bool inv = k >= 12;
+    V3<T> F0 = inv ? tet.v[1] : tet.v[0], F1 = inv ? tet.v[2] : tet.v[1], F2 = inv ? tet.v[3] : tet.v[2],
+          FV = inv ? tet.v[0] : tet.v[3];
+    V3<T> D0 = inv ? tet.dv[1] : tet.dv[0], D1 = inv ? tet.dv[2] : tet.dv[1], D2 = inv ? tet.dv[3] : tet.dv[2],
+          DV = inv ? tet.dv[0] : tet.dv[3];
+    T q0 = inv ? q[1] : q[0], q1 = inv ? q[2] : q[1], q2 = inv ? q[3] : q[2], qv = inv ? q[0] : q[3];
+    V3<T> t0 = F0 + D0 * root, t1 = F1 + D1 * root, t2 = F2 + D2 * root, tv = FV + DV * root;
+    V3<T> e1 = t0 - t1, e2 = t2 - t1, ep = tv - t1;
     T d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2), d20 = dot(ep, e1), d21 = dot(ep, e2);
     T denom = d00 * d11 - d01 * d01;
     T u, w, vv;
@@ -449,24 +505,50 @@ template <class T> __device__ __forceinline__ Contact<T> contact(const MTet<T>& 
         w = (d00 * d21 - d01 * d20) / denom;
     }
     vv = 1 - u - w;
-    const V3<T>* v = tet.v;
-    const V3<T>* dv = tet.dv;
-    V3<T> pt = v[f0] * u + v[f1] * vv + v[f2] * w;
-    V3<T> dpt = dv[f0] * u + dv[f1] * vv + dv[f2] * w;
-    V3<T> c0 = v[f0] + dv[f0] * root, c1 = v[f1] + dv[f1] * root, c2 = v[f2] + dv[f2] * root;
+    V3<T> pt = F0 * u + F1 * vv + F2 * w;
+    V3<T> dpt = D0 * u + D1 * vv + D2 * w;
+    V3<T> c0 = F0 + D0 * root, c1 = F1 + D1 * root, c2 = F2 + D2 * root;
     V3<T> nd = vnormalize(cross(c1 - c0, c2 - c0));
-    if (dot(v[fv] - pt, nd) < 0) nd = nd * (T)-1;
-    ct.vn = dot(dv[fv] - dpt, nd);
+    if (dot(FV - pt, nd) < 0) nd = nd * (T)-1;
+    ct.vn = dot(DV - dpt, nd);
     if (inv) nd = nd * (T)-1;
     ct.n = nd;
-    if (inv) {
-        ct.m0 = q[0];
-        ct.m1 = q[1] * u + q[2] * vv + q[3] * w;
-    } else {
-        ct.m0 = q[0] * u + q[1] * vv + q[2] * w;
-        ct.m1 = q[3];
-    }
+    T mface = q0 * u + q1 * vv + q2 * w;
+    ct.m0 = inv ? qv : mface;
+    ct.m1 = inv ? mface : qv;
     return ct;
+}
+
+// extrapolate_impulses + extrapolate_impulses_dv (collisions_impulses.cu:609-1067): impulses of
+// one contact added to the per-corner dv / dx sums and counters (F, 3, 3) / (F, 3)
+template <class T>
+__device__ __forceinline__ void apply_impulse(const MTet<T>& tet, long long gi, long long gj, int k, T root,
+                                              const Contact<T>& ct, T* dv_out, T* dx_out, int* cnt_out) {
+    T offset;
+    if (fabs((double)ct.vn) < 1e-15) offset = (T)0.1;
+    else offset = (T)((2 * CCC_THICKNESS) / (double)(-ct.vn));
+    offset = (T)fmin(fmax((double)offset, 0.), 1.);
+    T msum = ct.m0 + ct.m1;
+    T mf0, mf1;
+    if (fabs((double)msum) < 1e-15) { mf0 = (T)0.5; mf1 = (T)0.5; }
+    else { mf0 = ct.m0 / msum; mf1 = 1 - mf0; }
+    T mag0 = ct.vn * mf1;
+    T mag1 = -ct.vn * mf0;
+    T ro = (T)fmax((double)(root - offset), 0.);
+#pragma unroll
+    for (int pt = 0; pt < 4; ++pt) {
+        T mag = (k < 9) ? (pt < 2 ? mag0 : mag1) : (k < 12 ? (pt < 3 ? mag0 : mag1) : (pt < 1 ? mag0 : mag1));
+        V3<T> imp = ct.n * mag;
+        V3<T> nv = tet.dv[pt] + imp;
+        V3<T> idx = (nv - tet.dv[pt]) * (1 - ro);
+        long long tri = tet_side(k, pt) ? gj : gi;
+        int corner = tet_corner(k, pt);
+        T* d = dv_out + tri * 9 + corner * 3;
+        atomicAdd(d + 0, imp.x); atomicAdd(d + 1, imp.y); atomicAdd(d + 2, imp.z);
+        T* x = dx_out + tri * 9 + corner * 3;
+        atomicAdd(x + 0, idx.x); atomicAdd(x + 1, idx.y); atomicAdd(x + 2, idx.z);
+        atomicAdd(cnt_out + tri * 3 + corner, 1);
+    }
 }
 
 // ------------------------------------------------------------------ proximity

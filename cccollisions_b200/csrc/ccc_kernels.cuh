@@ -399,23 +399,38 @@ k_static_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, cons
 
 enum CcdMode { CCD_ROWS = 0, CCD_IMPULSES = 1, CCD_MINCOL = 2 };
 
-// continuous narrow phase (collisions_continuous.cu:14-765, collisions_impulses.cu:24-1067)
+// Continuous narrow phase (collisions_continuous.cu:14-765, collisions_impulses.cu:24-1067),
+// warp-cooperative.  Each warp takes 32 candidate pairs: every lane runs the shared-vertex
+// test and the 15 swept sub-box tests of its pair, the surviving (pair, type) items are
+// staged in shared memory, and then all 32 lanes solve items in lockstep, each loading only
+// the four points its item needs.  A one-thread-per-pair loop leaves most lanes idle, since
+// pairs have 0 to 15 cubic solves each.
 template <class T, int MODE>
-__global__ void __launch_bounds__(NARROW_THREADS)
+__global__ void __launch_bounds__(NARROW_THREADS, 3)
 k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ x0,
              const T* __restrict__ x1, const int* __restrict__ moff, int M, long long* __restrict__ rows,
              T* __restrict__ times, int max_per_tri, int* __restrict__ mesh_counters, const T* __restrict__ masses,
              T* __restrict__ dv_out, T* __restrict__ dx_out, int* __restrict__ cnt_out) {
-    int n = min(hdr->cand_count, cand_cap);
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-        int2 pr = cand[c];
-        MTri<T> a = load_mtri(x0, x1, pr.x), b = load_mtri(x0, x1, pr.y);
-        if (share_vertex(a.v, b.v)) continue;
-        uint32_t bits = ccd_subbox_mask(a, b);
-        while (bits) {
-            int k = __ffs(bits) - 1;
-            bits &= bits - 1;
-            if (MODE == CCD_MINCOL) {
+    constexpr int WARPS = NARROW_THREADS / 32;
+    __shared__ unsigned short items[WARPS][32 * 15];
+    __shared__ int2 pairs[WARPS][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned FULL = 0xffffffffu;
+    const int n = min(*(volatile int*)&hdr->cand_count, cand_cap);
+    for (long long base = ((long long)blockIdx.x * WARPS + warp) * 32; base < n;
+         base += (long long)gridDim.x * WARPS * 32) {
+        long long c = base + lane;
+        uint32_t bits = 0;
+        int2 pr = make_int2(0, 0);
+        if (c < n) {
+            pr = cand[c];
+            MTri<T> a = load_mtri(x0, x1, pr.x), b = load_mtri(x0, x1, pr.y);
+            if (!share_vertex(a.v, b.v)) bits = ccd_subbox_mask(a, b);
+        }
+        if (MODE == CCD_MINCOL) {
+            while (bits) {
+                int k = __ffs(bits) - 1;
+                bits &= bits - 1;
                 int m = find_mesh(moff, M, pr.x, 0);
                 long long cap = (long long)(moff[m + 1] - moff[m]) * max_per_tri;
                 long long r = append_row(mesh_counters, m, cap, &hdr->status);
@@ -425,9 +440,31 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                     rows[o * 3 + 1] = pr.y - moff[m];
                     rows[o * 3 + 2] = k;
                 }
-                continue;
             }
-            MTet<T> tet = make_tet(a, b, k);
+            continue;
+        }
+        // stage the work items of the 32 pairs
+        int cnt = __popc(bits);
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int v = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(FULL, incl, 31);
+        int pos = incl - cnt;
+        while (bits) {
+            int k = __ffs(bits) - 1;
+            bits &= bits - 1;
+            items[warp][pos++] = (unsigned short)((lane << 4) | k);
+        }
+        pairs[warp][lane] = pr;
+        __syncwarp();
+        for (int it = lane; it < total; it += 32) {
+            int item = items[warp][it];
+            int k = item & 15;
+            int2 q = pairs[warp][item >> 4];
+            MTet<T> tet = load_tet(x0, x1, q.x, q.y, k);
             T cf[4];
             cubic_coeffs(tet, cf);
             T rr[3];
@@ -438,51 +475,27 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                 if (!(root >= 0 && root <= 1)) continue;
                 if (!ccd_filter(tet, k, root)) continue;
                 if (MODE == CCD_ROWS) {
-                    int m = find_mesh(moff, M, pr.x, 0);
+                    int m = find_mesh(moff, M, q.x, 0);
                     long long cap = (long long)(moff[m + 1] - moff[m]) * max_per_tri;
                     long long r = append_row(mesh_counters, m, cap, &hdr->status);
                     if (r >= 0) {
                         long long o = (long long)moff[m] * max_per_tri + r;
-                        rows[o * 3 + 0] = pr.x - moff[m];
-                        rows[o * 3 + 1] = pr.y - moff[m];
+                        rows[o * 3 + 0] = q.x - moff[m];
+                        rows[o * 3 + 1] = q.y - moff[m];
                         rows[o * 3 + 2] = k;
                         times[o] = root;
                     }
                 } else {
-                    int side[4], corner[4];
-                    type_points(k, side, corner);
-                    T q[4];
+                    T mq[4];
 #pragma unroll
-                    for (int pt = 0; pt < 4; ++pt) q[pt] = masses[(long long)(side[pt] ? pr.y : pr.x) * 3 + corner[pt]];
-                    Contact<T> ct = contact(tet, k, root, q);
-                    // extrapolate_impulses (936-1067) + extrapolate_impulses_dv (609-933)
-                    T offset;
-                    if (fabs((double)ct.vn) < 1e-15) offset = (T)0.1;
-                    else offset = (T)((2 * CCC_THICKNESS) / (double)(-ct.vn));
-                    offset = (T)fmin(fmax((double)offset, 0.), 1.);
-                    T msum = ct.m0 + ct.m1;
-                    T mf0, mf1;
-                    if (fabs((double)msum) < 1e-15) { mf0 = (T)0.5; mf1 = (T)0.5; }
-                    else { mf0 = ct.m0 / msum; mf1 = 1 - mf0; }
-                    T mag0 = ct.vn * mf1;
-                    T mag1 = -ct.vn * mf0;
-                    T ro = (T)fmax((double)(root - offset), 0.);
-#pragma unroll
-                    for (int pt = 0; pt < 4; ++pt) {
-                        T mag = (k < 9) ? (pt < 2 ? mag0 : mag1) : (k < 12 ? (pt < 3 ? mag0 : mag1) : (pt < 1 ? mag0 : mag1));
-                        V3<T> imp = ct.n * mag;
-                        V3<T> nv = tet.dv[pt] + imp;
-                        V3<T> idx = (nv - tet.dv[pt]) * (1 - ro);
-                        long long tri = side[pt] ? pr.y : pr.x;
-                        T* d = dv_out + tri * 9 + corner[pt] * 3;
-                        atomicAdd(d + 0, imp.x); atomicAdd(d + 1, imp.y); atomicAdd(d + 2, imp.z);
-                        T* x = dx_out + tri * 9 + corner[pt] * 3;
-                        atomicAdd(x + 0, idx.x); atomicAdd(x + 1, idx.y); atomicAdd(x + 2, idx.z);
-                        atomicAdd(cnt_out + tri * 3 + corner[pt], 1);
-                    }
+                    for (int pt = 0; pt < 4; ++pt)
+                        mq[pt] = masses[(long long)(tet_side(k, pt) ? q.y : q.x) * 3 + tet_corner(k, pt)];
+                    Contact<T> ct = contact(tet, k, root, mq);
+                    apply_impulse(tet, q.x, q.y, k, root, ct, dv_out, dx_out, cnt_out);
                 }
             }
         }
+        __syncwarp();
     }
 }
 
@@ -531,36 +544,11 @@ k_impulses_from_rows(const long long* __restrict__ rows, const T* __restrict__ r
         int k = (int)kk;
         long long gi = b * F + i, gj = b * F + j;
         T root = roots[r];
-        MTri<T> a = load_mtri(x0, x1, gi), bb = load_mtri(x0, x1, gj);
-        MTet<T> tet = make_tet(a, bb, k);
-        int side[4], corner[4];
-        type_points(k, side, corner);
-        T q[4];
-        for (int pt = 0; pt < 4; ++pt) q[pt] = masses[(side[pt] ? gj : gi) * 3 + corner[pt]];
-        Contact<T> ct = contact(tet, k, root, q);
-        T offset;
-        if (fabs((double)ct.vn) < 1e-15) offset = (T)0.1;
-        else offset = (T)((2 * CCC_THICKNESS) / (double)(-ct.vn));
-        offset = (T)fmin(fmax((double)offset, 0.), 1.);
-        T msum = ct.m0 + ct.m1;
-        T mf0, mf1;
-        if (fabs((double)msum) < 1e-15) { mf0 = (T)0.5; mf1 = (T)0.5; }
-        else { mf0 = ct.m0 / msum; mf1 = 1 - mf0; }
-        T mag0 = ct.vn * mf1;
-        T mag1 = -ct.vn * mf0;
-        T ro = (T)fmax((double)(root - offset), 0.);
-        for (int pt = 0; pt < 4; ++pt) {
-            T mag = (k < 9) ? (pt < 2 ? mag0 : mag1) : (k < 12 ? (pt < 3 ? mag0 : mag1) : (pt < 1 ? mag0 : mag1));
-            V3<T> imp = ct.n * mag;
-            V3<T> nv = tet.dv[pt] + imp;
-            V3<T> idx = (nv - tet.dv[pt]) * (1 - ro);
-            long long tri = side[pt] ? gj : gi;
-            T* d = dv_out + tri * 9 + corner[pt] * 3;
-            atomicAdd(d + 0, imp.x); atomicAdd(d + 1, imp.y); atomicAdd(d + 2, imp.z);
-            T* x = dx_out + tri * 9 + corner[pt] * 3;
-            atomicAdd(x + 0, idx.x); atomicAdd(x + 1, idx.y); atomicAdd(x + 2, idx.z);
-            atomicAdd(cnt_out + tri * 3 + corner[pt], 1);
-        }
+        MTet<T> tet = load_tet(x0, x1, gi, gj, k);
+        T mq[4];
+        for (int pt = 0; pt < 4; ++pt) mq[pt] = masses[(tet_side(k, pt) ? gj : gi) * 3 + tet_corner(k, pt)];
+        Contact<T> ct = contact(tet, k, root, mq);
+        apply_impulse(tet, gi, gj, k, root, ct, dv_out, dx_out, cnt_out);
     }
 }
 

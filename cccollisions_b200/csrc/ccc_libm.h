@@ -5,32 +5,48 @@
 // library and the host C library give different last-bit results for those calls, which
 // would make the GPU path and the CPU oracle disagree by an ulp on times of impact.  To
 // make the two bit-identical, both include this header and evaluate the functions with
-// the same sequence of IEEE-754 double operations (+, -, *, /, sqrt only; no fused
-// multiply-add: the device side is compiled with -fmad=false, the host side with
-// -ffp-contract=off).
+// the same sequence of IEEE-754 double operations (+, -, *, /, sqrt and explicit fused
+// multiply-adds through ccc_fma; nothing is contracted implicitly: the device side is
+// compiled with -fmad=false, the host side with -ffp-contract=off).
 //
 // Methods (all from elementary analysis, not from any vendor library):
-//   ccc_cbrt : exponent split a = m * 2^(3q+r), linear first guess on [1,2) scaled by
-//              2^(r/3), then five Newton steps y <- y - (y^3 - m')/(3 y^2).
-//              Measured error <= 1 ulp against a correctly rounded reference.
-//   ccc_sin / ccc_cos : Maclaurin series in Horner form, terms 1/(2n+1)! and 1/(2n)!
+//   ccc_cbrt : exponent split a = m * 2^(3q+r); the inverse cube root of m' = m 2^r from a
+//              chord on [1,2) scaled by 2^(-r/3), three division-free Newton steps
+//              r <- r + r (1 - m' r^3) / 3, then y = m' r^2 and one Newton step
+//              y <- y - (y^3 - m') / (3 y^2) with an fma residual.  Error <= 1 ulp.
+//   ccc_sin / ccc_cos : Maclaurin series in fma Horner form, terms 1/(2n+1)! and 1/(2n)!
 //              (exact rationals rounded once to double), valid and accurate for |x| <= 1.1,
 //              which covers the solver's only use, k/3 with k = acos(.) in [0, pi].  Larger
 //              arguments are halved and recombined with the double-angle identities.
 //   ccc_acos : acos(x) = pi/2 - asin(x) for |x| < 1/2, 2 asin(sqrt((1-x)/2)) for x >= 1/2,
 //              pi - 2 asin(sqrt((1+x)/2)) for x <= -1/2; asin on [0, 1/2] by its Maclaurin
-//              series sum (2n)!/(4^n (n!)^2 (2n+1)) x^(2n+1), 30 terms.
+//              series sum (2n)!/(4^n (n!)^2 (2n+1)) x^(2n+1), 30 terms, evaluated as even and
+//              odd halves in x^4 (two independent fma chains).
 #pragma once
 
 #include <stdint.h>
 
 #if defined(__CUDACC__)
 #define CCC_HD __host__ __device__ __forceinline__
+// larger helpers are kept out of line on the device: the solver calls each several times
+// and warps in different branches would otherwise thrash the instruction cache
+#define CCC_HD_CALL __host__ __device__ __noinline__
 #else
 #define CCC_HD static inline
+#define CCC_HD_CALL static
 #include <math.h>
 #include <string.h>
 #endif
+
+// correctly rounded fused multiply-add on both sides (the solver's own arithmetic never
+// contracts; these helpers use fma explicitly, identically on host and device)
+CCC_HD double ccc_fma(double a, double b, double c) {
+#if defined(__CUDA_ARCH__)
+    return __fma_rn(a, b, c);
+#else
+    return fma(a, b, c);
+#endif
+}
 
 CCC_HD uint64_t ccc_dbits(double x) {
 #if defined(__CUDA_ARCH__)
@@ -100,7 +116,7 @@ CCC_HD int ccc_frexp_exp(double x) {
     return be - 1022;
 }
 
-CCC_HD double ccc_cbrt(double x) {
+CCC_HD_CALL double ccc_cbrt(double x) {
     if (x == 0.0 || x != x) return x + x;          // +-0 kept, NaN propagated
     uint64_t u = ccc_dbits(x);
     uint64_t sign = u & 0x8000000000000000ull;
@@ -119,14 +135,20 @@ CCC_HD double ccc_cbrt(double x) {
     int r = e - 3 * q;                                    // 0, 1, 2
     double mr = m;
     double scale = 1.0;
-    if (r == 1) { mr = m * 2.0; scale = 0x1.428a2f98d728bp+0; }   // 2^(1/3)
-    if (r == 2) { mr = m * 4.0; scale = 0x1.965fea53d6e3dp+0; }   // 2^(2/3)
-    // cbrt(m) on [1,2): chord 1 + 0.26 (m - 1), within 1.5 %
-    double y = (1.0 + 0.26 * (m - 1.0)) * scale;
-    for (int it = 0; it < 5; ++it) {
-        double t = y * y;
-        y = y - (t * y - mr) / (3.0 * t);
+    if (r == 1) { mr = m * 2.0; scale = 0x1.965fea53d6e3dp-1; }   // 2^(-1/3)
+    if (r == 2) { mr = m * 4.0; scale = 0x1.428a2f98d728bp-1; }   // 2^(-2/3)
+    // m^(-1/3) on [1,2): chord through the end points, within 2.7 %
+    double ri = ccc_fma(-0x1.a68056b0a470cp-3, m - 1.0, 1.0) * scale;
+    const double third = 0x1.5555555555555p-2;
+    for (int it = 0; it < 3; ++it) {
+        double r3 = ri * ri * ri;
+        double err = ccc_fma(-mr, r3, 1.0);
+        ri = ccc_fma(ri * err, third, ri);
     }
+    double y = (mr * ri) * ri;
+    double t = y * y;
+    double res = ccc_fma(t, y, -mr);
+    y = y - res / (3.0 * t);
     y = ccc_ldexp(y, q);
     return sign ? -y : y;
 }
@@ -139,39 +161,39 @@ CCC_HD float ccc_cbrtf(float x) {
 
 CCC_HD double ccc_sin_series(double x) {
     double z = x * x;
-    double p = 0x1.3f3ccdd165fa9p-84;            //  1/25!
-    p = p * z + -0x1.761b41316381ap-75;          // -1/23!
-    p = p * z + 0x1.71b8ef6dcf572p-66;           //  1/21!
-    p = p * z + -0x1.2f49b46814157p-57;          // -1/19!
-    p = p * z + 0x1.952c77030ad4ap-49;           //  1/17!
-    p = p * z + -0x1.ae7f3e733b81fp-41;          // -1/15!
-    p = p * z + 0x1.6124613a86d09p-33;           //  1/13!
-    p = p * z + -0x1.ae64567f544e4p-26;          // -1/11!
-    p = p * z + 0x1.71de3a556c734p-19;           //  1/9!
-    p = p * z + -0x1.a01a01a01a01ap-13;          // -1/7!
-    p = p * z + 0x1.1111111111111p-7;            //  1/5!
-    p = p * z + -0x1.5555555555555p-3;           // -1/3!
-    return x + x * (z * p);
+    double p = 0x1.3f3ccdd165fa9p-84;                     //  1/25!
+    p = ccc_fma(p, z, -0x1.761b41316381ap-75);            // -1/23!
+    p = ccc_fma(p, z, 0x1.71b8ef6dcf572p-66);             //  1/21!
+    p = ccc_fma(p, z, -0x1.2f49b46814157p-57);            // -1/19!
+    p = ccc_fma(p, z, 0x1.952c77030ad4ap-49);             //  1/17!
+    p = ccc_fma(p, z, -0x1.ae7f3e733b81fp-41);            // -1/15!
+    p = ccc_fma(p, z, 0x1.6124613a86d09p-33);             //  1/13!
+    p = ccc_fma(p, z, -0x1.ae64567f544e4p-26);            // -1/11!
+    p = ccc_fma(p, z, 0x1.71de3a556c734p-19);             //  1/9!
+    p = ccc_fma(p, z, -0x1.a01a01a01a01ap-13);            // -1/7!
+    p = ccc_fma(p, z, 0x1.1111111111111p-7);              //  1/5!
+    p = ccc_fma(p, z, -0x1.5555555555555p-3);             // -1/3!
+    return ccc_fma(x * z, p, x);
 }
 
 CCC_HD double ccc_cos_series(double x) {
     double z = x * x;
-    double p = 0x1.f2cf01972f578p-80;            //  1/24!
-    p = p * z + -0x1.0ce396db7f853p-70;          // -1/22!
-    p = p * z + 0x1.e542ba4020225p-62;           //  1/20!
-    p = p * z + -0x1.6827863b97d97p-53;          // -1/18!
-    p = p * z + 0x1.ae7f3e733b81fp-45;           //  1/16!
-    p = p * z + -0x1.93974a8c07c9dp-37;          // -1/14!
-    p = p * z + 0x1.1eed8eff8d898p-29;           //  1/12!
-    p = p * z + -0x1.27e4fb7789f5cp-22;          // -1/10!
-    p = p * z + 0x1.a01a01a01a01ap-16;           //  1/8!
-    p = p * z + -0x1.6c16c16c16c17p-10;          // -1/6!
-    p = p * z + 0x1.5555555555555p-5;            //  1/4!
-    p = p * z + -0x1.0000000000000p-1;           // -1/2!
-    return 1.0 + z * p;
+    double p = 0x1.f2cf01972f578p-80;                     //  1/24!
+    p = ccc_fma(p, z, -0x1.0ce396db7f853p-70);            // -1/22!
+    p = ccc_fma(p, z, 0x1.e542ba4020225p-62);             //  1/20!
+    p = ccc_fma(p, z, -0x1.6827863b97d97p-53);            // -1/18!
+    p = ccc_fma(p, z, 0x1.ae7f3e733b81fp-45);             //  1/16!
+    p = ccc_fma(p, z, -0x1.93974a8c07c9dp-37);            // -1/14!
+    p = ccc_fma(p, z, 0x1.1eed8eff8d898p-29);             //  1/12!
+    p = ccc_fma(p, z, -0x1.27e4fb7789f5cp-22);            // -1/10!
+    p = ccc_fma(p, z, 0x1.a01a01a01a01ap-16);             //  1/8!
+    p = ccc_fma(p, z, -0x1.6c16c16c16c17p-10);            // -1/6!
+    p = ccc_fma(p, z, 0x1.5555555555555p-5);              //  1/4!
+    p = ccc_fma(p, z, -0x1.0000000000000p-1);             // -1/2!
+    return ccc_fma(z, p, 1.0);
 }
 
-CCC_HD double ccc_sin(double x) {
+CCC_HD_CALL double ccc_sin(double x) {
     if (x != x) return x + x;
     double ax = x < 0 ? -x : x;
     if (ax <= 1.1) return ccc_sin_series(x);
@@ -189,7 +211,7 @@ CCC_HD double ccc_sin(double x) {
     return s;
 }
 
-CCC_HD double ccc_cos(double x) {
+CCC_HD_CALL double ccc_cos(double x) {
     if (x != x) return x + x;
     double ax = x < 0 ? -x : x;
     if (ax <= 1.1) return ccc_cos_series(x);
@@ -206,42 +228,45 @@ CCC_HD double ccc_cos(double x) {
     return c;
 }
 
-// asin on [0, 1/2] (also exact-sign for negative arguments of the same size)
+// asin on [0, 1/2]: x + x z P(z), z = x^2, with P(z) = E(w) + z O(w), w = z^2 (the even and
+// odd coefficient halves run as two independent fma chains)
 CCC_HD double ccc_asin_small(double x) {
     double z = x * x;
-    double p = 0x1.cf7dea5b6e830p-10;            // n = 29
-    p = p * z + 0x1.e82be60d9127ep-10;
-    p = p * z + 0x1.018f963c229bfp-9;
-    p = p * z + 0x1.1052bc5fa960ap-9;
-    p = p * z + 0x1.208d3570ae5a6p-9;
-    p = p * z + 0x1.3275586c5f2f0p-9;
-    p = p * z + 0x1.464c0950f7d47p-9;
-    p = p * z + 0x1.5c5f56efaaaabp-9;
-    p = p * z + 0x1.750de64d7d05fp-9;
-    p = p * z + 0x1.90cb77f60c7cep-9;
-    p = p * z + 0x1.b026f57b13b14p-9;
-    p = p * z + 0x1.d3d2a8e0dd67dp-9;
-    p = p * z + 0x1.fcaf8fb6db6dbp-9;
-    p = p * z + 0x1.15ee9d45d1746p-8;
-    p = p * z + 0x1.31683bdef7bdfp-8;
-    p = p * z + 0x1.51ba308d3dcb1p-8;
-    p = p * z + 0x1.782dda12f684cp-8;
-    p = p * z + 0x1.a6863d70a3d71p-8;
-    p = p * z + 0x1.df3bd37a6f4dfp-8;
-    p = p * z + 0x1.12ef3cf3cf3cfp-7;
-    p = p * z + 0x1.3fde50d79435ep-7;
-    p = p * z + 0x1.7a87878787878p-7;
-    p = p * z + 0x1.c99999999999ap-7;
-    p = p * z + 0x1.1c4ec4ec4ec4fp-6;
-    p = p * z + 0x1.6e8ba2e8ba2e9p-6;
-    p = p * z + 0x1.f1c71c71c71c7p-6;
-    p = p * z + 0x1.6db6db6db6db7p-5;
-    p = p * z + 0x1.3333333333333p-4;
-    p = p * z + 0x1.5555555555555p-3;            // n = 1
-    return x + x * (z * p);
+    double w = z * z;
+    double pe = 0x1.cf7dea5b6e830p-10;
+    pe = ccc_fma(pe, w, 0x1.018f963c229bfp-9);
+    pe = ccc_fma(pe, w, 0x1.208d3570ae5a6p-9);
+    pe = ccc_fma(pe, w, 0x1.464c0950f7d47p-9);
+    pe = ccc_fma(pe, w, 0x1.750de64d7d05fp-9);
+    pe = ccc_fma(pe, w, 0x1.b026f57b13b14p-9);
+    pe = ccc_fma(pe, w, 0x1.fcaf8fb6db6dbp-9);
+    pe = ccc_fma(pe, w, 0x1.31683bdef7bdfp-8);
+    pe = ccc_fma(pe, w, 0x1.782dda12f684cp-8);
+    pe = ccc_fma(pe, w, 0x1.df3bd37a6f4dfp-8);
+    pe = ccc_fma(pe, w, 0x1.3fde50d79435ep-7);
+    pe = ccc_fma(pe, w, 0x1.c99999999999ap-7);
+    pe = ccc_fma(pe, w, 0x1.6e8ba2e8ba2e9p-6);
+    pe = ccc_fma(pe, w, 0x1.6db6db6db6db7p-5);
+    pe = ccc_fma(pe, w, 0x1.5555555555555p-3);
+    double po = 0x1.e82be60d9127ep-10;
+    po = ccc_fma(po, w, 0x1.1052bc5fa960ap-9);
+    po = ccc_fma(po, w, 0x1.3275586c5f2f0p-9);
+    po = ccc_fma(po, w, 0x1.5c5f56efaaaabp-9);
+    po = ccc_fma(po, w, 0x1.90cb77f60c7cep-9);
+    po = ccc_fma(po, w, 0x1.d3d2a8e0dd67dp-9);
+    po = ccc_fma(po, w, 0x1.15ee9d45d1746p-8);
+    po = ccc_fma(po, w, 0x1.51ba308d3dcb1p-8);
+    po = ccc_fma(po, w, 0x1.a6863d70a3d71p-8);
+    po = ccc_fma(po, w, 0x1.12ef3cf3cf3cfp-7);
+    po = ccc_fma(po, w, 0x1.7a87878787878p-7);
+    po = ccc_fma(po, w, 0x1.1c4ec4ec4ec4fp-6);
+    po = ccc_fma(po, w, 0x1.f1c71c71c71c7p-6);
+    po = ccc_fma(po, w, 0x1.3333333333333p-4);
+    double p = ccc_fma(z, po, pe);
+    return ccc_fma(x * z, p, x);
 }
 
-CCC_HD double ccc_acos(double x) {
+CCC_HD_CALL double ccc_acos(double x) {
     const double PI = 0x1.921fb54442d18p+1;
     const double PI_2 = 0x1.921fb54442d18p+0;
     if (x != x) return x + x;

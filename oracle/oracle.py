@@ -35,6 +35,13 @@ def build(force: bool = False) -> str:
     os.makedirs(os.path.dirname(_LIB_PATH), exist_ok=True)
     cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC",
            "-shared", "-o", _LIB_PATH, _SRC]
+    # explicit fma() calls become single instructions where the CPU has FMA (results are
+    # identical either way: fma is correctly rounded in hardware and in libm)
+    try:
+        if " fma " in open("/proc/cpuinfo").read().replace("\n", " "):
+            cmd.insert(1, "-mfma")
+    except OSError:
+        pass
     subprocess.check_call(cmd)
     return _LIB_PATH
 
