@@ -13,6 +13,8 @@ LIB_PATH = os.path.join(_HERE, "libccc_b200.so")
 # return codes / status bits (mirrors include/ccc_b200.h)
 CCC_OK = 0
 CCC_ERR_TOO_LARGE = 4
+LIB_REFERENCE = 0
+LIB_PORTABLE = 1
 CCC_ST_CAND_OVERFLOW = 1
 CCC_ST_OUT_OVERFLOW = 2
 CCC_ST_STACK_OVERFLOW = 4
@@ -30,6 +32,9 @@ SIGNATURES = {
     "ccc_error_string": (ctypes.c_char_p, [_I]),
     "ccc_kernel_launches": (_I64, []),
     "ccc_debug_math": (_I, [_I, _P, _P, _I64, _P]),
+    "ccc_debug_stage": (_I, [_I, _I, _P, _I, _P, _I, _I64, _P]),
+    "ccc_set_math_library": (_I, [_I]),
+    "ccc_get_math_library": (_I, []),
     "ccc_timing_begin": (_I, []),
     "ccc_timing_end": (_I, [_I, _P, _I, _P, _P]),
     "ccc_workspace_size": (_I64, [_I, _I64, _I64, _I64]),
@@ -97,3 +102,21 @@ def timing_end(max_kernels: int = 64):
         nm = names.raw[i * name_len:(i + 1) * name_len].split(b"\0", 1)[0].decode()
         out[nm] = (float(ms[i]), int(cnt[i]))
     return out
+
+
+class math_library:
+    """Context manager selecting the solver's elementary functions (LIB_REFERENCE: CUDA's,
+    as the reference; LIB_PORTABLE: the library's own, shared bit for bit with the oracle)."""
+
+    def __init__(self, lib_id: int):
+        self.lib_id = lib_id
+        self.prev = None
+
+    def __enter__(self):
+        self.prev = lib().ccc_get_math_library()
+        check(lib().ccc_set_math_library(self.lib_id), "ccc_set_math_library")
+        return self
+
+    def __exit__(self, *exc):
+        lib().ccc_set_math_library(self.prev)
+        return False

@@ -36,6 +36,9 @@ inline int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 // Every kernel launch goes through CCC_LAUNCH, which counts it and, while timing is on,
 // brackets it with CUDA events on the launching stream.
 int64_t g_launches = 0;
+// elementary functions of the continuous-collision solver (MathLib); CUDA's own by default,
+// which is what the reference calls
+int g_math_lib = LIB_REFERENCE;
 bool g_timing = false;
 constexpr int MAX_TIMED = 8192;
 struct Timed { const char* name; cudaEvent_t a, b; };
@@ -226,7 +229,7 @@ int ccd_impl(const void* bboxes, const int64_t* tree, const void* x0, const void
     if (rc) return rc;
     CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_ROWS><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
         P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.moff, (int)B, (long long*)rows, (T*)times,
-        (int)maxcol, P.mesh_cnt, nullptr, nullptr, nullptr, nullptr));
+        (int)maxcol, P.mesh_cnt, nullptr, nullptr, nullptr, nullptr, g_math_lib));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -241,7 +244,7 @@ int mincol_impl(const void* bboxes, const int64_t* tree, const void* x0, const v
     if (rc) return rc;
     CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_MINCOL><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
         P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.moff, (int)B, (long long*)rows, nullptr,
-        (int)(maxc * 15), P.mesh_cnt, nullptr, nullptr, nullptr, nullptr));
+        (int)(maxc * 15), P.mesh_cnt, nullptr, nullptr, nullptr, nullptr, g_math_lib));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -272,7 +275,7 @@ int impulses_impl(const void* bboxes, const int64_t* tree, const void* x0, const
     if (rc) return rc;
     CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_IMPULSES><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
         P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.moff, (int)B, nullptr, nullptr, 0, P.mesh_cnt,
-        (const T*)masses, (T*)dv, (T*)dx, (int*)cnt));
+        (const T*)masses, (T*)dv, (T*)dx, (int*)cnt, g_math_lib));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -288,7 +291,7 @@ int from_rows_impl(const int64_t* rows, const void* roots, int64_t B, int64_t N,
     int g = (int)std::min<int64_t>(grid_for(B * N, NARROW_THREADS), (int64_t)narrow_grid());
     CCC_LAUNCH("k_impulses_from_rows", s, k_impulses_from_rows<T><<<g, NARROW_THREADS, 0, s>>>((const long long*)rows, (const T*)roots, (int)B, N, (int)F,
                                                          (const T*)x0, (const T*)x1, (const T*)masses, (T*)dv, (T*)dx,
-                                                         (int*)cnt, P.hdr));
+                                                         (int*)cnt, P.hdr, g_math_lib));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -300,6 +303,28 @@ extern "C" {
 int ccc_version(void) { return 1; }
 
 int64_t ccc_kernel_launches(void) { return g_launches; }
+
+int ccc_set_math_library(int lib) {
+    if (lib != LIB_REFERENCE && lib != LIB_PORTABLE) return CCC_ERR_INVALID_ARG;
+    g_math_lib = lib;
+    return CCC_OK;
+}
+
+int ccc_get_math_library(void) { return g_math_lib; }
+
+int ccc_debug_stage(int op, int lib, const double* in, int in_stride, double* out, int out_stride, int64_t n,
+                    void* stream) {
+    if (op < 0 || op > 5 || (lib != LIB_REFERENCE && lib != LIB_PORTABLE) || n < 0 || n >= ((int64_t)1 << 31))
+        return CCC_ERR_INVALID_ARG;
+    const int need_in[6] = {24, 4, 26, 30, 4, 1}, need_out[6] = {4, 3, 1, 6, 3, 3};
+    if (in_stride < need_in[op] || out_stride < need_out[op]) return CCC_ERR_INVALID_ARG;
+    if (n == 0) return CCC_OK;
+    if (!in || !out) return CCC_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    CCC_LAUNCH("k_debug_stage", s, k_debug_stage<<<grid_for(n, 128), 128, 0, s>>>(op, lib, in, in_stride, out, out_stride, (int)n));
+    CCC_LAUNCH_CHECK();
+    return CCC_OK;
+}
 
 int ccc_debug_math(int op, const double* in, double* out, int64_t n, void* stream) {
     if (op < 0 || op > 11 || n < 0 || (n > 0 && (!in || !out)) || n >= ((int64_t)1 << 31)) return CCC_ERR_INVALID_ARG;

@@ -2,8 +2,11 @@
 //
 // Every expression keeps the reference's evaluation order (Dolorousrtur/CCCollisions
 // src/figures.cu, src/aabb.cu, src/collisions_continuous.cu, src/collisions_impulses.cu,
-// src/proximity_static.cu).  The library is compiled with -fmad=false so no multiply-add
-// is contracted: results are the plain IEEE-754 float/double results of those expressions.
+// src/proximity_static.cu).  The reference is compiled with nvcc's default multiply-add
+// contraction; this library is compiled with -fmad=false and writes the same fusions out
+// explicitly (fmaT): a*b + c -> fma(a, b, c), c + a*b -> fma(a, b, c), a*b +- c*d fuses
+// the first product, dot / cross / norm2 are fixed fma chains.  Every other operation is
+// a single IEEE-754 rounding, so the CPU oracle (same model with std::fma) matches.
 #pragma once
 
 #include <stdint.h>
@@ -18,11 +21,31 @@ template <class T> __device__ __forceinline__ V3<T> mk(T x, T y, T z) { V3<T> r;
 template <class T> __device__ __forceinline__ V3<T> operator+(V3<T> a, V3<T> b) { return mk<T>(a.x + b.x, a.y + b.y, a.z + b.z); }
 template <class T> __device__ __forceinline__ V3<T> operator-(V3<T> a, V3<T> b) { return mk<T>(a.x - b.x, a.y - b.y, a.z - b.z); }
 template <class T> __device__ __forceinline__ V3<T> operator*(V3<T> a, T s) { return mk<T>(a.x * s, a.y * s, a.z * s); }
-template <class T> __device__ __forceinline__ T dot(V3<T> a, V3<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float fmaT(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmaT(double a, double b, double c) { return __fma_rn(a, b, c); }
+// a.x*b.x + a.y*b.y + a.z*b.z  ->  fma(a.z, b.z, fma(a.x, b.x, a.y*b.y))
+template <class T> __device__ __forceinline__ T dot(V3<T> a, V3<T> b) { return fmaT(a.z, b.z, fmaT(a.x, b.x, a.y * b.y)); }
+// a.y*b.z - a.z*b.y  ->  fma(a.y, b.z, -(a.z*b.y)), and cyclically
 template <class T> __device__ __forceinline__ V3<T> cross(V3<T> a, V3<T> b) {
-    return mk<T>(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+    return mk<T>(fmaT(a.y, b.z, -(a.z * b.y)), fmaT(a.z, b.x, -(a.x * b.z)), fmaT(a.x, b.y, -(a.y * b.x)));
 }
-template <class T> __device__ __forceinline__ T norm2(V3<T> a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
+template <class T> __device__ __forceinline__ T norm2(V3<T> a) { return fmaT(a.z, a.z, fmaT(a.x, a.x, a.y * a.y)); }
+// v + d * t  ->  fma(d, t, v) per component
+template <class T> __device__ __forceinline__ V3<T> axpy(V3<T> v, V3<T> d, T t) {
+    return mk<T>(fmaT(d.x, t, v.x), fmaT(d.y, t, v.y), fmaT(d.z, t, v.z));
+}
+// a*u + b*v + c*w  ->  fma(c, w, fma(a, u, b*v)) per component
+template <class T> __device__ __forceinline__ V3<T> lin3(V3<T> a, T u, V3<T> b, T v, V3<T> c, T w) {
+    return mk<T>(fmaT(c.x, w, fmaT(a.x, u, b.x * v)), fmaT(c.y, w, fmaT(a.y, u, b.y * v)),
+                 fmaT(c.z, w, fmaT(a.z, u, b.z * v)));
+}
+// a*b - c*d  ->  fma(a, b, -(c*d))
+template <class T> __device__ __forceinline__ T fms2(T a, T b, T c, T d) { return fmaT(a, b, -(c * d)); }
+
+// Elementary functions of the cubic solver and of normalize(): CUDA's own (the reference's
+// calls: cbrt, cbrtf, acos, cos, sin, pow(x, 2), rsqrt) or this library's portable ones,
+// which the CPU oracle shares bit for bit.
+enum MathLib { LIB_REFERENCE = 0, LIB_PORTABLE = 1 };
 __device__ __forceinline__ float fmn(float a, float b) { return fminf(a, b); }
 __device__ __forceinline__ float fmx(float a, float b) { return fmaxf(a, b); }
 __device__ __forceinline__ double fmn(double a, double b) { return fmin(a, b); }
@@ -288,57 +311,57 @@ template <class T> __device__ __forceinline__ void cubic_coeffs(const MTet<T>& t
     V3<T> v0 = t.v[0] - t.v[3], v1 = t.v[1] - t.v[3], v2 = t.v[2] - t.v[3];
     V3<T> dv0 = t.dv[0] - t.dv[3], dv1 = t.dv[1] - t.dv[3], dv2 = t.dv[2] - t.dv[3];
     T k3 = 0;
-    k3 += dv2.z * dv1.y * dv0.x;
-    k3 += -dv1.z * dv2.y * dv0.x;
-    k3 += -dv2.z * dv0.y * dv1.x;
-    k3 += dv0.z * dv2.y * dv1.x;
-    k3 += dv1.z * dv0.y * dv2.x;
-    k3 += -dv0.z * dv1.y * dv2.x;
+    k3 = fmaT(dv2.z * dv1.y, dv0.x, k3);
+    k3 = fmaT(-dv1.z * dv2.y, dv0.x, k3);
+    k3 = fmaT(-dv2.z * dv0.y, dv1.x, k3);
+    k3 = fmaT(dv0.z * dv2.y, dv1.x, k3);
+    k3 = fmaT(dv1.z * dv0.y, dv2.x, k3);
+    k3 = fmaT(-dv0.z * dv1.y, dv2.x, k3);
     T k2 = 0;
-    k2 += v2.z * dv1.y * dv0.x;
-    k2 += dv2.z * v1.y * dv0.x;
-    k2 += dv2.z * dv1.y * v0.x;
-    k2 += -v1.z * dv2.y * dv0.x;
-    k2 += -dv1.z * v2.y * dv0.x;
-    k2 += -dv1.z * dv2.y * v0.x;
-    k2 += -v2.z * dv0.y * dv1.x;
-    k2 += -dv2.z * v0.y * dv1.x;
-    k2 += -dv2.z * dv0.y * v1.x;
-    k2 += v0.z * dv2.y * dv1.x;
-    k2 += dv0.z * v2.y * dv1.x;
-    k2 += dv0.z * dv2.y * v1.x;
-    k2 += v1.z * dv0.y * dv2.x;
-    k2 += dv1.z * v0.y * dv2.x;
-    k2 += dv1.z * dv0.y * v2.x;
-    k2 += -v0.z * dv1.y * dv2.x;
-    k2 += -dv0.z * v1.y * dv2.x;
-    k2 += -dv0.z * dv1.y * v2.x;
+    k2 = fmaT(v2.z * dv1.y, dv0.x, k2);
+    k2 = fmaT(dv2.z * v1.y, dv0.x, k2);
+    k2 = fmaT(dv2.z * dv1.y, v0.x, k2);
+    k2 = fmaT(-v1.z * dv2.y, dv0.x, k2);
+    k2 = fmaT(-dv1.z * v2.y, dv0.x, k2);
+    k2 = fmaT(-dv1.z * dv2.y, v0.x, k2);
+    k2 = fmaT(-v2.z * dv0.y, dv1.x, k2);
+    k2 = fmaT(-dv2.z * v0.y, dv1.x, k2);
+    k2 = fmaT(-dv2.z * dv0.y, v1.x, k2);
+    k2 = fmaT(v0.z * dv2.y, dv1.x, k2);
+    k2 = fmaT(dv0.z * v2.y, dv1.x, k2);
+    k2 = fmaT(dv0.z * dv2.y, v1.x, k2);
+    k2 = fmaT(v1.z * dv0.y, dv2.x, k2);
+    k2 = fmaT(dv1.z * v0.y, dv2.x, k2);
+    k2 = fmaT(dv1.z * dv0.y, v2.x, k2);
+    k2 = fmaT(-v0.z * dv1.y, dv2.x, k2);
+    k2 = fmaT(-dv0.z * v1.y, dv2.x, k2);
+    k2 = fmaT(-dv0.z * dv1.y, v2.x, k2);
     T k1 = 0;
-    k1 += v2.z * v1.y * dv0.x;
-    k1 += v2.z * dv1.y * v0.x;
-    k1 += dv2.z * v1.y * v0.x;
-    k1 += -v1.z * v2.y * dv0.x;
-    k1 += -v1.z * dv2.y * v0.x;
-    k1 += -dv1.z * v2.y * v0.x;
-    k1 += -v2.z * v0.y * dv1.x;
-    k1 += -v2.z * dv0.y * v1.x;
-    k1 += -dv2.z * v0.y * v1.x;
-    k1 += v0.z * v2.y * dv1.x;
-    k1 += v0.z * dv2.y * v1.x;
-    k1 += dv0.z * v2.y * v1.x;
-    k1 += v1.z * v0.y * dv2.x;
-    k1 += v1.z * dv0.y * v2.x;
-    k1 += dv1.z * v0.y * v2.x;
-    k1 += -v0.z * v1.y * dv2.x;
-    k1 += -v0.z * dv1.y * v2.x;
-    k1 += -dv0.z * v1.y * v2.x;
+    k1 = fmaT(v2.z * v1.y, dv0.x, k1);
+    k1 = fmaT(v2.z * dv1.y, v0.x, k1);
+    k1 = fmaT(dv2.z * v1.y, v0.x, k1);
+    k1 = fmaT(-v1.z * v2.y, dv0.x, k1);
+    k1 = fmaT(-v1.z * dv2.y, v0.x, k1);
+    k1 = fmaT(-dv1.z * v2.y, v0.x, k1);
+    k1 = fmaT(-v2.z * v0.y, dv1.x, k1);
+    k1 = fmaT(-v2.z * dv0.y, v1.x, k1);
+    k1 = fmaT(-dv2.z * v0.y, v1.x, k1);
+    k1 = fmaT(v0.z * v2.y, dv1.x, k1);
+    k1 = fmaT(v0.z * dv2.y, v1.x, k1);
+    k1 = fmaT(dv0.z * v2.y, v1.x, k1);
+    k1 = fmaT(v1.z * v0.y, dv2.x, k1);
+    k1 = fmaT(v1.z * dv0.y, v2.x, k1);
+    k1 = fmaT(dv1.z * v0.y, v2.x, k1);
+    k1 = fmaT(-v0.z * v1.y, dv2.x, k1);
+    k1 = fmaT(-v0.z * dv1.y, v2.x, k1);
+    k1 = fmaT(-dv0.z * v1.y, v2.x, k1);
     T k0 = 0;
-    k0 += v2.z * v1.y * v0.x;
-    k0 += -v1.z * v2.y * v0.x;
-    k0 += -v2.z * v0.y * v1.x;
-    k0 += v0.z * v2.y * v1.x;
-    k0 += v1.z * v0.y * v2.x;
-    k0 += -v0.z * v1.y * v2.x;
+    k0 = fmaT(v2.z * v1.y, v0.x, k0);
+    k0 = fmaT(-v1.z * v2.y, v0.x, k0);
+    k0 = fmaT(-v2.z * v0.y, v1.x, k0);
+    k0 = fmaT(v0.z * v2.y, v1.x, k0);
+    k0 = fmaT(v1.z * v0.y, v2.x, k0);
+    k0 = fmaT(-v0.z * v1.y, v2.x, k0);
     c[0] = k3; c[1] = k2; c[2] = k1; c[3] = k0;
 }
 
@@ -352,13 +375,13 @@ template <class T> __device__ __forceinline__ void add_root(T r[3], T x, int& nr
 }
 
 // solveCubic with computeG / computeH (collisions_continuous.cu:472-613); roots start at -1.
-template <class T> __device__ __noinline__ void solve_cubic(double a, double b, double c, double d, T r[3]) {
+template <class T> __device__ __noinline__ void solve_cubic(double a, double b, double c, double d, T r[3], int lib) {
     r[0] = r[1] = r[2] = (T)-1;
     int nr = 0;
     if (a == 0 && b == 0) {
         return;     // linear case: the reference never stores its root
     } else if (fabs(a) < CCC_EPS) {
-        double D = c * c - 4.0 * b * d;
+        double D = fmaT(c, c, -(4.0 * b * d));
         if (D >= 0) {
             D = ccc_sqrt(D);
             double x1 = (-c + D) / (2.0 * b);
@@ -377,35 +400,52 @@ template <class T> __device__ __noinline__ void solve_cubic(double a, double b, 
         double p3 = 27.0 * d / a;
         double g = (p1 - p2 + p3) / 27.0;
         double f3 = ccc_cube_hi(f);
-        double h = g * g / 4.0 + f3 / 27.0;
+        // the reference's pow(g, 2) resolves (through std::pow's promotion) to CUDA's general
+        // pow(double, double), which is not always the rounded square
+        double g2 = lib == LIB_REFERENCE ? pow(g, 2.0) : g * g;
+        double h = g2 / 4.0 + f3 / 27.0;
         if (f == 0 && g == 0 && h == 0) {
             float k = (float)(d / a);
             double x1;
-            if (k >= 0) x1 = (double)(ccc_cbrtf(k) * -1);
-            else x1 = (double)ccc_cbrtf(-k);
+            float cr = lib == LIB_REFERENCE ? cbrtf(k >= 0 ? k : -k) : ccc_cbrtf(k >= 0 ? k : -k);
+            if (k >= 0) x1 = (double)(cr * -1);
+            else x1 = (double)cr;
             add_root<T>(r, (T)x1, nr);
         } else if (h <= 0) {
             double i = ccc_sqrt(((g * g) / 4.0) - h);
-            double j = ccc_cbrt(i);
-            double k = ccc_acos(-(g / (2 * i)));
+            double j, k, M, sn;
+            if (lib == LIB_REFERENCE) {
+                j = cbrt(i);
+                k = acos(-(g / (2 * i)));
+                M = cos(k / 3.0);
+                sn = sin(k / 3.0);
+            } else {
+                j = ccc_cbrt(i);
+                k = ccc_acos(-(g / (2 * i)));
+                M = ccc_cos(k / 3.0);
+                sn = ccc_sin(k / 3.0);
+            }
+            // N = sqrt(3) * sin(k/3) is fused into M + N and M - N and each result into
+            // L * (.) + P; the first root 2 j cos(k/3) - b/(3a) is rounded twice (unfused)
+            const double r3 = ccc_sqrt(3.0);
             double L = j * -1;
-            double M = ccc_cos(k / 3.0);
-            double N = ccc_sqrt(3.0) * ccc_sin(k / 3.0);
             double P = (b / (3.0 * a)) * -1;
-            double x1 = 2 * j * ccc_cos(k / 3.0) - (b / (3.0 * a));
-            double x2 = L * (M + N) + P;
-            double x3 = L * (M - N) + P;
+            double x1 = (2 * j) * M - (b / (3.0 * a));
+            double x2 = fmaT(L, fmaT(r3, sn, M), P);
+            double x3 = fmaT(L, fmaT(-r3, sn, M), P);
             add_root<T>(r, (T)x1, nr);
             add_root<T>(r, (T)x2, nr);
             add_root<T>(r, (T)x3, nr);
         } else {
             double R = -(g / 2.0) + ccc_sqrt(h);
             double S, U;
-            if (R >= 0) S = ccc_cbrt(R);
-            else S = -ccc_cbrt(-R);
+            double Ra = R >= 0 ? R : -R;
+            S = lib == LIB_REFERENCE ? cbrt(Ra) : ccc_cbrt(Ra);
+            if (R < 0) S = -S;
             double V = -(g / 2.0) - ccc_sqrt(h);
-            if (V >= 0) U = ccc_cbrt(V);
-            else U = -ccc_cbrt(-V);
+            double Va = V >= 0 ? V : -V;
+            U = lib == LIB_REFERENCE ? cbrt(Va) : ccc_cbrt(Va);
+            if (V < 0) U = -U;
             double x1 = (S + U) - (b / (3.0 * a));
             add_root<T>(r, (T)x1, nr);
         }
@@ -416,9 +456,9 @@ template <class T> __device__ __noinline__ void solve_cubic(double a, double b, 
 template <class T> __device__ __forceinline__ bool is_inside(V3<T> v0, V3<T> v1, V3<T> v2, V3<T> vt) {
     V3<T> e1 = v0 - v1, e2 = v2 - v1, ep = vt - v1;
     T d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2), d20 = dot(ep, e1), d21 = dot(ep, e2);
-    T denom = d00 * d11 - d01 * d01;
-    T v = (d11 * d20 - d01 * d21) / denom;
-    T w = (d00 * d21 - d01 * d20) / denom;
+    T denom = fms2(d00, d11, d01, d01);
+    T v = fms2(d11, d20, d01, d21) / denom;
+    T w = fms2(d00, d21, d01, d20) / denom;
     T u = 1 - v - w;
     if (v < 0 || v > 1) return false;
     if (w < 0 || w > 1) return false;
@@ -426,7 +466,7 @@ template <class T> __device__ __forceinline__ bool is_inside(V3<T> v0, V3<T> v1,
     return true;
 }
 
-template <class T> __device__ __forceinline__ V3<T> at_time(const MTet<T>& t, int i, T root) { return t.v[i] + t.dv[i] * root; }
+template <class T> __device__ __forceinline__ V3<T> at_time(const MTet<T>& t, int i, T root) { return axpy(t.v[i], t.dv[i], root); }
 
 // filterCollisions (collisions_continuous.cu:640-684)
 template <class T> __device__ __forceinline__ bool ccd_filter(const MTet<T>& tet, int k, T root) {
@@ -448,10 +488,12 @@ template <class T> __device__ __forceinline__ bool ccd_filter(const MTet<T>& tet
 
 #define CCC_THICKNESS 2e-3   // collisions_impulses.cu:12-14
 
-template <class T> __device__ __forceinline__ V3<T> vnormalize(V3<T> a) {
-    T n = a.x * a.x + a.y * a.y + a.z * a.z;
-    T inv = (T)1 / (T)ccc_sqrt((double)n);
-    return a * inv;
+// normalize(double3) = a * rsqrt(|a|^2) (utils.cu:91-93); the portable form uses 1 / sqrt
+__device__ __forceinline__ float rsqrt_lib(float n, int lib) { return lib == LIB_REFERENCE ? rsqrtf(n) : 1.0f / sqrtf(n); }
+__device__ __forceinline__ double rsqrt_lib(double n, int lib) { return lib == LIB_REFERENCE ? rsqrt(n) : 1.0 / ccc_sqrt(n); }
+template <class T> __device__ __forceinline__ V3<T> vnormalize(V3<T> a, int lib) {
+    T n = norm2(a);
+    return a * rsqrt_lib(n, lib);
 }
 
 template <class T> struct Contact { V3<T> n; T vn, m0, m1; };
@@ -460,7 +502,7 @@ template <class T> struct Contact { V3<T> n; T vn, m0, m1; };
 // q holds the masses of the four tetrahedron points.  For vertex-face types the points
 // are first put in (face 0, face 1, face 2, vertex) order with selects: types 9..11 are
 // already in that order, types 12..14 have the vertex first.
-template <class T> __device__ __forceinline__ Contact<T> contact(const MTet<T>& tet, int k, T root, const T q[4]) {
+template <class T> __device__ __forceinline__ Contact<T> contact(const MTet<T>& tet, int k, T root, const T q[4], int lib) {
     Contact<T> ct;
     if (k < 9) {
         V3<T> th0 = at_time(tet, 0, root), th1 = at_time(tet, 1, root), th2 = at_time(tet, 2, root),
@@ -475,17 +517,17 @@ template <class T> __device__ __forceinline__ Contact<T> contact(const MTet<T>& 
         }
         const V3<T>* v = tet.v;
         const V3<T>* dv = tet.dv;
-        V3<T> p0 = v[0] + (v[1] - v[0]) * s;
-        V3<T> p1 = v[2] + (v[3] - v[2]) * t;
-        V3<T> dp0 = dv[0] + (dv[1] - dv[0]) * s;
-        V3<T> dp1 = dv[2] + (dv[3] - dv[2]) * t;
-        V3<T> c0 = v[0] + dv[0] * root, c1 = v[1] + dv[1] * root, c2 = v[2] + dv[2] * root;
-        V3<T> nd = vnormalize(cross(c1 - c0, c2 - c0));
+        V3<T> p0 = axpy(v[0], v[1] - v[0], s);
+        V3<T> p1 = axpy(v[2], v[3] - v[2], t);
+        V3<T> dp0 = axpy(dv[0], dv[1] - dv[0], s);
+        V3<T> dp1 = axpy(dv[2], dv[3] - dv[2], t);
+        V3<T> c0 = axpy(v[0], dv[0], root), c1 = axpy(v[1], dv[1], root), c2 = axpy(v[2], dv[2], root);
+        V3<T> nd = vnormalize(cross(c1 - c0, c2 - c0), lib);
         if (dot(p1 - p0, nd) < 0) nd = nd * (T)-1;
         ct.n = nd;
         ct.vn = dot(dp1 - dp0, nd);
-        ct.m0 = q[0] * (1 - s) + q[1] * s;
-        ct.m1 = q[2] * (1 - t) + q[3] * t;
+        ct.m0 = fmaT(q[0], 1 - s, q[1] * s);
+        ct.m1 = fmaT(q[2], 1 - t, q[3] * t);
         return ct;
     }
     const bool inv = k >= 12;
@@ -494,26 +536,26 @@ template <class T> __device__ __forceinline__ Contact<T> contact(const MTet<T>& 
     V3<T> D0 = inv ? tet.dv[1] : tet.dv[0], D1 = inv ? tet.dv[2] : tet.dv[1], D2 = inv ? tet.dv[3] : tet.dv[2],
           DV = inv ? tet.dv[0] : tet.dv[3];
     T q0 = inv ? q[1] : q[0], q1 = inv ? q[2] : q[1], q2 = inv ? q[3] : q[2], qv = inv ? q[0] : q[3];
-    V3<T> t0 = F0 + D0 * root, t1 = F1 + D1 * root, t2 = F2 + D2 * root, tv = FV + DV * root;
+    V3<T> t0 = axpy(F0, D0, root), t1 = axpy(F1, D1, root), t2 = axpy(F2, D2, root), tv = axpy(FV, DV, root);
     V3<T> e1 = t0 - t1, e2 = t2 - t1, ep = tv - t1;
     T d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2), d20 = dot(ep, e1), d21 = dot(ep, e2);
-    T denom = d00 * d11 - d01 * d01;
+    T denom = fms2(d00, d11, d01, d01);
     T u, w, vv;
     if (fabs((double)denom) < 1e-15) { u = (T)(1. / 3.); w = (T)(1. / 3.); }
     else {
-        u = (d11 * d20 - d01 * d21) / denom;
-        w = (d00 * d21 - d01 * d20) / denom;
+        u = fms2(d11, d20, d01, d21) / denom;
+        w = fms2(d00, d21, d01, d20) / denom;
     }
     vv = 1 - u - w;
-    V3<T> pt = F0 * u + F1 * vv + F2 * w;
-    V3<T> dpt = D0 * u + D1 * vv + D2 * w;
-    V3<T> c0 = F0 + D0 * root, c1 = F1 + D1 * root, c2 = F2 + D2 * root;
-    V3<T> nd = vnormalize(cross(c1 - c0, c2 - c0));
+    V3<T> pt = lin3(F0, u, F1, vv, F2, w);
+    V3<T> dpt = lin3(D0, u, D1, vv, D2, w);
+    V3<T> c0 = axpy(F0, D0, root), c1 = axpy(F1, D1, root), c2 = axpy(F2, D2, root);
+    V3<T> nd = vnormalize(cross(c1 - c0, c2 - c0), lib);
     if (dot(FV - pt, nd) < 0) nd = nd * (T)-1;
     ct.vn = dot(DV - dpt, nd);
     if (inv) nd = nd * (T)-1;
     ct.n = nd;
-    T mface = q0 * u + q1 * vv + q2 * w;
+    T mface = fmaT(q2, w, fmaT(q0, u, q1 * vv));
     ct.m0 = inv ? qv : mface;
     ct.m1 = inv ? mface : qv;
     return ct;
@@ -578,7 +620,7 @@ template <class T> __device__ __forceinline__ void pt_seg(V3<T> p, V3<T> a, V3<T
     T t = dot(ap, ab) / dot(ab, ab);
     if (t < (T)0.0) t = (T)0.0;
     if (t > (T)1.0) t = (T)1.0;
-    V3<T> c = mk<T>(a.x + t * ab.x, a.y + t * ab.y, a.z + t * ab.z);
+    V3<T> c = mk<T>(fmaT(t, ab.x, a.x), fmaT(t, ab.y, a.y), fmaT(t, ab.z, a.z));
     T nd = (T)__fsqrt_rn(sq_diff_f(p, c));
     if (nd < dc[0]) {
         dc[0] = nd;
@@ -609,18 +651,18 @@ template <class T> __device__ __forceinline__ T prox_distance(const Tri<T>& a, c
         }
         bool sv = (s >= 0 && s <= 1), tv = (t >= 0 && t <= 1);
         if (!sv || !tv) return (T)-1;
-        return (T)__fsqrt_rn(sq_diff_f(v[0] + da * s, v[2] + db * t));
+        return (T)__fsqrt_rn(sq_diff_f(axpy(v[0], da, s), axpy(v[2], db, t)));
     }
     int f0 = k < 12 ? 0 : 1, f1 = k < 12 ? 1 : 2, f2 = k < 12 ? 2 : 3, fv = k < 12 ? 3 : 0;
     V3<T> e1 = v[f0] - v[f1], e2 = v[f2] - v[f1], ep = v[fv] - v[f1];
     T d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2), d20 = dot(ep, e1), d21 = dot(ep, e2);
-    T denom = d00 * d11 - d01 * d01;
-    T u = (d11 * d20 - d01 * d21) / denom;
-    T w = (d00 * d21 - d01 * d20) / denom;
+    T denom = fms2(d00, d11, d01, d01);
+    T u = fms2(d11, d20, d01, d21) / denom;
+    T w = fms2(d00, d21, d01, d20) / denom;
     T vv = 1 - w - u;
     bool ok = (vv >= 0 && vv <= 1) && (w >= 0 && w <= 1) && (u >= 0 && u <= 1);
     if (!ok) return (T)-1;
-    V3<T> pt = v[f0] * u + v[f1] * vv + v[f2] * w;
+    V3<T> pt = lin3(v[f0], u, v[f1], vv, v[f2], w);
     return (T)__fsqrt_rn(sq_diff_f(v[fv], pt));
 }
 

@@ -410,7 +410,7 @@ __global__ void __launch_bounds__(NARROW_THREADS, 3)
 k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ x0,
              const T* __restrict__ x1, const int* __restrict__ moff, int M, long long* __restrict__ rows,
              T* __restrict__ times, int max_per_tri, int* __restrict__ mesh_counters, const T* __restrict__ masses,
-             T* __restrict__ dv_out, T* __restrict__ dx_out, int* __restrict__ cnt_out) {
+             T* __restrict__ dv_out, T* __restrict__ dx_out, int* __restrict__ cnt_out, int lib) {
     constexpr int WARPS = NARROW_THREADS / 32;
     __shared__ unsigned short items[WARPS][32 * 15];
     __shared__ int2 pairs[WARPS][32];
@@ -468,7 +468,7 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
             T cf[4];
             cubic_coeffs(tet, cf);
             T rr[3];
-            solve_cubic<T>((double)cf[0], (double)cf[1], (double)cf[2], (double)cf[3], rr);
+            solve_cubic<T>((double)cf[0], (double)cf[1], (double)cf[2], (double)cf[3], rr, lib);
 #pragma unroll 1
             for (int s = 0; s < 3; ++s) {
                 T root = rr[s];
@@ -490,7 +490,7 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
 #pragma unroll
                     for (int pt = 0; pt < 4; ++pt)
                         mq[pt] = masses[(long long)(tet_side(k, pt) ? q.y : q.x) * 3 + tet_corner(k, pt)];
-                    Contact<T> ct = contact(tet, k, root, mq);
+                    Contact<T> ct = contact(tet, k, root, mq, lib);
                     apply_impulse(tet, q.x, q.y, k, root, ct, dv_out, dx_out, cnt_out);
                 }
             }
@@ -534,7 +534,7 @@ template <class T>
 __global__ void __launch_bounds__(NARROW_THREADS)
 k_impulses_from_rows(const long long* __restrict__ rows, const T* __restrict__ roots, int B, long long N, int F,
                      const T* __restrict__ x0, const T* __restrict__ x1, const T* __restrict__ masses,
-                     T* __restrict__ dv_out, T* __restrict__ dx_out, int* __restrict__ cnt_out, WsHeader* hdr) {
+                     T* __restrict__ dv_out, T* __restrict__ dx_out, int* __restrict__ cnt_out, WsHeader* hdr, int lib) {
     long long total = (long long)B * N;
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < total;
          r += (long long)gridDim.x * blockDim.x) {
@@ -547,7 +547,7 @@ k_impulses_from_rows(const long long* __restrict__ rows, const T* __restrict__ r
         MTet<T> tet = load_tet(x0, x1, gi, gj, k);
         T mq[4];
         for (int pt = 0; pt < 4; ++pt) mq[pt] = masses[(tet_side(k, pt) ? gj : gi) * 3 + tet_corner(k, pt)];
-        Contact<T> ct = contact(tet, k, root, mq);
+        Contact<T> ct = contact(tet, k, root, mq, lib);
         apply_impulse(tet, gi, gj, k, root, ct, dv_out, dx_out, cnt_out);
     }
 }
@@ -574,7 +574,7 @@ __global__ void k_debug_math(int op, const double* __restrict__ in, double* __re
             o[1] = d.lo;
             break;
         }
-        case 5: solve_cubic<double>(a[0], a[1], a[2], a[3], o); break;
+        case 5: solve_cubic<double>(a[0], a[1], a[2], a[3], o, LIB_PORTABLE); break;
         case 6: o[0] = cbrt(a[0]); break;
         case 7: o[0] = acos(a[0]); break;
         case 8: o[0] = cos(a[0]); break;
@@ -592,6 +592,57 @@ __global__ void k_debug_math(int op, const double* __restrict__ in, double* __re
             break;
         }
         default: break;
+    }
+}
+
+// Stages of the continuous narrow phase on caller tetrahedra (v0..v3, dv0..dv3 = 24
+// doubles per element), for tests against the reference's own kernels and the oracle.
+// op 0: cubic coefficients -> 4 doubles; op 1: cubic solve (in: 4 coefficients) -> 3
+// roots; op 2: root filter (in: tet, type, root) -> 1.0 / 0.0; op 3: contact kinematics
+// (in: tet, type, root, 4 masses) -> normal (3), normal velocity, mass pair (2).
+// lib selects the elementary functions (MathLib).
+__global__ void k_debug_stage(int op, int lib, const double* __restrict__ in, int in_stride,
+                              double* __restrict__ out, int out_stride, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double* a = in + (long long)i * in_stride;
+    double* o = out + (long long)i * out_stride;
+    MTet<double> t;
+    if (op != 1) {
+        for (int p = 0; p < 4; ++p) {
+            t.v[p] = mk<double>(a[3 * p], a[3 * p + 1], a[3 * p + 2]);
+            t.dv[p] = mk<double>(a[12 + 3 * p], a[12 + 3 * p + 1], a[12 + 3 * p + 2]);
+        }
+    }
+    if (op == 0) {
+        cubic_coeffs(t, o);
+    } else if (op == 1) {
+        solve_cubic<double>(a[0], a[1], a[2], a[3], o, lib);
+    } else if (op == 2) {
+        o[0] = ccd_filter(t, (int)a[24], a[25]) ? 1.0 : 0.0;
+    } else if (op == 4) {
+        // (f, g, h) of the solver prefix for coefficients (c3, c2, c1, c0)
+        double A = a[0], B = a[1], Cc = a[2], D = a[3];
+        double f = ((3.0 * Cc / A) - ((B * B) / (A * A))) / 3.0;
+        double b3 = 2 * ccc_cube_hi(B);
+        ccc_dd a2dd = ccc_sq_dd(A);
+        double a3 = ccc_certmul(a2dd.hi, a2dd.lo, 2, A).hi;
+        double g = (b3 / a3 - (B * Cc * 9) / a2dd.hi + 27.0 * D / A) / 27.0;
+        double g2 = lib == LIB_REFERENCE ? pow(g, 2.0) : g * g;
+        o[0] = f;
+        o[1] = g;
+        o[2] = g2 / 4.0 + ccc_cube_hi(f) / 27.0;
+    } else if (op == 5) {
+        // squares of a[0]: pow(x, 2), pow(x, 2.0), x * x
+        double x = a[0];
+        volatile int two = 2;
+        o[0] = pow(x, two);
+        o[1] = pow(x, (double)two);
+        o[2] = x * x;
+    } else if (op == 3) {
+        double q[4] = {a[26], a[27], a[28], a[29]};
+        Contact<double> ct = contact(t, (int)a[24], a[25], q, lib);
+        o[0] = ct.n.x; o[1] = ct.n.y; o[2] = ct.n.z; o[3] = ct.vn; o[4] = ct.m0; o[5] = ct.m1;
     }
 }
 

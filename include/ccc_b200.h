@@ -60,6 +60,25 @@ int64_t ccc_kernel_launches(void);
 int ccc_timing_begin(void);
 int ccc_timing_end(int max_kernels, char* names, int name_len, float* total_ms, int32_t* count);
 
+/* Elementary functions used by the continuous-collision solver and the impulse normals
+ * (no counterpart in the reference, which always uses CUDA's): CCC_LIB_REFERENCE (default)
+ * calls CUDA's cbrt, acos, cos, sin, pow and rsqrt exactly where the reference does;
+ * CCC_LIB_PORTABLE uses this library's own implementations, which the CPU oracle shares
+ * bit for bit.  Process-wide; returns CCC_ERR_INVALID_ARG for other values. */
+#define CCC_LIB_REFERENCE 0
+#define CCC_LIB_PORTABLE 1
+int ccc_set_math_library(int lib);
+int ccc_get_math_library(void);
+
+/* Test hook (no counterpart in the reference): one stage of the continuous narrow phase on
+ * caller tetrahedra (device arrays; rows of in_stride / out_stride doubles).  op 0: cubic
+ * coefficients of (v0..v3, dv0..dv3) -> (c3, c2, c1, c0); op 1: cubic solve of
+ * (c3, c2, c1, c0) -> three roots (-1 = none); op 2: root filter of (tet, type, root) ->
+ * 1 / 0; op 3: contact kinematics of (tet, type, root, four masses) -> (normal, normal
+ * velocity, mass pair).  lib: CCC_LIB_REFERENCE or CCC_LIB_PORTABLE. */
+int ccc_debug_stage(int op, int lib, const double* in, int in_stride, double* out, int out_stride, int64_t n,
+                    void* stream);
+
 /* Test hook (no counterpart in the reference): evaluates the continuous-collision solver's
  * arithmetic element-wise on the device so tests can compare it with the CPU oracle.
  * op: 0 cbrt, 1 acos, 2 cos, 3 sin (the library's own), 4 certified product

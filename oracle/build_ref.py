@@ -57,9 +57,33 @@ def build(src="/root/reference", force=False) -> str:
     return so
 
 
+def build_probe(src="/root/reference", force=False) -> str:
+    """oracle/_ref/libref_probe.so: oracle/ref_probe.cu + the reference sources (stage probe)."""
+    so = os.path.join(OUT, "libref_probe.so")
+    if os.path.exists(so) and not force:
+        return so
+    import torch.utils.cpp_extension as ce
+    os.makedirs(OUT, exist_ok=True)
+    inc = ce.include_paths()
+    py = sysconfig.get_paths()["include"]
+    libdir = ce.library_paths()[0]
+    cmd = ["/usr/local/cuda/bin/nvcc", "-shared", "-Xcompiler", "-fPIC", "-o", so, os.path.join(HERE, "ref_probe.cu"),
+           "-gencode", "arch=compute_100,code=sm_100", "-std=c++17", "-D__CUDA_NO_HALF_OPERATORS__",
+           "-D__CUDA_NO_HALF_CONVERSIONS__", "-D__CUDA_NO_BFLOAT16_CONVERSIONS__", "-D__CUDA_NO_HALF2_OPERATORS__",
+           "--expt-relaxed-constexpr", "-w", "-include", os.path.join(SHIM, "torch_compat.h"),
+           f"-I{os.path.join(src, 'src')}", f"-I{os.path.join(src, 'include')}", f"-I{SHIM}", f"-I{py}",
+           "-DTORCH_EXTENSION_NAME=ref_probe", "-D_GLIBCXX_USE_CXX11_ABI=1", "-DAT_CHECK=TORCH_CHECK"]
+    cmd += [f"-I{p}" for p in inc]
+    cmd += [f"-L{libdir}", "-lc10", "-lc10_cuda", "-ltorch", "-ltorch_cpu", "-ltorch_cuda", f"-Xlinker",
+            f"-rpath,{libdir}"]
+    subprocess.check_call(cmd)
+    return so
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--src", default="/root/reference")
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()
     print(build(a.src, a.force))
+    print(build_probe(a.src, a.force))

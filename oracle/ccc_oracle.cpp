@@ -16,8 +16,13 @@
 //   * impulses (src/collisions_impulses.cu:24-1067)
 //   * proximity (src/proximity_static.cu:11-508)
 //
-// Arithmetic: plain IEEE-754 float/double with no contraction (built with
-// -ffp-contract=off), the reference's evaluation order kept term by term.  The
+// Arithmetic: IEEE-754 float/double in the reference's evaluation order, term by term.
+// The reference is compiled by nvcc with its default fused multiply-add contraction, so
+// the restatement writes those fusions out explicitly (fmaT) where nvcc forms them:
+// a*b + c -> fma(a, b, c); c + a*b -> fma(a, b, c); a*b + c*d and a*b - c*d fuse the first
+// product; dot / cross / norm2 become fixed fma chains.  This model reproduces the
+// reference's cubic coefficients and root filters bit for bit (tests/test_golden.py).
+// Nothing else is contracted (built with -ffp-contract=off).  The
 // transcendental calls of the cubic solver go through ccc_libm.h and the CAMPARY products
 // through ccc_ddmul.h, which the CUDA path includes too, so results agree to the bit.
 //
@@ -48,11 +53,26 @@ template <class T> static inline V3<T> operator+(V3<T> a, V3<T> b) { return mk<T
 template <class T> static inline V3<T> operator-(V3<T> a, V3<T> b) { return mk<T>(a.x - b.x, a.y - b.y, a.z - b.z); }
 template <class T> static inline V3<T> operator*(V3<T> a, T s) { return mk<T>(a.x * s, a.y * s, a.z * s); }
 template <class T> static inline V3<T> operator/(V3<T> a, T s) { return mk<T>(a.x / s, a.y / s, a.z / s); }
-template <class T> static inline T dot(V3<T> a, V3<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline float fmaT(float a, float b, float c) { return fmaf(a, b, c); }
+static inline double fmaT(double a, double b, double c) { return fma(a, b, c); }
+// a.x*b.x + a.y*b.y + a.z*b.z  ->  fma(a.z, b.z, fma(a.x, b.x, a.y*b.y))
+template <class T> static inline T dot(V3<T> a, V3<T> b) { return fmaT(a.z, b.z, fmaT(a.x, b.x, a.y * b.y)); }
+// a.y*b.z - a.z*b.y  ->  fma(a.y, b.z, -(a.z*b.y)), and cyclically
 template <class T> static inline V3<T> cross(V3<T> a, V3<T> b) {
-    return mk<T>(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+    return mk<T>(fmaT(a.y, b.z, -(a.z * b.y)), fmaT(a.z, b.x, -(a.x * b.z)), fmaT(a.x, b.y, -(a.y * b.x)));
 }
-template <class T> static inline T norm2(V3<T> a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
+template <class T> static inline T norm2(V3<T> a) { return fmaT(a.z, a.z, fmaT(a.x, a.x, a.y * a.y)); }
+// v + d * t  ->  fma(d, t, v) per component
+template <class T> static inline V3<T> axpy(V3<T> v, V3<T> d, T t) {
+    return mk<T>(fmaT(d.x, t, v.x), fmaT(d.y, t, v.y), fmaT(d.z, t, v.z));
+}
+// a*u + b*v + c*w  ->  fma(c, w, fma(a, u, b*v)) per component
+template <class T> static inline V3<T> lin3(V3<T> a, T u, V3<T> b, T v, V3<T> c, T w) {
+    return mk<T>(fmaT(c.x, w, fmaT(a.x, u, b.x * v)), fmaT(c.y, w, fmaT(a.y, u, b.y * v)),
+                 fmaT(c.z, w, fmaT(a.z, u, b.z * v)));
+}
+// a*b - c*d  ->  fma(a, b, -(c*d))
+template <class T> static inline T fms2(T a, T b, T c, T d) { return fmaT(a, b, -(c * d)); }
 // CUDA min/max on floating point follow fmin/fmax (a NaN operand yields the other one)
 template <class T> static inline T fmn(T a, T b) { return (T)fmin(a, b); }
 template <class T> static inline T fmx(T a, T b) { return (T)fmax(a, b); }
@@ -532,57 +552,57 @@ template <class T> static void cubic_coeffs(const MTet<T>& t, T c[4]) {
     V3<T> dv0 = t.dv[0] - t.dv[3], dv1 = t.dv[1] - t.dv[3], dv2 = t.dv[2] - t.dv[3];
     // SCALE == 1 (flags.h:57-59): multiplying by it is exact and omitted
     T k3 = 0;
-    k3 += dv2.z * dv1.y * dv0.x;
-    k3 += -dv1.z * dv2.y * dv0.x;
-    k3 += -dv2.z * dv0.y * dv1.x;
-    k3 += dv0.z * dv2.y * dv1.x;
-    k3 += dv1.z * dv0.y * dv2.x;
-    k3 += -dv0.z * dv1.y * dv2.x;
+    k3 = fmaT(dv2.z * dv1.y, dv0.x, k3);
+    k3 = fmaT(-dv1.z * dv2.y, dv0.x, k3);
+    k3 = fmaT(-dv2.z * dv0.y, dv1.x, k3);
+    k3 = fmaT(dv0.z * dv2.y, dv1.x, k3);
+    k3 = fmaT(dv1.z * dv0.y, dv2.x, k3);
+    k3 = fmaT(-dv0.z * dv1.y, dv2.x, k3);
     T k2 = 0;
-    k2 += v2.z * dv1.y * dv0.x;
-    k2 += dv2.z * v1.y * dv0.x;
-    k2 += dv2.z * dv1.y * v0.x;
-    k2 += -v1.z * dv2.y * dv0.x;
-    k2 += -dv1.z * v2.y * dv0.x;
-    k2 += -dv1.z * dv2.y * v0.x;
-    k2 += -v2.z * dv0.y * dv1.x;
-    k2 += -dv2.z * v0.y * dv1.x;
-    k2 += -dv2.z * dv0.y * v1.x;
-    k2 += v0.z * dv2.y * dv1.x;
-    k2 += dv0.z * v2.y * dv1.x;
-    k2 += dv0.z * dv2.y * v1.x;
-    k2 += v1.z * dv0.y * dv2.x;
-    k2 += dv1.z * v0.y * dv2.x;
-    k2 += dv1.z * dv0.y * v2.x;
-    k2 += -v0.z * dv1.y * dv2.x;
-    k2 += -dv0.z * v1.y * dv2.x;
-    k2 += -dv0.z * dv1.y * v2.x;
+    k2 = fmaT(v2.z * dv1.y, dv0.x, k2);
+    k2 = fmaT(dv2.z * v1.y, dv0.x, k2);
+    k2 = fmaT(dv2.z * dv1.y, v0.x, k2);
+    k2 = fmaT(-v1.z * dv2.y, dv0.x, k2);
+    k2 = fmaT(-dv1.z * v2.y, dv0.x, k2);
+    k2 = fmaT(-dv1.z * dv2.y, v0.x, k2);
+    k2 = fmaT(-v2.z * dv0.y, dv1.x, k2);
+    k2 = fmaT(-dv2.z * v0.y, dv1.x, k2);
+    k2 = fmaT(-dv2.z * dv0.y, v1.x, k2);
+    k2 = fmaT(v0.z * dv2.y, dv1.x, k2);
+    k2 = fmaT(dv0.z * v2.y, dv1.x, k2);
+    k2 = fmaT(dv0.z * dv2.y, v1.x, k2);
+    k2 = fmaT(v1.z * dv0.y, dv2.x, k2);
+    k2 = fmaT(dv1.z * v0.y, dv2.x, k2);
+    k2 = fmaT(dv1.z * dv0.y, v2.x, k2);
+    k2 = fmaT(-v0.z * dv1.y, dv2.x, k2);
+    k2 = fmaT(-dv0.z * v1.y, dv2.x, k2);
+    k2 = fmaT(-dv0.z * dv1.y, v2.x, k2);
     T k1 = 0;
-    k1 += v2.z * v1.y * dv0.x;
-    k1 += v2.z * dv1.y * v0.x;
-    k1 += dv2.z * v1.y * v0.x;
-    k1 += -v1.z * v2.y * dv0.x;
-    k1 += -v1.z * dv2.y * v0.x;
-    k1 += -dv1.z * v2.y * v0.x;
-    k1 += -v2.z * v0.y * dv1.x;
-    k1 += -v2.z * dv0.y * v1.x;
-    k1 += -dv2.z * v0.y * v1.x;
-    k1 += v0.z * v2.y * dv1.x;
-    k1 += v0.z * dv2.y * v1.x;
-    k1 += dv0.z * v2.y * v1.x;
-    k1 += v1.z * v0.y * dv2.x;
-    k1 += v1.z * dv0.y * v2.x;
-    k1 += dv1.z * v0.y * v2.x;
-    k1 += -v0.z * v1.y * dv2.x;
-    k1 += -v0.z * dv1.y * v2.x;
-    k1 += -dv0.z * v1.y * v2.x;
+    k1 = fmaT(v2.z * v1.y, dv0.x, k1);
+    k1 = fmaT(v2.z * dv1.y, v0.x, k1);
+    k1 = fmaT(dv2.z * v1.y, v0.x, k1);
+    k1 = fmaT(-v1.z * v2.y, dv0.x, k1);
+    k1 = fmaT(-v1.z * dv2.y, v0.x, k1);
+    k1 = fmaT(-dv1.z * v2.y, v0.x, k1);
+    k1 = fmaT(-v2.z * v0.y, dv1.x, k1);
+    k1 = fmaT(-v2.z * dv0.y, v1.x, k1);
+    k1 = fmaT(-dv2.z * v0.y, v1.x, k1);
+    k1 = fmaT(v0.z * v2.y, dv1.x, k1);
+    k1 = fmaT(v0.z * dv2.y, v1.x, k1);
+    k1 = fmaT(dv0.z * v2.y, v1.x, k1);
+    k1 = fmaT(v1.z * v0.y, dv2.x, k1);
+    k1 = fmaT(v1.z * dv0.y, v2.x, k1);
+    k1 = fmaT(dv1.z * v0.y, v2.x, k1);
+    k1 = fmaT(-v0.z * v1.y, dv2.x, k1);
+    k1 = fmaT(-v0.z * dv1.y, v2.x, k1);
+    k1 = fmaT(-dv0.z * v1.y, v2.x, k1);
     T k0 = 0;
-    k0 += v2.z * v1.y * v0.x;
-    k0 += -v1.z * v2.y * v0.x;
-    k0 += -v2.z * v0.y * v1.x;
-    k0 += v0.z * v2.y * v1.x;
-    k0 += v1.z * v0.y * v2.x;
-    k0 += -v0.z * v1.y * v2.x;
+    k0 = fmaT(v2.z * v1.y, v0.x, k0);
+    k0 = fmaT(-v1.z * v2.y, v0.x, k0);
+    k0 = fmaT(-v2.z * v0.y, v1.x, k0);
+    k0 = fmaT(v0.z * v2.y, v1.x, k0);
+    k0 = fmaT(v1.z * v0.y, v2.x, k0);
+    k0 = fmaT(-v0.z * v1.y, v2.x, k0);
     c[0] = k3; c[1] = k2; c[2] = k1; c[3] = k0;
 }
 
@@ -604,7 +624,7 @@ template <class T> static void solve_cubic(double a, double b, double c, double 
         // linear case: the reference computes -d/c into a local and never stores it
         return;
     } else if (fabs(a) < EPS) {
-        double D = c * c - 4.0 * b * d;
+        double D = fmaT(c, c, -(4.0 * b * d));
         if (D >= 0) {
             D = ccc_sqrt(D);
             double x1 = (-c + D) / (2.0 * b);
@@ -638,11 +658,13 @@ template <class T> static void solve_cubic(double a, double b, double c, double 
             double k = ccc_acos(-(g / (2 * i)));
             double L = j * -1;
             double M = ccc_cos(k / 3.0);
-            double N = ccc_sqrt(3.0) * ccc_sin(k / 3.0);
+            // N = sqrt(3) * sin(k/3) feeds M + N and M - N, and nvcc fuses both (and each
+            // result into L * (.) + P); the first root is rounded twice, as compiled
+            double sn = ccc_sin(k / 3.0);
             double P = (b / (3.0 * a)) * -1;
-            double x1 = 2 * j * ccc_cos(k / 3.0) - (b / (3.0 * a));
-            double x2 = L * (M + N) + P;
-            double x3 = L * (M - N) + P;
+            double x1 = (2 * j) * ccc_cos(k / 3.0) - (b / (3.0 * a));
+            double x2 = fmaT(L, fmaT(ccc_sqrt(3.0), sn, M), P);
+            double x3 = fmaT(L, fmaT(-ccc_sqrt(3.0), sn, M), P);
             add_root<T>(r, (T)x1, nr);
             add_root<T>(r, (T)x2, nr);
             add_root<T>(r, (T)x3, nr);
@@ -664,9 +686,9 @@ template <class T> static void solve_cubic(double a, double b, double c, double 
 template <class T> static bool is_inside(V3<T> v0, V3<T> v1, V3<T> v2, V3<T> vt) {
     V3<T> e1 = v0 - v1, e2 = v2 - v1, ep = vt - v1;
     T d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2), d20 = dot(ep, e1), d21 = dot(ep, e2);
-    T denom = d00 * d11 - d01 * d01;
-    T v = (d11 * d20 - d01 * d21) / denom;
-    T w = (d00 * d21 - d01 * d20) / denom;
+    T denom = fms2(d00, d11, d01, d01);
+    T v = fms2(d11, d20, d01, d21) / denom;
+    T w = fms2(d00, d21, d01, d20) / denom;
     T u = 1 - v - w;
     if (v < 0 || v > 1) return false;
     if (w < 0 || w > 1) return false;
@@ -674,7 +696,7 @@ template <class T> static bool is_inside(V3<T> v0, V3<T> v1, V3<T> v2, V3<T> vt)
     return true;
 }
 
-template <class T> static inline V3<T> at_time(const MTet<T>& t, int i, T root) { return t.v[i] + t.dv[i] * root; }
+template <class T> static inline V3<T> at_time(const MTet<T>& t, int i, T root) { return axpy(t.v[i], t.dv[i], root); }
 
 // filterCollisions (collisions_continuous.cu:640-684)
 template <class T> static bool ccd_filter(const MTet<T>& tet, int k, T root) {
@@ -728,7 +750,7 @@ static const double THICKNESS = 2e-3;   // collisions_impulses.cu:12-14
 
 template <class T> static inline V3<T> vnormalize(V3<T> a) {
     // normalize(double3) = a * rsqrt(|a|^2) (utils.cu:91-93); taken as a * (1 / sqrt(|a|^2))
-    T n = a.x * a.x + a.y * a.y + a.z * a.z;
+    T n = norm2(a);
     T inv = (T)1 / (T)sqrt((double)n);
     return a * inv;
 }
@@ -764,18 +786,18 @@ template <class T> static Contact<T> contact(const MTet<T>& tet, int k, T root, 
         // compute_normal_direction_edge_edge (330-447), on the t = 0 tetrahedron
         const V3<T>* v = tet.v;
         const V3<T>* dv = tet.dv;
-        V3<T> p0 = v[0] + (v[1] - v[0]) * s;
-        V3<T> p1 = v[2] + (v[3] - v[2]) * t;
-        V3<T> dp0 = dv[0] + (dv[1] - dv[0]) * s;
-        V3<T> dp1 = dv[2] + (dv[3] - dv[2]) * t;
-        V3<T> c0 = v[0] + dv[0] * root, c1 = v[1] + dv[1] * root, c2 = v[2] + dv[2] * root;
+        V3<T> p0 = axpy(v[0], v[1] - v[0], s);
+        V3<T> p1 = axpy(v[2], v[3] - v[2], t);
+        V3<T> dp0 = axpy(dv[0], dv[1] - dv[0], s);
+        V3<T> dp1 = axpy(dv[2], dv[3] - dv[2], t);
+        V3<T> c0 = axpy(v[0], dv[0], root), c1 = axpy(v[1], dv[1], root), c2 = axpy(v[2], dv[2], root);
         V3<T> nd = vnormalize(cross(c1 - c0, c2 - c0));
         if (dot(p1 - p0, nd) < 0) nd = nd * (T)-1;
         ct.n = nd;
         ct.vn = dot(dp1 - dp0, nd);
         // compute_masses_edge_edge (449-454)
-        ct.m0 = q[0] * (1 - s) + q[1] * s;
-        ct.m1 = q[2] * (1 - t) + q[3] * t;
+        ct.m0 = fmaT(q[0], 1 - s, q[1] * s);
+        ct.m1 = fmaT(q[2], 1 - t, q[3] * t);
         return ct;
     }
     // triangle-vertex: types 9..11 face = points 0,1,2, vertex = 3; types 12..14 face =
@@ -785,20 +807,20 @@ template <class T> static Contact<T> contact(const MTet<T>& tet, int k, T root, 
     // compute_coeficients_triangle_vertex (162-193), at the collision time
     V3<T> e1 = thz.v[f0] - thz.v[f1], e2 = thz.v[f2] - thz.v[f1], ep = thz.v[fv] - thz.v[f1];
     T d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2), d20 = dot(ep, e1), d21 = dot(ep, e2);
-    T denom = d00 * d11 - d01 * d01;
+    T denom = fms2(d00, d11, d01, d01);
     T u, w, vv;
     if (fabs((double)denom) < 1e-15) { u = (T)(1. / 3.); w = (T)(1. / 3.); }
     else {
-        u = (d11 * d20 - d01 * d21) / denom;
-        w = (d00 * d21 - d01 * d20) / denom;
+        u = fms2(d11, d20, d01, d21) / denom;
+        w = fms2(d00, d21, d01, d20) / denom;
     }
     vv = 1 - u - w;
     // compute_normal_direction_triangle_vertex (196-304)
     const V3<T>* v = tet.v;
     const V3<T>* dv = tet.dv;
-    V3<T> pt = v[f0] * u + v[f1] * vv + v[f2] * w;
-    V3<T> dpt = dv[f0] * u + dv[f1] * vv + dv[f2] * w;
-    V3<T> c0 = v[f0] + dv[f0] * root, c1 = v[f1] + dv[f1] * root, c2 = v[f2] + dv[f2] * root;
+    V3<T> pt = lin3(v[f0], u, v[f1], vv, v[f2], w);
+    V3<T> dpt = lin3(dv[f0], u, dv[f1], vv, dv[f2], w);
+    V3<T> c0 = axpy(v[f0], dv[f0], root), c1 = axpy(v[f1], dv[f1], root), c2 = axpy(v[f2], dv[f2], root);
     V3<T> nd = vnormalize(cross(c1 - c0, c2 - c0));
     if (dot(v[fv] - pt, nd) < 0) nd = nd * (T)-1;
     ct.vn = dot(dv[fv] - dpt, nd);
@@ -807,9 +829,9 @@ template <class T> static Contact<T> contact(const MTet<T>& tet, int k, T root, 
     // compute_masses_triangle_vertex (456-468)
     if (inv) {
         ct.m0 = q[0];
-        ct.m1 = q[1] * u + q[2] * vv + q[3] * w;
+        ct.m1 = fmaT(q[3], w, fmaT(q[1], u, q[2] * vv));
     } else {
-        ct.m0 = q[0] * u + q[1] * vv + q[2] * w;
+        ct.m0 = fmaT(q[2], w, fmaT(q[0], u, q[1] * vv));
         ct.m1 = q[3];
     }
     return ct;
@@ -880,7 +902,7 @@ template <class T> static void pt_seg(V3<T> p, V3<T> a, V3<T> b, T dc[3], bool s
     T t = dot(ap, ab) / dot(ab, ab);
     if (t < 0.0) t = 0.0;
     if (t > 1.0) t = 1.0;
-    V3<T> c = mk<T>(a.x + t * ab.x, a.y + t * ab.y, a.z + t * ab.z);
+    V3<T> c = mk<T>(fmaT(t, ab.x, a.x), fmaT(t, ab.y, a.y), fmaT(t, ab.z, a.z));
     T nd = (T)sqrtf(sq_diff_f(p, c));
     if (nd < dc[0]) {
         dc[0] = nd;
@@ -911,18 +933,18 @@ template <class T> static T prox_distance(const Tri<T>& a, const Tri<T>& b, int 
         }
         bool sv = (s >= 0 && s <= 1), tv = (t >= 0 && t <= 1);
         if (!sv || !tv) return (T)-1;
-        return (T)sqrtf(sq_diff_f(v[0] + da * s, v[2] + db * t));
+        return (T)sqrtf(sq_diff_f(axpy(v[0], da, s), axpy(v[2], db, t)));
     }
     int f0 = k < 12 ? 0 : 1, f1 = k < 12 ? 1 : 2, f2 = k < 12 ? 2 : 3, fv = k < 12 ? 3 : 0;
     V3<T> e1 = v[f0] - v[f1], e2 = v[f2] - v[f1], ep = v[fv] - v[f1];
     T d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2), d20 = dot(ep, e1), d21 = dot(ep, e2);
-    T denom = d00 * d11 - d01 * d01;
-    T u = (d11 * d20 - d01 * d21) / denom;
-    T w = (d00 * d21 - d01 * d20) / denom;
+    T denom = fms2(d00, d11, d01, d01);
+    T u = fms2(d11, d20, d01, d21) / denom;
+    T w = fms2(d00, d21, d01, d20) / denom;
     T vv = 1 - w - u;
     bool ok = (vv >= 0 && vv <= 1) && (w >= 0 && w <= 1) && (u >= 0 && u <= 1);
     if (!ok) return (T)-1;
-    V3<T> pt = v[f0] * u + v[f1] * vv + v[f2] * w;
+    V3<T> pt = lin3(v[f0], u, v[f1], vv, v[f2], w);
     return (T)sqrtf(sq_diff_f(v[fv], pt));
 }
 
@@ -1178,6 +1200,24 @@ ORC_API void orc_cubic_coeffs(const double* tet /* v0..v3, dv0..dv3: 24 doubles 
         t.dv[i] = mk<double>(tet[12 + 3 * i], tet[12 + 3 * i + 1], tet[12 + 3 * i + 2]);
     }
     cubic_coeffs(t, c);
+}
+// root filter and contact kinematics of one tetrahedron (v0..v3, dv0..dv3) of type k
+ORC_API int orc_filter(const double* tet, int k, double root) {
+    MTet<double> t;
+    for (int i = 0; i < 4; ++i) {
+        t.v[i] = mk<double>(tet[3 * i], tet[3 * i + 1], tet[3 * i + 2]);
+        t.dv[i] = mk<double>(tet[12 + 3 * i], tet[12 + 3 * i + 1], tet[12 + 3 * i + 2]);
+    }
+    return ccd_filter(t, k, root) ? 1 : 0;
+}
+ORC_API void orc_contact(const double* tet, int k, double root, const double* q, double* out) {
+    MTet<double> t;
+    for (int i = 0; i < 4; ++i) {
+        t.v[i] = mk<double>(tet[3 * i], tet[3 * i + 1], tet[3 * i + 2]);
+        t.dv[i] = mk<double>(tet[12 + 3 * i], tet[12 + 3 * i + 1], tet[12 + 3 * i + 2]);
+    }
+    Contact<double> c = contact(t, k, root, q);
+    out[0] = c.n.x; out[1] = c.n.y; out[2] = c.n.z; out[3] = c.vn; out[4] = c.m0; out[5] = c.m1;
 }
 ORC_API int orc_sat(int dtype, const void* a, const void* b, double th) {
     if (dtype == 0) {

@@ -82,6 +82,9 @@ def lib():
             getattr(L, f).argtypes = [ctypes.c_double]
             getattr(L, f).restype = ctypes.c_double
         L.orc_cubic_coeffs.argtypes = [_P, _P]
+        L.orc_filter.argtypes = [_P, ctypes.c_int, ctypes.c_double]
+        L.orc_filter.restype = ctypes.c_int
+        L.orc_contact.argtypes = [_P, ctypes.c_int, ctypes.c_double, _P, _P]
         L.orc_sat.argtypes = [ctypes.c_int, _P, _P, ctypes.c_double]
         L.orc_sat.restype = ctypes.c_int
         L.orc_num_threads.restype = ctypes.c_int
@@ -269,6 +272,20 @@ def cubic_coeffs(tet24):
     c = np.zeros(4, dtype=np.float64)
     lib().orc_cubic_coeffs(_ptr(t), _ptr(c))
     return c
+
+
+def ccd_filter(tet24, k, root):
+    t = np.ascontiguousarray(np.asarray(tet24, dtype=np.float64).reshape(24))
+    return bool(lib().orc_filter(_ptr(t), int(k), float(root)))
+
+
+def contact(tet24, k, root, masses4):
+    """(normal (3), normal velocity, mass pair (2)) of one contact."""
+    t = np.ascontiguousarray(np.asarray(tet24, dtype=np.float64).reshape(24))
+    q = np.ascontiguousarray(np.asarray(masses4, dtype=np.float64).reshape(4))
+    o = np.zeros(6)
+    lib().orc_contact(_ptr(t), int(k), float(root), _ptr(q), _ptr(o))
+    return o
 
 
 def sat(tri_a, tri_b, threshold=0.0):

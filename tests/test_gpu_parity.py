@@ -18,6 +18,16 @@ from conftest import random_mesh_soup
 pytestmark = pytest.mark.gpu
 
 TOI_RTOL = 1e-9
+
+
+@pytest.fixture(autouse=True)
+def portable_math(cuda):
+    """The oracle shares the library's portable elementary functions, so bit-exact parity
+    is checked in that mode (the default mode calls CUDA's, as the reference does, and is
+    checked against the reference's own outputs in test_gpu_reference.py)."""
+    from cccollisions_b200 import _native as N
+    with N.math_library(N.LIB_PORTABLE):
+        yield
 IMPULSE_RTOL = 1e-6
 
 
