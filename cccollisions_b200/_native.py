@@ -1,4 +1,5 @@
-"""ctypes binding of the C ABI in ``include/ccc_b200.h`` (``libccc_b200.so``).
+"""ctypes binding of the C ABI in ``include/ccc_b200.h`` and ``include/ccc_engine.h``
+(``libccc_b200.so``).
 
 There is no fallback: if the library is missing or fails to load, every operation raises.
 """
@@ -49,7 +50,40 @@ SIGNATURES = {
     "ccc_find_collisions_continuous_static": (_I, [_I, _P, _P, _P, _P, _P, _I64, _I64, _I64, _I64, _P, _P, _P]),
     "ccc_compute_impulses_from_collisions": (_I, [_I, _P, _P, _I64, _I64, _P, _P, _P, _I64, _P, _P, _P, _P, _I64,
                                                  _P]),
+    # resident engine (include/ccc_engine.h)
+    "ccc_engine_bytes": (_I64, [_I, _I64, _I64, _I64, _I64, _I64]),
+    "ccc_engine_create": (_I, [_I, _I64, _I64, _I64, _I64, _I64, _P, _I64, _P, _P]),
+    "ccc_engine_destroy": (_I, [_P]),
+    "ccc_engine_add_mesh": (_I, [_P, _I64, _I64, _P]),
+    "ccc_engine_remove_mesh": (_I, [_P, ctypes.c_int32]),
+    "ccc_engine_mesh_view": (_I, [_P, ctypes.c_int32, _P]),
+    "ccc_engine_free_slots": (_I, [_P, _P, _P]),
+    "ccc_engine_set_active": (_I, [_P, _P, _I64, _P]),
+    "ccc_engine_build": (_I, [_P, _P, _I64, _P]),
+    "ccc_engine_ccd": (_I, [_P, _P]),
+    "ccc_engine_loop_prepare": (_I, [_P, _P, _I64, _P]),
+    "ccc_engine_loop_step": (_I, [_P, ctypes.c_int32, _P]),
+    "ccc_engine_capture": (_I, [_P, _I, ctypes.c_int32, _P]),
+    "ccc_engine_replay": (_I, [_P, _I, _P]),
+    "ccc_engine_autotune": (_I, [_P, _P, _P]),
+    "ccc_engine_read_state": (_I, [_P, _P, _I64, _P, _P, _P, _P, _P, _P]),
 }
+
+# engine constants (mirrors include/ccc_engine.h)
+CCC_MESH_DONE = 1
+CCC_MESH_CONVERGED = 2
+CCC_ST_NONFINITE = 16
+ENGINE_OP_CCD = 0
+ENGINE_OP_LOOP_STEP = 1
+
+
+class MeshView(ctypes.Structure):
+    """ccc_mesh_view"""
+    _fields_ = [("F", ctypes.c_int64), ("V", ctypes.c_int64), ("x0", ctypes.c_void_p), ("x1", ctypes.c_void_p),
+                ("masses", ctypes.c_void_p), ("faces", ctypes.c_void_p), ("verts0", ctypes.c_void_p),
+                ("verts1", ctypes.c_void_p), ("vel", ctypes.c_void_p), ("rows", ctypes.c_void_p),
+                ("times", ctypes.c_void_p)]
+
 
 _lib = None
 

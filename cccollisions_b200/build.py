@@ -2,8 +2,9 @@
 
     python -m cccollisions_b200.build
 
-Produces ``cccollisions_b200/libccc_b200.so`` from ``csrc/ccc_capi.cu`` (a single
-translation unit that includes the kernel headers).  Flags:
+Produces ``cccollisions_b200/libccc_b200.so`` from ``csrc/ccc_capi.cu`` (the reference-format
+operations) and ``csrc/ccc_engine.cu`` (the resident multi-mesh engine), which share the
+kernel headers.  Flags:
 
 * ``-gencode arch=compute_100a,code=sm_100a`` — B200 only;
 * ``-fmad=false`` — no multiply-add contraction, so every floating-point expression rounds
@@ -19,8 +20,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libccc_b200.so")
-SOURCES = ["ccc_capi.cu"]
-HEADERS = ["ccc_kernels.cuh", "ccc_geom.cuh", "ccc_libm.h", "ccc_ddmul.h"]
+SOURCES = ["ccc_capi.cu", "ccc_engine.cu"]
+HEADERS = ["ccc_kernels.cuh", "ccc_engine.cuh", "ccc_runtime.cuh", "ccc_geom.cuh", "ccc_libm.h", "ccc_ddmul.h"]
 ROOT = os.path.dirname(HERE)
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-fmad=false", "-std=c++17",
@@ -38,7 +39,8 @@ def up_to_date() -> bool:
     if not os.path.exists(LIB):
         return False
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "ccc_b200.h")]
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", h)
+                                                                  for h in ("ccc_b200.h", "ccc_engine.h")]
     return all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d))
 
 

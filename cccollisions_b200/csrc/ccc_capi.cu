@@ -11,10 +11,11 @@
 
 #include "../../include/ccc_b200.h"
 #include "ccc_kernels.cuh"
+#include "ccc_runtime.cuh"
 
 using namespace ccc;
 
-namespace {
+namespace ccc {
 
 int g_num_sms[64] = {0};
 
@@ -30,11 +31,7 @@ int num_sms() {
     return g_num_sms[dev];
 }
 
-inline int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
-
 // ---- launch accounting and optional per-kernel event timing ----
-// Every kernel launch goes through CCC_LAUNCH, which counts it and, while timing is on,
-// brackets it with CUDA events on the launching stream.
 int64_t g_launches = 0;
 // elementary functions of the continuous-collision solver (MathLib); CUDA's own by default,
 // which is what the reference calls
@@ -47,9 +44,11 @@ int g_ntimed = 0;
 cudaEvent_t g_pool[2 * MAX_TIMED];
 int g_pool_init = 0;
 
-inline void timing_before(const char* name, cudaStream_t s, int* slot) {
+void timing_before(const char* name, cudaStream_t s, int* slot) {
     *slot = -1;
     if (!g_timing || g_ntimed >= MAX_TIMED) return;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
     int i = g_ntimed++;
     if (g_pool_init <= 2 * i + 1) {
         while (g_pool_init <= 2 * i + 1) cudaEventCreate(&g_pool[g_pool_init++]);
@@ -60,24 +59,21 @@ inline void timing_before(const char* name, cudaStream_t s, int* slot) {
     cudaEventRecord(g_timed[i].a, s);
     *slot = i;
 }
-inline void timing_after(int slot, cudaStream_t s) {
+void timing_after(int slot, cudaStream_t s) {
     ++g_launches;
     if (slot >= 0) cudaEventRecord(g_timed[slot].b, s);
 }
 
-#define CCC_LAUNCH(name, s, ...)                  \
-    do {                                          \
-        int slot__;                               \
-        timing_before(name, s, &slot__);          \
-        __VA_ARGS__;                              \
-        timing_after(slot__, s);                  \
-    } while (0)
+}  // namespace ccc
+
+namespace {
 
 // Workspace layout (every section 256-byte aligned):
 //   [header 64 B][mesh counters M][visit counters total-M]   <- zeroed per call
-//   [moff M+1][rightmost total-M][nodes (total-M) x 64 B][candidates cap x 8 B]
+//   [mesh table: count, offsets M+1, data offsets M, slot ids M][rightmost total-M]
+//   [nodes total x 64 B (mesh m's F-1 nodes from slot m*F)][candidates cap x 8 B]
 struct Layout {
-    int64_t hdr, mesh_cnt, visits, zero_end, moff, rmk, nodes, cand, end;
+    int64_t hdr, mesh_cnt, visits, zero_end, moff, table, rmk, nodes, cand, end;
     int64_t cand_cap;
 };
 
@@ -90,23 +86,16 @@ Layout layout(int64_t B, int64_t F, int64_t maxc, bool need_nodes) {
     L.visits = align_up(L.mesh_cnt + B * 4, 256);
     L.zero_end = align_up(L.visits + internal * 4, 256);
     L.moff = L.zero_end;
-    L.rmk = align_up(L.moff + (B + 1) * 4, 256);
+    L.table = align_up(L.moff + (B + 1) * 4, 256);
+    L.rmk = align_up(L.table + (3 * B + 4) * 4, 256);
     L.nodes = need_nodes ? align_up(L.rmk + internal * 4, 256) : L.rmk;
-    L.cand = need_nodes ? align_up(L.nodes + internal * (int64_t)sizeof(TNode), 256) : L.nodes;
+    L.cand = need_nodes ? align_up(L.nodes + total * (int64_t)sizeof(TNode), 256) : L.nodes;
     L.cand_cap = need_nodes ? total * maxc : 0;
     L.end = align_up(L.cand + L.cand_cap * 8, 256);
     return L;
 }
 
-inline int grid_for(int64_t n, int threads) { return (int)((n + threads - 1) / threads); }
-
 inline int narrow_grid() { return num_sms() * 8; }
-
-#define CCC_LAUNCH_CHECK()                                         \
-    do {                                                           \
-        cudaError_t e__ = cudaGetLastError();                      \
-        if (e__ != cudaSuccess) return CCC_ERR_CUDA;               \
-    } while (0)
 
 int check_common(int dtype, int64_t B, int64_t F) {
     if (dtype != 0 && dtype != 1) return CCC_ERR_INVALID_ARG;
@@ -126,6 +115,8 @@ struct Prepared {
     int* rmk;
     TNode* nodes;
     int2* cand;
+    int* table;
+    Forest forest;
 };
 
 int prepare(void* ws, int64_t ws_bytes, int64_t B, int64_t F, int64_t maxc, bool need_nodes, cudaStream_t s,
@@ -140,8 +131,15 @@ int prepare(void* ws, int64_t ws_bytes, int64_t B, int64_t F, int64_t maxc, bool
     P.rmk = (int*)(P.base + P.L.rmk);
     P.nodes = (TNode*)(P.base + P.L.nodes);
     P.cand = (int2*)(P.base + P.L.cand);
+    P.table = (int*)(P.base + P.L.table);
+    // the packed table is stored twice over: moff (= voff) feeds the tensor-layout kernels
+    P.forest.nm = P.table;
+    P.forest.voff = P.moff;
+    P.forest.poff = P.table + 4;
+    P.forest.sid = P.table + 4 + B;
     if (cudaMemsetAsync(P.base, 0, (size_t)P.L.zero_end, s) != cudaSuccess) return CCC_ERR_CUDA;
-    CCC_LAUNCH("k_uniform_offsets", s, k_uniform_offsets<<<grid_for(B + 1, 256), 256, 0, s>>>(P.moff, (int)B, (int)F));
+    CCC_LAUNCH("k_uniform_offsets", s, k_uniform_offsets<<<grid_for(B + 1, 256), 256, 0, s>>>(
+        P.table, P.moff, P.table + 4, P.table + 4 + B, (int)B, (int)F));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -162,20 +160,21 @@ int run_broad_phase(const void* bboxes, const int64_t* tree, const uint8_t* mask
     CCC_LAUNCH_CHECK();
     int g = grid_for(total, TRAV_THREADS);
     int cap = (int)P.L.cand_cap;
+    TensorLeaves<T> lv{bb, tr};
     if (mask) {
         if (exact_f32)
-            CCC_LAUNCH("k_traverse", s, k_traverse<T, true, true><<<g, TRAV_THREADS, 0, s>>>(P.nodes, bb, tr, P.moff, M, total, mask, th, P.cand,
-                                                                  cap, P.hdr));
+            CCC_LAUNCH("k_traverse", s, k_traverse<T, true, true><<<g, TRAV_THREADS, 0, s>>>(P.nodes, lv, P.forest, mask, th,
+                                                                                             P.cand, cap, P.hdr, nullptr));
         else
-            CCC_LAUNCH("k_traverse", s, k_traverse<T, true, false><<<g, TRAV_THREADS, 0, s>>>(P.nodes, bb, tr, P.moff, M, total, mask, th, P.cand,
-                                                                   cap, P.hdr));
+            CCC_LAUNCH("k_traverse", s, k_traverse<T, true, false><<<g, TRAV_THREADS, 0, s>>>(P.nodes, lv, P.forest, mask, th,
+                                                                                              P.cand, cap, P.hdr, nullptr));
     } else {
         if (exact_f32)
-            CCC_LAUNCH("k_traverse", s, k_traverse<T, false, true><<<g, TRAV_THREADS, 0, s>>>(P.nodes, bb, tr, P.moff, M, total, mask, th,
-                                                                   P.cand, cap, P.hdr));
+            CCC_LAUNCH("k_traverse", s, k_traverse<T, false, true><<<g, TRAV_THREADS, 0, s>>>(P.nodes, lv, P.forest, mask, th,
+                                                                                              P.cand, cap, P.hdr, nullptr));
         else
-            CCC_LAUNCH("k_traverse", s, k_traverse<T, false, false><<<g, TRAV_THREADS, 0, s>>>(P.nodes, bb, tr, P.moff, M, total, mask, th,
-                                                                    P.cand, cap, P.hdr));
+            CCC_LAUNCH("k_traverse", s, k_traverse<T, false, false><<<g, TRAV_THREADS, 0, s>>>(P.nodes, lv, P.forest, mask,
+                                                                                               th, P.cand, cap, P.hdr, nullptr));
     }
     CCC_LAUNCH_CHECK();
     return CCC_OK;
@@ -211,9 +210,8 @@ int static_impl(const void* bboxes, const int64_t* tree, const void* tri, int64_
     T th = (T)(float)threshold;
     rc = run_broad_phase<T>(bboxes, tree, nullptr, B, F, th, is_f32<T>() && th == 0, P, s);
     if (rc) return rc;
-    CCC_LAUNCH("k_static_narrow", s, k_static_narrow<T><<<narrow_grid(), NARROW_THREADS, 0, s>>>(P.cand, (int)P.L.cand_cap, P.hdr, (const T*)tri, P.moff,
-                                                                (int)B, th, (long long*)out, (int)max_collisions,
-                                                                P.mesh_cnt));
+    CCC_LAUNCH("k_static_narrow", s, k_static_narrow<T><<<narrow_grid(), NARROW_THREADS, 0, s>>>(P.cand, (int)P.L.cand_cap, P.hdr, (const T*)tri, P.forest,
+                                                                th, (long long*)out, (int)max_collisions, P.mesh_cnt));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -227,9 +225,9 @@ int ccd_impl(const void* bboxes, const int64_t* tree, const void* x0, const void
     if (rc) return rc;
     rc = run_broad_phase<T>(bboxes, tree, mask, B, F, (T)0, is_f32<T>(), P, s);
     if (rc) return rc;
-    CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_ROWS><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
-        P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.moff, (int)B, (long long*)rows, (T*)times,
-        (int)maxcol, P.mesh_cnt, nullptr, nullptr, nullptr, nullptr, g_math_lib));
+    CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_ROWS, CornerSink<T>><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
+        P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, (long long*)rows, (T*)times,
+        (int)maxcol, P.mesh_cnt, CornerSink<T>{}, g_math_lib));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -242,9 +240,9 @@ int mincol_impl(const void* bboxes, const int64_t* tree, const void* x0, const v
     if (rc) return rc;
     rc = run_broad_phase<T>(bboxes, tree, nullptr, B, F, (T)0, is_f32<T>(), P, s);
     if (rc) return rc;
-    CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_MINCOL><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
-        P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.moff, (int)B, (long long*)rows, nullptr,
-        (int)(maxc * 15), P.mesh_cnt, nullptr, nullptr, nullptr, nullptr, g_math_lib));
+    CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_MINCOL, CornerSink<T>><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
+        P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, (long long*)rows, nullptr,
+        (int)(maxc * 15), P.mesh_cnt, CornerSink<T>{}, g_math_lib));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -258,8 +256,8 @@ int prox_impl(const void* bboxes, const int64_t* tree, const void* tri, int64_t 
     T th = (T)(float)threshold;
     rc = run_broad_phase<T>(bboxes, tree, nullptr, B, F, th, is_f32<T>() && th == 0, P, s);
     if (rc) return rc;
-    CCC_LAUNCH("k_prox_narrow", s, k_prox_narrow<T><<<narrow_grid(), NARROW_THREADS, 0, s>>>(P.cand, (int)P.L.cand_cap, P.hdr, (const T*)tri, P.moff,
-                                                              (int)B, th, (long long*)rows, (int)maxc, P.mesh_cnt));
+    CCC_LAUNCH("k_prox_narrow", s, k_prox_narrow<T><<<narrow_grid(), NARROW_THREADS, 0, s>>>(P.cand, (int)P.L.cand_cap, P.hdr, (const T*)tri, P.forest,
+                                                              th, (long long*)rows, (int)maxc, P.mesh_cnt));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -273,9 +271,9 @@ int impulses_impl(const void* bboxes, const int64_t* tree, const void* x0, const
     if (rc) return rc;
     rc = run_broad_phase<T>(bboxes, tree, mask, B, F, (T)0, is_f32<T>(), P, s);
     if (rc) return rc;
-    CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_IMPULSES><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
-        P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.moff, (int)B, nullptr, nullptr, 0, P.mesh_cnt,
-        (const T*)masses, (T*)dv, (T*)dx, (int*)cnt, g_math_lib));
+    CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_IMPULSES, CornerSink<T>><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
+        P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, nullptr, nullptr, 0, P.mesh_cnt,
+        CornerSink<T>{(const T*)masses, (T*)dv, (T*)dx, (int*)cnt}, g_math_lib));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }

@@ -1,0 +1,533 @@
+// ccc_engine.cuh — kernels of the resident multi-mesh engine.
+//
+// The engine keeps many meshes of uneven size on the device at once, each in its own
+// slot range of one arena, and runs every step over a device-resident mesh table
+// (Forest), so one captured launch sequence serves whatever meshes are active.
+//
+// Per mesh, the tree is a Karras radix tree over 30-bit Morton codes of the triangles'
+// swept centroids, normalised by the mesh's own centroid bounds, sorted by a stable LSD
+// radix sort (keys: mesh index above the code, so one sort orders every mesh at once).
+// Topology is built once; every step only refits the boxes, bottom-up, straight into the
+// traversal nodes (TNode, fp32 rounded outward).  The exact (T precision) leaf boxes are
+// kept beside them for the leaf recheck, so the candidate pairs are exactly the pairs
+// whose T-precision swept boxes overlap, as in the reference's traversal.
+//
+// The impulse loop adds a vertex arena: faces map triangle corners to vertices, contacts
+// add their impulses to per-vertex fixed-point accumulators (integer atomics, so the sums
+// do not depend on the order the contacts arrive in), and the averaged corrections move
+// the vertices, after which the end-of-step triangle soup is regathered.
+#pragma once
+
+#include "ccc_kernels.cuh"
+
+namespace ccc {
+
+// non-finite impulse skipped by the loop accumulators
+static constexpr int ST_NONFINITE = 16;
+
+// Vertex arena of the mesh table: dense vertex prefix (M + 1) and vertex data bases (M).
+struct VertTable {
+    const int* vvoff;
+    const int* vpoff;
+};
+
+// ---------------------------------------------------------------------------------------
+// Tree build
+
+// order-preserving map of floats to unsigned ints, for atomicMin / atomicMax
+__device__ __forceinline__ unsigned f2ord(float f) {
+    unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord2f(unsigned u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+template <class T> __device__ __forceinline__ float3 swept_centroid(const T* x0, const T* x1, long long slot) {
+    const T* a = x0 + slot * 9;
+    const T* b = x1 + slot * 9;
+    T c[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) c[d] = ((a[d] + a[3 + d] + a[6 + d]) + (b[d] + b[3 + d] + b[6 + d])) / (T)6;
+    return make_float3((float)c[0], (float)c[1], (float)c[2]);
+}
+
+// per-mesh centroid bounds (6 ordered words per slot id: min xyz, max xyz; the caller sets
+// the min words to 0xffffffff and the max words to 0 first)
+template <class T>
+__global__ void k_mesh_bounds(Forest F, const T* __restrict__ x0, const T* __restrict__ x1,
+                              unsigned* __restrict__ bounds) {
+    const int M = forest_size(F);
+    const int total = __ldg(F.voff + M);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
+        int m = find_mesh(F.voff, M, v, 0);
+        long long slot = (long long)__ldg(F.poff + m) + (v - __ldg(F.voff + m));
+        float3 c = swept_centroid(x0, x1, slot);
+        cg::coalesced_group act = cg::coalesced_threads();
+        cg::coalesced_group grp = cg::labeled_partition(act, m);
+        float lo[3] = {c.x, c.y, c.z}, hi[3] = {c.x, c.y, c.z};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = cg::reduce(grp, lo[d], cg::less<float>());
+            hi[d] = cg::reduce(grp, hi[d], cg::greater<float>());
+        }
+        if (grp.thread_rank() == 0) {
+            unsigned* b = bounds + 6 * __ldg(F.sid + m);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                atomicMin(b + d, f2ord(lo[d]));
+                atomicMax(b + 3 + d, f2ord(hi[d]));
+            }
+        }
+    }
+}
+
+// 10 bits of x spread to every third bit (bit i -> bit 3i)
+__device__ __forceinline__ unsigned spread3(unsigned x) {
+    x &= 0x3ffu;
+    x = (x | (x << 16)) & 0x030000ffu;
+    x = (x | (x << 8)) & 0x0300f00fu;
+    x = (x | (x << 4)) & 0x030c30c3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
+__device__ __forceinline__ unsigned quantize1024(float c, float lo, float hi) {
+    float ext = hi - lo;
+    float t = ext > 0.f ? (c - lo) / ext : 0.f;
+    float q = fminf(fmaxf(t * 1024.f, 0.f), 1023.f);
+    return (unsigned)q;
+}
+
+// sort keys (mesh index << 30 | Morton code) and values (mesh-local triangle id)
+template <class T>
+__global__ void k_morton(Forest F, const T* __restrict__ x0, const T* __restrict__ x1,
+                         const unsigned* __restrict__ bounds, unsigned long long* __restrict__ keys,
+                         int* __restrict__ vals) {
+    const int M = forest_size(F);
+    const int total = __ldg(F.voff + M);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
+        int m = find_mesh(F.voff, M, v, 0);
+        int local = v - __ldg(F.voff + m);
+        float3 c = swept_centroid(x0, x1, (long long)__ldg(F.poff + m) + local);
+        const unsigned* b = bounds + 6 * __ldg(F.sid + m);
+        unsigned qx = quantize1024(c.x, ord2f(b[0]), ord2f(b[3]));
+        unsigned qy = quantize1024(c.y, ord2f(b[1]), ord2f(b[4]));
+        unsigned qz = quantize1024(c.z, ord2f(b[2]), ord2f(b[5]));
+        unsigned code = (spread3(qx) << 2) | (spread3(qy) << 1) | spread3(qz);
+        keys[v] = ((unsigned long long)m << 30) | code;
+        vals[v] = local;
+    }
+}
+
+// ---- stable LSD radix sort, 8-bit digits: histogram, scan, scatter per pass ----
+static constexpr int SORT_THREADS = 256;
+static constexpr int SORT_ROUNDS = 8;
+static constexpr int SORT_TILE = SORT_THREADS * SORT_ROUNDS;
+
+// counts[d * nblk + b] = number of keys of tile b with digit d
+static __global__ void __launch_bounds__(SORT_THREADS)
+k_radix_hist(const unsigned long long* __restrict__ keys, int n, int shift, int* __restrict__ counts, int nblk) {
+    __shared__ int h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    long long base = (long long)blockIdx.x * SORT_TILE;
+    for (int r = 0; r < SORT_ROUNDS; ++r) {
+        long long i = base + r * SORT_THREADS + threadIdx.x;
+        if (i < n) atomicAdd(&h[(keys[i] >> shift) & 255], 1);
+    }
+    __syncthreads();
+    counts[(long long)threadIdx.x * nblk + blockIdx.x] = h[threadIdx.x];
+}
+
+// exclusive prefix sum of len ints in place, one block of 1024 threads
+static __global__ void __launch_bounds__(1024) k_exclusive_scan(int* __restrict__ a, int len) {
+    __shared__ int part[1024];
+    const int t = threadIdx.x;
+    const int chunk = (len + 1023) / 1024;
+    const long long lo = (long long)t * chunk;
+    const long long hi = min((long long)len, lo + chunk);
+    int sum = 0;
+    for (long long i = lo; i < hi; ++i) sum += a[i];
+    part[t] = sum;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        int v = t >= o ? part[t - o] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int run = part[t] - sum;
+    for (long long i = lo; i < hi; ++i) {
+        int c = a[i];
+        a[i] = run;
+        run += c;
+    }
+}
+
+// stable scatter: keys of tile b with digit d go to offs[d * nblk + b] onwards, in input order
+static __global__ void __launch_bounds__(SORT_THREADS)
+k_radix_scatter(const unsigned long long* __restrict__ kin, const int* __restrict__ vin,
+                unsigned long long* __restrict__ kout, int* __restrict__ vout, int n, int shift,
+                const int* __restrict__ offs, int nblk) {
+    constexpr int WARPS = SORT_THREADS / 32;
+    __shared__ int whist[WARPS][256];
+    __shared__ int base[256];
+    __shared__ int round_total[256];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    base[t] = offs[(long long)t * nblk + blockIdx.x];
+    const unsigned lt = (1u << lane) - 1u;
+    for (int r = 0; r < SORT_ROUNDS; ++r) {
+        long long i = (long long)blockIdx.x * SORT_TILE + r * SORT_THREADS + t;
+        bool valid = i < n;
+        unsigned long long key = valid ? kin[i] : 0ull;
+        int d = valid ? (int)((key >> shift) & 255) : 256;
+        for (int j = t; j < WARPS * 256; j += SORT_THREADS) (&whist[0][0])[j] = 0;
+        __syncthreads();
+        unsigned peers = __match_any_sync(0xffffffffu, d);
+        int rank = __popc(peers & lt);
+        if (valid && rank == 0) whist[w][d] = __popc(peers);
+        __syncthreads();
+        {
+            int run = 0;
+            for (int ww = 0; ww < WARPS; ++ww) {
+                int c = whist[ww][t];
+                whist[ww][t] = run;
+                run += c;
+            }
+            round_total[t] = run;
+        }
+        __syncthreads();
+        if (valid) {
+            int pos = base[d] + whist[w][d] + rank;
+            kout[pos] = key;
+            vout[pos] = vin[i];
+        }
+        __syncthreads();
+        base[t] += round_total[t];
+        __syncthreads();
+    }
+}
+
+// Karras radix tree over the sorted codes of each mesh (Karras 2012, "Maximizing Parallelism
+// in the Construction of BVHs, Octrees, and k-d Trees"), equal codes ordered by position.
+// Writes the child references of every internal node (ref >= 0 internal node, ~pos leaf),
+// their aux words (rightmost leaf position of an internal child, triangle id of a leaf),
+// the parent codes ((parent << 1) | side) of nodes and leaves and the leaf -> triangle map,
+// and clears the refit counters.
+__device__ __forceinline__ int karras_delta(const unsigned long long* k, int n, int i, int j) {
+    if (j < 0 || j > n - 1) return -1;
+    unsigned a = (unsigned)(k[i] & 0x3fffffffull), b = (unsigned)(k[j] & 0x3fffffffull);
+    return a == b ? 32 + __clz(i ^ j) : __clz(a ^ b);
+}
+
+static __global__ void k_karras_build(Forest F, const unsigned long long* __restrict__ keys,
+                                      const int* __restrict__ vals, TNode* __restrict__ nodes,
+                                      int* __restrict__ nparent, int* __restrict__ lparent,
+                                      int* __restrict__ leaf_tri, unsigned* __restrict__ visits,
+                                      int* __restrict__ status) {
+    const int M = forest_size(F);
+    const int total_internal = __ldg(F.voff + M) - M;
+    for (int gi = blockIdx.x * blockDim.x + threadIdx.x; gi < total_internal; gi += gridDim.x * blockDim.x) {
+        int m = find_mesh(F.voff, M, gi, 1);
+        int vo = __ldg(F.voff + m), po = __ldg(F.poff + m);
+        int n = __ldg(F.voff + m + 1) - vo;
+        int i = gi - (vo - m);
+        const unsigned long long* k = keys + vo;
+        int d = (karras_delta(k, n, i, i + 1) - karras_delta(k, n, i, i - 1)) >= 0 ? 1 : -1;
+        int dmin = karras_delta(k, n, i, i - d);
+        int lmax = 2;
+        for (int g = 0; g < 32 && karras_delta(k, n, i, i + lmax * d) > dmin; ++g) lmax *= 2;
+        int l = 0;
+        for (int t = lmax / 2; t >= 1; t /= 2)
+            if (karras_delta(k, n, i, i + (l + t) * d) > dmin) l += t;
+        int j = i + l * d;
+        int dnode = karras_delta(k, n, i, j);
+        int s = 0;
+        for (int t = l;;) {
+            t = (t + 1) >> 1;
+            if (karras_delta(k, n, i, i + (s + t) * d) > dnode) s += t;
+            if (t <= 1) break;
+        }
+        int split = i + s * d + min(d, 0);
+        int lo = min(i, j), hi = max(i, j);
+        if (split < lo || split + 1 > hi) {      // cannot happen for a valid sort
+            atomicOr(status, ST_MALFORMED_TREE);
+            continue;
+        }
+        int lref, rref, laux, raux;
+        if (lo == split) {
+            lref = ~split;
+            laux = __ldg(vals + vo + split);
+            lparent[po + split] = (i << 1) | 0;
+            leaf_tri[po + split] = laux;
+        } else {
+            lref = split;
+            laux = split;
+            nparent[po + split] = (i << 1) | 0;
+        }
+        if (hi == split + 1) {
+            rref = ~(split + 1);
+            raux = __ldg(vals + vo + split + 1);
+            lparent[po + split + 1] = (i << 1) | 1;
+            leaf_tri[po + split + 1] = raux;
+        } else {
+            rref = split + 1;
+            raux = hi;
+            nparent[po + split + 1] = (i << 1) | 1;
+        }
+        nodes[po + i].d = make_int4(lref, rref, laux, raux);
+        visits[po + i] = 0u;
+        if (i == 0) nparent[po] = -1;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Refit: exact swept leaf boxes, then the fp32 child boxes of every node, bottom-up.
+
+template <class T> __device__ __forceinline__ void box_outward_f32(const Box<T>& b, float lo[3], float hi[3]) {
+    T l[3] = {b.lo.x, b.lo.y, b.lo.z}, h[3] = {b.hi.x, b.hi.y, b.hi.z};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        if (sizeof(T) == 4) {
+            lo[c] = (float)l[c];
+            hi[c] = (float)h[c];
+        } else {
+            lo[c] = __double2float_rd((double)l[c]);
+            hi[c] = __double2float_ru((double)h[c]);
+        }
+    }
+}
+
+// child slot `side` of node: left = a.xyzw b.xy, right = b.zw c.xyzw
+__device__ __forceinline__ void write_child_box(TNode* nd, int side, const float lo[3], const float hi[3]) {
+    float4* f = reinterpret_cast<float4*>(nd);
+    float2* h = reinterpret_cast<float2*>(nd);
+    if (side == 0) {
+        f[0] = make_float4(lo[0], lo[1], lo[2], hi[0]);
+        h[2] = make_float2(hi[1], hi[2]);
+    } else {
+        h[3] = make_float2(lo[0], lo[1]);
+        f[2] = make_float4(lo[2], hi[0], hi[1], hi[2]);
+    }
+}
+
+// union of both child boxes of node, read through L2 (written by other blocks)
+__device__ __forceinline__ void node_box(const TNode* nd, float lo[3], float hi[3]) {
+    const float4* f = reinterpret_cast<const float4*>(nd);
+    float4 A = __ldcg(f + 0), B = __ldcg(f + 1), C = __ldcg(f + 2);
+    lo[0] = fminf(A.x, B.z); lo[1] = fminf(A.y, B.w); lo[2] = fminf(A.z, C.x);
+    hi[0] = fmaxf(A.w, C.y); hi[1] = fmaxf(B.x, C.z); hi[2] = fmaxf(B.y, C.w);
+}
+
+// Every node is reached twice per refit; the refit counters only ever grow, and the
+// arrival that finds an odd count is the second one, so nothing has to be cleared between
+// steps.  Meshes with MF_DONE set in mflags (when given) are skipped.
+template <class T>
+__global__ void k_engine_refit(Forest F, const T* __restrict__ x0, const T* __restrict__ x1,
+                               const int* __restrict__ leaf_tri, const int* __restrict__ lparent,
+                               const int* __restrict__ nparent, TNode* nodes, unsigned* visits, T* __restrict__ lbox,
+                               const int* __restrict__ mflags, int* status) {
+    const int M = forest_size(F);
+    const int total = __ldg(F.voff + M);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
+        int m = find_mesh(F.voff, M, v, 0);
+        int vo = __ldg(F.voff + m), po = __ldg(F.poff + m);
+        int n = __ldg(F.voff + m + 1) - vo;
+        if (n < 2) continue;
+        if (mflags && (__ldg(mflags + __ldg(F.sid + m)) & MF_DONE)) continue;
+        int p = v - vo;
+        int t = __ldg(leaf_tri + po + p);
+        if (t < 0 || t >= n) { atomicOr(status, ST_MALFORMED_TREE); continue; }
+        long long slot = (long long)po + t;
+        Box<T> b = merge(tri_box(load_tri(x0, slot)), tri_box(load_tri(x1, slot)));
+        store_box(lbox + ((long long)po + p) * 6, b);
+        float lo[3], hi[3];
+        box_outward_f32(b, lo, hi);
+        TNode* nd = nodes + po;
+        int code = __ldg(lparent + po + p);
+        for (int guard = 0; guard < n; ++guard) {
+            int node = code >> 1;
+            if (code < 0 || node >= n - 1) { atomicOr(status, ST_MALFORMED_TREE); break; }
+            write_child_box(nd + node, code & 1, lo, hi);
+            __threadfence();
+            if ((atomicAdd(visits + po + node, 1u) & 1u) == 0u) break;     // first arrival
+            node_box(nd + node, lo, hi);
+            code = __ldg(nparent + po + node);
+            if (code < 0) break;                                           // root done
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Impulse loop
+
+static constexpr double FIX_SCALE = 72057594037927936.0;        // 2^56
+static constexpr double FIX_INV = 1.3877787807814457e-17;       // 2^-56
+static constexpr double FIX_LIMIT = 64.0;
+
+// fixed-point value of one impulse component (|x| < 64), 0 and false when out of range
+__device__ __forceinline__ bool to_fix(double x, long long& q) {
+    if (!(fabs(x) < FIX_LIMIT)) return false;
+    q = __double2ll_rn(x * FIX_SCALE);
+    return true;
+}
+
+// the contact's four point impulses, added to the vertices they move
+template <class T>
+__device__ __forceinline__ void loop_impulse(const MTet<T>& tet, long long gi, long long gj, int k, T root,
+                                             const Contact<T>& ct, int m, const int* faces, const VertTable& vt,
+                                             long long* acc, int* status) {
+    ImpulseScale<T> sc = impulse_scale(ct, root);
+    const int vbase = __ldg(vt.vpoff + m);
+    const int nv = __ldg(vt.vvoff + m + 1) - __ldg(vt.vvoff + m);
+#pragma unroll 1
+    for (int pt = 0; pt < 4; ++pt) {
+        V3<T> imp, idx;
+        impulse_point(tet, k, pt, ct, sc, imp, idx);
+        long long tri = tet_side(k, pt) ? gj : gi;
+        int corner = tet_corner(k, pt);
+        long long q[6];
+        bool ok = to_fix((double)idx.x, q[0]) && to_fix((double)idx.y, q[1]) && to_fix((double)idx.z, q[2]) &&
+                  to_fix((double)imp.x, q[3]) && to_fix((double)imp.y, q[4]) && to_fix((double)imp.z, q[5]);
+        if (!ok) {
+            atomicOr(status, ST_NONFINITE);
+            continue;
+        }
+        int vid = __ldg(faces + tri * 3 + corner);
+        if (vid < 0 || vid >= nv) {
+            atomicOr(status, ST_MALFORMED_TREE);
+            continue;
+        }
+        long long vslot = (long long)vbase + vid;
+        unsigned long long* a = reinterpret_cast<unsigned long long*>(acc + vslot * 8);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) atomicAdd(a + c, (unsigned long long)q[c]);
+        atomicAdd(a + 6, 1ull);
+    }
+}
+
+// Receiver of the impulses of the engine's loop iteration: counts the contacts of each mesh
+// and adds their impulses to the per-vertex accumulators.
+template <class T> struct LoopSink {
+    const T* masses;       // 3 per triangle slot
+    const int* faces;      // 3 mesh-local vertex ids per triangle slot
+    VertTable vt;
+    long long* acc;        // 8 words per vertex slot: dx xyz, dv xyz, count, unused
+    int* contacts;         // per slot id
+    __device__ __forceinline__ void add(const MTet<T>& tet, long long gi, long long gj, int k, T root,
+                                        const Contact<T>& ct, const Forest& F, int M, int* status) const {
+        int m = forest_slot_mesh(F, M, gi);
+        atomicAdd(contacts + __ldg(F.sid + m), 1);
+        loop_impulse(tet, gi, gj, k, root, ct, m, faces, vt, acc, status);
+    }
+};
+
+// after a loop iteration's collision check: a mesh without contacts has converged; one with
+// contacts takes this iteration's corrections and stops at max_iter iterations
+static __global__ void k_loop_update(Forest F, const int* __restrict__ contacts, int* __restrict__ iters,
+                                     int* __restrict__ flags, int max_iter) {
+    const int M = forest_size(F);
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+        int sid = __ldg(F.sid + m);
+        int f = flags[sid];
+        if (f & MF_DONE) continue;
+        if (contacts[sid] == 0) {
+            flags[sid] = f | MF_DONE | MF_CONVERGED;
+        } else {
+            int it = iters[sid] + 1;
+            iters[sid] = it;
+            if (it >= max_iter) flags[sid] = f | MF_DONE;
+        }
+    }
+}
+
+// average correction of every vertex touched this iteration; clears the accumulators
+template <class T>
+__global__ void k_loop_apply(Forest F, VertTable vt, const int* __restrict__ contacts, long long* __restrict__ acc,
+                             T* __restrict__ verts1, T* __restrict__ vel) {
+    const int M = forest_size(F);
+    const int total = __ldg(vt.vvoff + M);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
+        int m = find_mesh(vt.vvoff, M, v, 0);
+        if (__ldg(contacts + __ldg(F.sid + m)) == 0) continue;
+        long long vs = (long long)__ldg(vt.vpoff + m) + (v - __ldg(vt.vvoff + m));
+        long long* a = acc + vs * 8;
+        long long cnt = a[6];
+        if (cnt == 0) continue;
+        double c = (double)cnt;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double dx = ((double)a[d] * FIX_INV) / c;
+            double dv = ((double)a[3 + d] * FIX_INV) / c;
+            verts1[vs * 3 + d] = (T)((double)verts1[vs * 3 + d] + dx);
+            vel[vs * 3 + d] = (T)((double)vel[vs * 3 + d] + dv);
+        }
+#pragma unroll
+        for (int d = 0; d < 8; ++d) a[d] = 0;
+    }
+}
+
+// triangle soup of the vertices (all meshes in the table, or only those with contacts
+// this iteration when contacts is given)
+template <class T>
+__global__ void k_gather_soup(Forest F, VertTable vt, const int* __restrict__ contacts, const int* __restrict__ faces,
+                              const T* __restrict__ verts, T* __restrict__ soup, int* status) {
+    const int M = forest_size(F);
+    const int total = __ldg(F.voff + M);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
+        int m = find_mesh(F.voff, M, v, 0);
+        if (contacts && __ldg(contacts + __ldg(F.sid + m)) == 0) continue;
+        long long slot = (long long)__ldg(F.poff + m) + (v - __ldg(F.voff + m));
+        long long vb = __ldg(vt.vpoff + m);
+        int nv = __ldg(vt.vvoff + m + 1) - __ldg(vt.vvoff + m);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            int vid = __ldg(faces + slot * 3 + c);
+            if (vid < 0 || vid >= nv) {
+                atomicOr(status, ST_MALFORMED_TREE);
+                continue;
+            }
+            long long vs = vb + vid;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) soup[slot * 9 + c * 3 + d] = verts[vs * 3 + d];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Per-mesh resets over a table
+
+// centroid bounds of every mesh in the table to (empty): min words high, max words low
+static __global__ void k_reset_bounds(Forest F, unsigned* __restrict__ bounds) {
+    const int M = forest_size(F);
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+        unsigned* b = bounds + 6 * __ldg(F.sid + m);
+        b[0] = b[1] = b[2] = 0xffffffffu;
+        b[3] = b[4] = b[5] = 0u;
+    }
+}
+
+// loop counters and flags of every mesh in the table
+static __global__ void k_loop_reset(Forest F, int* __restrict__ iters, int* __restrict__ flags) {
+    const int M = forest_size(F);
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+        int sid = __ldg(F.sid + m);
+        iters[sid] = 0;
+        flags[sid] = 0;
+    }
+}
+
+// vertex accumulators of every mesh in the table
+static __global__ void k_zero_acc(Forest F, VertTable vt, long long* __restrict__ acc) {
+    const int M = forest_size(F);
+    const int total = __ldg(vt.vvoff + M);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
+        int m = find_mesh(vt.vvoff, M, v, 0);
+        long long vs = (long long)__ldg(vt.vpoff + m) + (v - __ldg(vt.vvoff + m));
+#pragma unroll
+        for (int d = 0; d < 8; ++d) acc[vs * 8 + d] = 0;
+    }
+}
+
+}  // namespace ccc

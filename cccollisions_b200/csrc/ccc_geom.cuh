@@ -563,9 +563,11 @@ template <class T> __device__ __forceinline__ Contact<T> contact(const MTet<T>& 
 
 // extrapolate_impulses + extrapolate_impulses_dv (collisions_impulses.cu:609-1067): impulses of
 // one contact added to the per-corner dv / dx sums and counters (F, 3, 3) / (F, 3)
-template <class T>
-__device__ __forceinline__ void apply_impulse(const MTet<T>& tet, long long gi, long long gj, int k, T root,
-                                              const Contact<T>& ct, T* dv_out, T* dx_out, int* cnt_out) {
+// Impulse magnitudes of one contact: mag0 on the face / edge-0 side, mag1 on the other,
+// and keep = 1 - max(root - offset, 0), the share of the step left after the contact.
+template <class T> struct ImpulseScale { T mag0, mag1, keep; };
+
+template <class T> __device__ __forceinline__ ImpulseScale<T> impulse_scale(const Contact<T>& ct, T root) {
     T offset;
     if (fabs((double)ct.vn) < 1e-15) offset = (T)0.1;
     else offset = (T)((2 * CCC_THICKNESS) / (double)(-ct.vn));
@@ -574,15 +576,33 @@ __device__ __forceinline__ void apply_impulse(const MTet<T>& tet, long long gi, 
     T mf0, mf1;
     if (fabs((double)msum) < 1e-15) { mf0 = (T)0.5; mf1 = (T)0.5; }
     else { mf0 = ct.m0 / msum; mf1 = 1 - mf0; }
-    T mag0 = ct.vn * mf1;
-    T mag1 = -ct.vn * mf0;
-    T ro = (T)fmax((double)(root - offset), 0.);
+    ImpulseScale<T> sc;
+    sc.mag0 = ct.vn * mf1;
+    sc.mag1 = -ct.vn * mf0;
+    sc.keep = 1 - (T)fmax((double)(root - offset), 0.);
+    return sc;
+}
+
+// velocity change imp and position change idx of tetrahedron point pt
+template <class T>
+__device__ __forceinline__ void impulse_point(const MTet<T>& tet, int k, int pt, const Contact<T>& ct,
+                                              const ImpulseScale<T>& sc, V3<T>& imp, V3<T>& idx) {
+    T mag = (k < 9) ? (pt < 2 ? sc.mag0 : sc.mag1) : (k < 12 ? (pt < 3 ? sc.mag0 : sc.mag1) : (pt < 1 ? sc.mag0 : sc.mag1));
+    imp = ct.n * mag;
+    V3<T> nv = tet.dv[pt] + imp;
+    idx = (nv - tet.dv[pt]) * sc.keep;
+}
+
+// extrapolate_impulses + extrapolate_impulses_dv (collisions_impulses.cu:609-1067): impulses of
+// one contact added to the per-corner dv / dx sums and counters (F, 3, 3) / (F, 3)
+template <class T>
+__device__ __forceinline__ void apply_impulse(const MTet<T>& tet, long long gi, long long gj, int k, T root,
+                                              const Contact<T>& ct, T* dv_out, T* dx_out, int* cnt_out) {
+    ImpulseScale<T> sc = impulse_scale(ct, root);
 #pragma unroll
     for (int pt = 0; pt < 4; ++pt) {
-        T mag = (k < 9) ? (pt < 2 ? mag0 : mag1) : (k < 12 ? (pt < 3 ? mag0 : mag1) : (pt < 1 ? mag0 : mag1));
-        V3<T> imp = ct.n * mag;
-        V3<T> nv = tet.dv[pt] + imp;
-        V3<T> idx = (nv - tet.dv[pt]) * (1 - ro);
+        V3<T> imp, idx;
+        impulse_point(tet, k, pt, ct, sc, imp, idx);
         long long tri = tet_side(k, pt) ? gj : gi;
         int corner = tet_corner(k, pt);
         T* d = dv_out + tri * 9 + corner * 3;

@@ -25,6 +25,12 @@ enum StatusBits {
     ST_MALFORMED_TREE = 8,    // child / parent index out of range or a cycle in the tree
 };
 
+// per-mesh state flags of the resident engine's impulse loop
+enum MeshFlags {
+    MF_DONE = 1,         // the impulse loop has stopped for this mesh
+    MF_CONVERGED = 2,    // ... because a collision check found no contact
+};
+
 // Workspace header (int32 words) shared by all operations.
 struct WsHeader {
     int status;
@@ -58,11 +64,37 @@ __device__ __forceinline__ int find_mesh(const int* __restrict__ off, int M, lon
     return lo;
 }
 
+// Mesh table of the traversal and narrow-phase kernels.  Mesh m (0 <= m < *nm) owns the
+// work items [voff[m], voff[m+1]) (a dense prefix that assigns threads to meshes) and the
+// data slots [poff[m], poff[m] + F_m) of the triangle, node, leaf and per-triangle output
+// arrays (ascending and non-overlapping; poff = voff for a packed batch).  sid[m] is the
+// mesh's stable slot id, which indexes its per-mesh counters and state.  All four live in
+// device memory, so a captured launch sequence serves whatever table is current.
+struct Forest {
+    const int* nm;
+    const int* voff;
+    const int* poff;
+    const int* sid;
+};
+
+__device__ __forceinline__ int forest_size(const Forest& f) { return __ldg(f.nm); }
+
+// mesh owning data slot g (the last m with poff[m] <= g)
+__device__ __forceinline__ int forest_slot_mesh(const Forest& f, int M, long long g) {
+    return find_mesh(f.poff, M, g, 0);
+}
+
 // ---------------------------------------------------------------------------------------
-// uniform mesh offsets for the reference API (B meshes of F triangles)
-__global__ void k_uniform_offsets(int* moff, int M, int F) {
+// packed mesh table for the reference API (B meshes of F triangles): nm = B,
+// voff[i] = poff[i] = i * F, sid[i] = i
+static __global__ void k_uniform_offsets(int* nm, int* voff, int* poff, int* sid, int M, int F) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i <= M) moff[i] = i * F;
+    if (i == 0) *nm = M;
+    if (i <= M) voff[i] = i * F;
+    if (i < M) {
+        poff[i] = i * F;
+        sid[i] = i;
+    }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -100,7 +132,7 @@ __device__ __forceinline__ int delta_id(int i, int j, int n) {
 // BuildRadixTree (build_bvh.cu:74-143) for identity order.  The split search is the
 // standard Karras one (steps ceil(l/2), ceil(l/4), ..., 1), which reaches the same split
 // as the reference's loop.
-__global__ void k_karras_identity(const int* __restrict__ moff, int M, int total_internal, long long* __restrict__ tree) {
+static __global__ void k_karras_identity(const int* __restrict__ moff, int M, int total_internal, long long* __restrict__ tree) {
     int gi = blockIdx.x * blockDim.x + threadIdx.x;
     if (gi >= total_internal) return;
     int m = find_mesh(moff, M, gi, 1);
@@ -219,11 +251,11 @@ __global__ void k_import_nodes(const int* __restrict__ moff, int M, int total_in
     t.b = make_float4(hi[0][1], hi[0][2], lo[1][0], lo[1][1]);
     t.c = make_float4(lo[1][2], hi[1][0], hi[1][1], hi[1][2]);
     t.d = make_int4(ref[0], ref[1], aux[0], aux[1]);
-    nodes[gi] = t;
+    nodes[moff[m] + k] = t;      // mesh m's nodes start at its first triangle slot
 }
 
 // rightmost leaf position of every internal subtree, written into the parent's aux slot
-__global__ void k_import_rightmost(const int* __restrict__ moff, int M, int total, const long long* __restrict__ tree,
+static __global__ void k_import_rightmost(const int* __restrict__ moff, int M, int total, const long long* __restrict__ tree,
                                    TNode* nodes, int* __restrict__ visits, int* __restrict__ rmk, int* status) {
     int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= total) return;
@@ -233,21 +265,22 @@ __global__ void k_import_rightmost(const int* __restrict__ moff, int M, int tota
     int p = g - moff[m];
     long long base = 2LL * moff[m] - m;
     int ioff = moff[m] - m;
+    TNode* nd = nodes + moff[m];
     long long node = tree[(base + n - 1 + p) * 4 + 0];
     for (int guard = 0; guard < n; ++guard) {
         if (node < 0 || node >= n - 1) { atomicOr(status, ST_MALFORMED_TREE); return; }
         __threadfence();
         if (atomicAdd(visits + ioff + node, 1) == 0) return;
-        int4 d = nodes[ioff + node].d;
+        int4 d = nd[node].d;
         int rl = d.x < 0 ? ~d.x : __ldcg(rmk + ioff + d.x);
         int rr = d.y < 0 ? ~d.y : __ldcg(rmk + ioff + d.y);
         int r = max(rl, rr);
         rmk[ioff + node] = r;
         long long par = tree[(base + node) * 4 + 0];
         if (par >= 0 && par < n - 1) {
-            int4 pd = nodes[ioff + par].d;
-            if (pd.x == (int)node) nodes[ioff + par].d.z = r;
-            else nodes[ioff + par].d.w = r;
+            int4 pd = nd[par].d;
+            if (pd.x == (int)node) nd[par].d.z = r;
+            else nd[par].d.w = r;
         }
         if (node == 0) return;
         node = par;
@@ -264,93 +297,124 @@ __global__ void k_import_rightmost(const int* __restrict__ moff, int M, int tota
 __device__ __forceinline__ float nudge_down(float x) { return nextafterf(x, -INFINITY); }
 __device__ __forceinline__ float nudge_up(float x) { return nextafterf(x, INFINITY); }
 
-template <class T, bool MASKED, bool EXACT_F32>
+// Where traversal finds the leaves of mesh m (n triangles): the query's exact box and
+// triangle id, and the exact box of a hit leaf, by sorted leaf position.
+//   TensorLeaves: the reference's exported tensors; mesh m's rows start at 2 voff[m] - m.
+//   SceneLeaves: resident arrays indexed by data slot poff[m] + position.
+template <class T> struct TensorLeaves {
+    const T* bboxes;
+    const long long* tree;
+    __device__ __forceinline__ long long row(int m, int vo, int n, int pos) const {
+        return 2LL * vo - m + (n - 1) + pos;
+    }
+    __device__ __forceinline__ Box<T> box(int m, int vo, int po, int n, int pos) const {
+        return load_box(bboxes + row(m, vo, n, pos) * 6);
+    }
+    __device__ __forceinline__ long long id(int m, int vo, int po, int n, int pos) const {
+        return tree[row(m, vo, n, pos) * 4 + 3];
+    }
+};
+template <class T> struct SceneLeaves {
+    const T* lbox;          // 6 values per leaf slot: min xyz, max xyz
+    const int* leaf_tri;    // mesh-local triangle id per leaf slot
+    __device__ __forceinline__ Box<T> box(int m, int vo, int po, int n, int pos) const {
+        return load_box(lbox + (long long)(po + pos) * 6);
+    }
+    __device__ __forceinline__ long long id(int m, int vo, int po, int n, int pos) const {
+        return __ldg(leaf_tri + po + pos);
+    }
+};
+
+template <class T, bool MASKED, bool EXACT_F32, class Leaves>
 __global__ void __launch_bounds__(TRAV_THREADS)
-k_traverse(const TNode* __restrict__ nodes, const T* __restrict__ bboxes, const long long* __restrict__ tree,
-           const int* __restrict__ moff, int M, int total, const uint8_t* __restrict__ mask, T th,
-           int2* __restrict__ cand, int cand_cap, WsHeader* hdr) {
+k_traverse(const TNode* __restrict__ nodes, Leaves leaves, Forest F, const uint8_t* __restrict__ mask, T th,
+           int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const int* __restrict__ mflags) {
     __shared__ int stack[STACK_DEPTH][TRAV_THREADS];
     const int tid = threadIdx.x;
-    int g = blockIdx.x * blockDim.x + tid;
-    if (g >= total) return;
-    if (MASKED && !mask[g]) return;
-    int m = find_mesh(moff, M, g, 0);
-    int n = moff[m + 1] - moff[m];
-    if (n < 2) return;
-    int p = g - moff[m];
-    long long base = 2LL * moff[m] - m;
-    const TNode* nd = nodes + (moff[m] - m);
-    long long qrow = base + n - 1 + p;
-    Box<T> q = load_box(bboxes + qrow * 6);
-    long long qid64 = tree[qrow * 4 + 3];
-    if (qid64 < 0 || qid64 >= n) {
-        atomicOr(&hdr->status, ST_MALFORMED_TREE);
-        return;
-    }
-    int qid = (int)qid64;
-    // conservative fp32 query box: threshold folded in, rounded outward, nudged one more ulp
-    float qlo[3], qhi[3];
-    {
-        T lo[3] = {q.lo.x, q.lo.y, q.lo.z}, hi[3] = {q.hi.x, q.hi.y, q.hi.z};
-        for (int c = 0; c < 3; ++c) {
-            if (EXACT_F32) {
-                qlo[c] = (float)lo[c];
-                qhi[c] = (float)hi[c];
-            } else {
-                qlo[c] = nudge_down(__double2float_rd((double)lo[c] - (double)th));
-                qhi[c] = nudge_up(__double2float_ru((double)hi[c] + (double)th));
+    const int M = forest_size(F);
+    const int total = __ldg(F.voff + M);
+    for (int v = blockIdx.x * blockDim.x + tid; v < total; v += gridDim.x * blockDim.x) {
+        int m = find_mesh(F.voff, M, v, 0);
+        int vo = __ldg(F.voff + m), po = __ldg(F.poff + m);
+        int n = __ldg(F.voff + m + 1) - vo;
+        int p = v - vo;
+        if (n < 2) continue;
+        if (MASKED && !mask[po + p]) continue;
+        if (mflags && (__ldg(mflags + __ldg(F.sid + m)) & MF_DONE)) continue;
+        const TNode* nd = nodes + po;
+        Box<T> q = leaves.box(m, vo, po, n, p);
+        long long qid64 = leaves.id(m, vo, po, n, p);
+        if (qid64 < 0 || qid64 >= n) {
+            atomicOr(&hdr->status, ST_MALFORMED_TREE);
+            continue;
+        }
+        int qid = (int)qid64;
+        // conservative fp32 query box: threshold folded in, rounded outward, nudged one more ulp
+        float qlo[3], qhi[3];
+        {
+            T lo[3] = {q.lo.x, q.lo.y, q.lo.z}, hi[3] = {q.hi.x, q.hi.y, q.hi.z};
+            for (int c = 0; c < 3; ++c) {
+                if (EXACT_F32) {
+                    qlo[c] = (float)lo[c];
+                    qhi[c] = (float)hi[c];
+                } else {
+                    qlo[c] = nudge_down(__double2float_rd((double)lo[c] - (double)th));
+                    qhi[c] = nudge_up(__double2float_ru((double)hi[c] + (double)th));
+                }
             }
         }
-    }
-    int sp = 0;
-    int node = 0;
-    const int limit = 4 * n + 64;
-    for (int it = 0;; ++it) {
-        if (it > limit) { atomicOr(&hdr->status, ST_MALFORMED_TREE); break; }
-        const float4* np = reinterpret_cast<const float4*>(nd + node);
-        float4 A = __ldg(np + 0), B = __ldg(np + 1), C = __ldg(np + 2);
-        int4 D = __ldg(reinterpret_cast<const int4*>(np + 3));
-        bool ol = (qlo[0] <= A.w) && (qhi[0] >= A.x) && (qlo[1] <= B.x) && (qhi[1] >= A.y) && (qlo[2] <= B.y) &&
-                  (qhi[2] >= A.z);
-        bool orr = (qlo[0] <= C.y) && (qhi[0] >= B.z) && (qlo[1] <= C.z) && (qhi[1] >= B.w) && (qlo[2] <= C.w) &&
-                   (qhi[2] >= C.x);
-        if (!MASKED) {
-            int rml = D.x < 0 ? ~D.x : D.z;
-            int rmr = D.y < 0 ? ~D.y : D.w;
-            if (p >= rml) ol = false;
-            if (p >= rmr) orr = false;
-        }
+        int sp = 0;
+        int node = 0;
+        const int limit = 4 * n + 64;
+        for (int it = 0;; ++it) {
+            if (it > limit) { atomicOr(&hdr->status, ST_MALFORMED_TREE); break; }
+            const float4* np = reinterpret_cast<const float4*>(nd + node);
+            float4 A = __ldg(np + 0), B = __ldg(np + 1), C = __ldg(np + 2);
+            int4 D = __ldg(reinterpret_cast<const int4*>(np + 3));
+            // child references inside this mesh: internal < n - 1, leaf position < n
+            if (D.x >= n - 1 || D.y >= n - 1 || ~D.x >= n || ~D.y >= n) {
+                atomicOr(&hdr->status, ST_MALFORMED_TREE);
+                break;
+            }
+            bool ol = (qlo[0] <= A.w) && (qhi[0] >= A.x) && (qlo[1] <= B.x) && (qhi[1] >= A.y) && (qlo[2] <= B.y) &&
+                      (qhi[2] >= A.z);
+            bool orr = (qlo[0] <= C.y) && (qhi[0] >= B.z) && (qlo[1] <= C.z) && (qhi[1] >= B.w) && (qlo[2] <= C.w) &&
+                       (qhi[2] >= C.x);
+            if (!MASKED) {
+                int rml = D.x < 0 ? ~D.x : D.z;
+                int rmr = D.y < 0 ? ~D.y : D.w;
+                if (p >= rml) ol = false;
+                if (p >= rmr) orr = false;
+            }
 #pragma unroll
-        for (int s = 0; s < 2; ++s) {
-            int ref = s ? D.y : D.x;
-            bool hit = (s ? orr : ol) && ref < 0;
-            if (hit) {
-                int cpos = ~ref;
-                int cid = s ? D.w : D.z;
-                if (MASKED && mask[moff[m] + cid] && !(qid < cid)) hit = false;
-                if (hit && !EXACT_F32) {
-                    Box<T> cb = load_box(bboxes + (base + n - 1 + cpos) * 6);
-                    hit = overlap(q, cb, th);
-                }
+            for (int s = 0; s < 2; ++s) {
+                int ref = s ? D.y : D.x;
+                bool hit = (s ? orr : ol) && ref < 0;
                 if (hit) {
-                    cg::coalesced_group grp = cg::coalesced_threads();
-                    int slot = 0;
-                    if (grp.thread_rank() == 0) slot = atomicAdd(&hdr->cand_count, (int)grp.size());
-                    slot = grp.shfl(slot, 0) + grp.thread_rank();
-                    if (slot < cand_cap) cand[slot] = make_int2(moff[m] + min(qid, cid), moff[m] + max(qid, cid));
-                    else atomicOr(&hdr->status, ST_CAND_OVERFLOW);
+                    int cpos = ~ref;
+                    int cid = s ? D.w : D.z;
+                    if (MASKED && mask[po + cid] && !(qid < cid)) hit = false;
+                    if (hit && !EXACT_F32) hit = overlap(q, leaves.box(m, vo, po, n, cpos), th);
+                    if (hit) {
+                        cg::coalesced_group grp = cg::coalesced_threads();
+                        int slot = 0;
+                        if (grp.thread_rank() == 0) slot = atomicAdd(&hdr->cand_count, (int)grp.size());
+                        slot = grp.shfl(slot, 0) + grp.thread_rank();
+                        if (slot < cand_cap) cand[slot] = make_int2(po + min(qid, cid), po + max(qid, cid));
+                        else atomicOr(&hdr->status, ST_CAND_OVERFLOW);
+                    }
                 }
             }
-        }
-        bool tl = ol && D.x >= 0, tr = orr && D.y >= 0;
-        if (!tl && !tr) {
-            if (sp == 0) break;
-            node = stack[--sp][tid];
-        } else {
-            node = tl ? D.x : D.y;
-            if (tl && tr) {
-                if (sp >= STACK_DEPTH) { atomicOr(&hdr->status, ST_STACK_OVERFLOW); break; }
-                stack[sp++][tid] = D.y;
+            bool tl = ol && D.x >= 0, tr = orr && D.y >= 0;
+            if (!tl && !tr) {
+                if (sp == 0) break;
+                node = stack[--sp][tid];
+            } else {
+                node = tl ? D.x : D.y;
+                if (tl && tr) {
+                    if (sp >= STACK_DEPTH) { atomicOr(&hdr->status, ST_STACK_OVERFLOW); break; }
+                    stack[sp++][tid] = D.y;
+                }
             }
         }
     }
@@ -359,12 +423,27 @@ k_traverse(const TNode* __restrict__ nodes, const T* __restrict__ bboxes, const 
 // ---------------------------------------------------------------------------------------
 // Narrow phases.  Grid-stride over the candidate buffer; the count is read on the device.
 
+// Output region of the mesh that owns data slot g: rows [poff[m] * per_tri, ... + F_m * per_tri)
+struct OutRegion {
+    int m;              // table index
+    int po;             // first data slot
+    long long cap;      // F_m * per_tri
+};
+__device__ __forceinline__ OutRegion out_region(const Forest& F, int M, long long g, int per_tri) {
+    OutRegion r;
+    r.m = forest_slot_mesh(F, M, g);
+    r.po = __ldg(F.poff + r.m);
+    r.cap = (long long)(__ldg(F.voff + r.m + 1) - __ldg(F.voff + r.m)) * per_tri;
+    return r;
+}
+
 // per-mesh append of one row; returns the row index within the mesh region or -1 when full
-__device__ __forceinline__ long long append_row(int* mesh_counters, int m, long long cap, int* status) {
+__device__ __forceinline__ long long append_row(int* mesh_counters, const Forest& F, int m, long long cap,
+                                                int* status) {
     cg::coalesced_group act = cg::coalesced_threads();
     cg::coalesced_group grp = cg::labeled_partition(act, m);
     int slot = 0;
-    if (grp.thread_rank() == 0) slot = atomicAdd(mesh_counters + m, (int)grp.size());
+    if (grp.thread_rank() == 0) slot = atomicAdd(mesh_counters + __ldg(F.sid + m), (int)grp.size());
     slot = grp.shfl(slot, 0) + grp.thread_rank();
     if ((long long)slot >= cap) {
         atomicOr(status, ST_OUT_OVERFLOW);
@@ -376,22 +455,21 @@ __device__ __forceinline__ long long append_row(int* mesh_counters, int m, long 
 // find_collisions: SAT + shared-vertex count (collisions_static.cu:123-159)
 template <class T>
 __global__ void __launch_bounds__(NARROW_THREADS)
-k_static_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ tri,
-                const int* __restrict__ moff, int M, T th, long long* __restrict__ rows, int max_per_tri,
-                int* __restrict__ mesh_counters) {
+k_static_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ tri, Forest F,
+                T th, long long* __restrict__ rows, int max_per_tri, int* __restrict__ mesh_counters) {
+    const int M = forest_size(F);
     int n = min(hdr->cand_count, cand_cap);
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
         int2 pr = cand[c];
         Tri<T> a = load_tri(tri, pr.x), b = load_tri(tri, pr.y);
         bool keep = sat(a, b, th) && !(count_shared(a, b) > 0);
         if (keep) {
-            int m = find_mesh(moff, M, pr.x, 0);
-            long long cap = (long long)(moff[m + 1] - moff[m]) * max_per_tri;
-            long long r = append_row(mesh_counters, m, cap, &hdr->status);
+            OutRegion R = out_region(F, M, pr.x, max_per_tri);
+            long long r = append_row(mesh_counters, F, R.m, R.cap, &hdr->status);
             if (r >= 0) {
-                long long o = (long long)moff[m] * max_per_tri + r;
-                rows[o * 2 + 0] = pr.x - moff[m];
-                rows[o * 2 + 1] = pr.y - moff[m];
+                long long o = (long long)R.po * max_per_tri + r;
+                rows[o * 2 + 0] = pr.x - R.po;
+                rows[o * 2 + 1] = pr.y - R.po;
             }
         }
     }
@@ -399,19 +477,32 @@ k_static_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, cons
 
 enum CcdMode { CCD_ROWS = 0, CCD_IMPULSES = 1, CCD_MINCOL = 2 };
 
+// Receiver of the impulses of CCD_IMPULSES: per-corner sums and counters (F, 3, 3) / (F, 3)
+// of the reference's compute_impulses.  Per-corner masses (F, 3) feed the contact.
+template <class T> struct CornerSink {
+    const T* masses;
+    T* dv;
+    T* dx;
+    int* cnt;
+    __device__ __forceinline__ void add(const MTet<T>& tet, long long gi, long long gj, int k, T root,
+                                        const Contact<T>& ct, const Forest&, int, int*) const {
+        apply_impulse(tet, gi, gj, k, root, ct, dv, dx, cnt);
+    }
+};
+
 // Continuous narrow phase (collisions_continuous.cu:14-765, collisions_impulses.cu:24-1067),
 // warp-cooperative.  Each warp takes 32 candidate pairs: every lane runs the shared-vertex
 // test and the 15 swept sub-box tests of its pair, the surviving (pair, type) items are
 // staged in shared memory, and then all 32 lanes solve items in lockstep, each loading only
 // the four points its item needs.  A one-thread-per-pair loop leaves most lanes idle, since
 // pairs have 0 to 15 cubic solves each.
-template <class T, int MODE>
+template <class T, int MODE, class Sink>
 __global__ void __launch_bounds__(NARROW_THREADS, 3)
 k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ x0,
-             const T* __restrict__ x1, const int* __restrict__ moff, int M, long long* __restrict__ rows,
-             T* __restrict__ times, int max_per_tri, int* __restrict__ mesh_counters, const T* __restrict__ masses,
-             T* __restrict__ dv_out, T* __restrict__ dx_out, int* __restrict__ cnt_out, int lib) {
+             const T* __restrict__ x1, Forest F, long long* __restrict__ rows, T* __restrict__ times, int max_per_tri,
+             int* __restrict__ mesh_counters, Sink sink, int lib) {
     constexpr int WARPS = NARROW_THREADS / 32;
+    const int M = forest_size(F);
     __shared__ unsigned short items[WARPS][32 * 15];
     __shared__ int2 pairs[WARPS][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -431,13 +522,12 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
             while (bits) {
                 int k = __ffs(bits) - 1;
                 bits &= bits - 1;
-                int m = find_mesh(moff, M, pr.x, 0);
-                long long cap = (long long)(moff[m + 1] - moff[m]) * max_per_tri;
-                long long r = append_row(mesh_counters, m, cap, &hdr->status);
+                OutRegion R = out_region(F, M, pr.x, max_per_tri);
+                long long r = append_row(mesh_counters, F, R.m, R.cap, &hdr->status);
                 if (r >= 0) {
-                    long long o = (long long)moff[m] * max_per_tri + r;
-                    rows[o * 3 + 0] = pr.x - moff[m];
-                    rows[o * 3 + 1] = pr.y - moff[m];
+                    long long o = (long long)R.po * max_per_tri + r;
+                    rows[o * 3 + 0] = pr.x - R.po;
+                    rows[o * 3 + 1] = pr.y - R.po;
                     rows[o * 3 + 2] = k;
                 }
             }
@@ -475,13 +565,12 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                 if (!(root >= 0 && root <= 1)) continue;
                 if (!ccd_filter(tet, k, root)) continue;
                 if (MODE == CCD_ROWS) {
-                    int m = find_mesh(moff, M, q.x, 0);
-                    long long cap = (long long)(moff[m + 1] - moff[m]) * max_per_tri;
-                    long long r = append_row(mesh_counters, m, cap, &hdr->status);
+                    OutRegion R = out_region(F, M, q.x, max_per_tri);
+                    long long r = append_row(mesh_counters, F, R.m, R.cap, &hdr->status);
                     if (r >= 0) {
-                        long long o = (long long)moff[m] * max_per_tri + r;
-                        rows[o * 3 + 0] = q.x - moff[m];
-                        rows[o * 3 + 1] = q.y - moff[m];
+                        long long o = (long long)R.po * max_per_tri + r;
+                        rows[o * 3 + 0] = q.x - R.po;
+                        rows[o * 3 + 1] = q.y - R.po;
                         rows[o * 3 + 2] = k;
                         times[o] = root;
                     }
@@ -489,9 +578,9 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                     T mq[4];
 #pragma unroll
                     for (int pt = 0; pt < 4; ++pt)
-                        mq[pt] = masses[(long long)(tet_side(k, pt) ? q.y : q.x) * 3 + tet_corner(k, pt)];
+                        mq[pt] = sink.masses[(long long)(tet_side(k, pt) ? q.y : q.x) * 3 + tet_corner(k, pt)];
                     Contact<T> ct = contact(tet, k, root, mq, lib);
-                    apply_impulse(tet, q.x, q.y, k, root, ct, dv_out, dx_out, cnt_out);
+                    sink.add(tet, q.x, q.y, k, root, ct, F, M, &hdr->status);
                 }
             }
         }
@@ -502,9 +591,9 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
 // proximity (proximity_static.cu:11-508)
 template <class T>
 __global__ void __launch_bounds__(NARROW_THREADS)
-k_prox_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ tri,
-              const int* __restrict__ moff, int M, T th, long long* __restrict__ rows, int max_per_tri,
-              int* __restrict__ mesh_counters) {
+k_prox_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ tri, Forest F, T th,
+              long long* __restrict__ rows, int max_per_tri, int* __restrict__ mesh_counters) {
+    const int M = forest_size(F);
     int n = min(hdr->cand_count, cand_cap);
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
         int2 pr = cand[c];
@@ -514,13 +603,12 @@ k_prox_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const 
             if (!prox_subbox(a, b, k, th)) continue;
             T d = prox_distance(a, b, k);
             if (!(d <= th && d >= 0)) continue;
-            int m = find_mesh(moff, M, pr.x, 0);
-            long long cap = (long long)(moff[m + 1] - moff[m]) * max_per_tri;
-            long long r = append_row(mesh_counters, m, cap, &hdr->status);
+            OutRegion R = out_region(F, M, pr.x, max_per_tri);
+            long long r = append_row(mesh_counters, F, R.m, R.cap, &hdr->status);
             if (r >= 0) {
-                long long o = (long long)moff[m] * max_per_tri + r;
-                rows[o * 3 + 0] = pr.x - moff[m];
-                rows[o * 3 + 1] = pr.y - moff[m];
+                long long o = (long long)R.po * max_per_tri + r;
+                rows[o * 3 + 0] = pr.x - R.po;
+                rows[o * 3 + 1] = pr.y - R.po;
                 rows[o * 3 + 2] = k;
             }
         }
@@ -557,7 +645,7 @@ k_impulses_from_rows(const long long* __restrict__ rows, const T* __restrict__ r
 // op 0 cbrt, 1 acos, 2 cos, 3 sin, 4 certified product (in: x0, x1, k, y; out: r0, r1),
 // 5 solve_cubic (in: a, b, c, d; out: three roots), 6 CUDA cbrt, 7 CUDA acos, 8 CUDA cos,
 // 9 CUDA sin.  in has 4 doubles per element, out 3.
-__global__ void k_debug_math(int op, const double* __restrict__ in, double* __restrict__ out, int n) {
+static __global__ void k_debug_math(int op, const double* __restrict__ in, double* __restrict__ out, int n) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double* a = in + 4 * i;
@@ -601,7 +689,7 @@ __global__ void k_debug_math(int op, const double* __restrict__ in, double* __re
 // roots; op 2: root filter (in: tet, type, root) -> 1.0 / 0.0; op 3: contact kinematics
 // (in: tet, type, root, 4 masses) -> normal (3), normal velocity, mass pair (2).
 // lib selects the elementary functions (MathLib).
-__global__ void k_debug_stage(int op, int lib, const double* __restrict__ in, int in_stride,
+static __global__ void k_debug_stage(int op, int lib, const double* __restrict__ in, int in_stride,
                               double* __restrict__ out, int out_stride, int n) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;

@@ -30,7 +30,7 @@
 #define CCC_HD __host__ __device__ __forceinline__
 // larger helpers are kept out of line on the device: the solver calls each several times
 // and warps in different branches would otherwise thrash the instruction cache
-#define CCC_HD_CALL __host__ __device__ __noinline__
+#define CCC_HD_CALL static __host__ __device__ __noinline__
 #else
 #define CCC_HD static inline
 #define CCC_HD_CALL static

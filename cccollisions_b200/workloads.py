@@ -14,6 +14,7 @@ All randomness comes from ``numpy.random.Generator(PCG64(seed))``.
 """
 from __future__ import annotations
 
+import functools
 import math
 
 import numpy as np
@@ -40,8 +41,18 @@ def grid(nx: int, ny: int, x0=0.0, x1=1.0, y0=0.0, y1=1.0):
     return verts, faces.astype(np.int64)
 
 
+@functools.lru_cache(maxsize=8)
+def _icosphere_unit(level: int):
+    return icosphere_build(level)
+
+
 def icosphere(level: int, radius: float = 1.0):
     """Subdivided icosahedron projected onto a sphere (20 * 4^level faces)."""
+    v, f = _icosphere_unit(level)
+    return v * radius, f.copy()
+
+
+def icosphere_build(level: int):
     t = (1.0 + math.sqrt(5.0)) / 2.0
     v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
          (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
@@ -65,7 +76,7 @@ def icosphere(level: int, radius: float = 1.0):
             ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
             nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
         faces = nf
-    return np.array(verts) * radius, np.array(faces, dtype=np.int64)
+    return np.array(verts), np.array(faces, dtype=np.int64)
 
 
 def soup(verts, faces):
@@ -176,4 +187,41 @@ def batched(num_meshes: int = 64, lo: float = 1e3, hi: float = 1e5, seed0: int =
         nx, ny = grid_for_count(g, tris)
         x0, x1 = cloth_sphere(seed=seed0 + i, nx=nx, ny=ny, level=level, dtype=dtype)
         out.append((x0[0], x1[0]))
+    return out
+
+
+def impulse_fold_mesh(seed: int = 0, nx: int = 256, ny: int = 256, dtype=np.float64):
+    """Indexed form of the impulse workload (jittered cloth, x > 0.5 half folded 0.005 above
+    the rest, moving 0.01 down with N(0, 0.002^2) noise) on an nx-by-ny grid scaled to the
+    grid's aspect: verts0 (V, 3), verts1 (V, 3), vel (V, 3) = verts1 - verts0, faces (F, 3)
+    int32, per-corner unit masses (F, 3)."""
+    g = rng(seed)
+    sy = (ny - 1) / (nx - 1)
+    verts, faces = grid(nx, ny, 0.0, 1.0, 0.0, sy)
+    verts[:, 2] = g.normal(0.0, 0.01, verts.shape[0])
+    m = verts[:, 0] > 0.5
+    verts[m, 0] = 1.0 - verts[m, 0]
+    verts[m, 2] += 0.005
+    v1 = verts.copy()
+    v1[:, 2] -= 0.01
+    v1 += g.normal(0.0, 0.002, verts.shape)
+    masses = np.ones((faces.shape[0], 3), dtype=dtype)
+    return (verts.astype(dtype), v1.astype(dtype), (v1 - verts).astype(dtype), faces.astype(np.int32), masses)
+
+
+def served_stream(num_requests: int = 256, rate: float = 2000.0, lo: float = 2e3, hi: float = 2e5,
+                  seed: int = 0, seed0: int = 1000, dtype=np.float64):
+    """Poisson request stream: (arrival seconds, request seed, nx, ny) per request.
+
+    Inter-arrival times are exponential with the given rate (seed `seed`); request i has
+    log-uniform triangle count in [lo, hi] and builds its mesh with impulse_fold_mesh(seed0 + i).
+    """
+    g = rng(seed)
+    t = np.cumsum(g.exponential(1.0 / rate, num_requests))
+    out = []
+    for i in range(num_requests):
+        gi = rng(seed0 + i)
+        tris = math.exp(gi.uniform(math.log(lo), math.log(hi)))
+        nx, ny = grid_for_count(gi, tris)
+        out.append((float(t[i]), seed0 + i, nx, ny))
     return out

@@ -227,7 +227,8 @@ static void refit(int n, const Topo& tp, std::vector<Box<T>>& box, std::vector<i
 // initial AABB() = (-MAX, +MAX) (aabb.cu:114-122, build_bvh.cu:243), so it is unbounded,
 // every normalised centroid divides by an infinite extent, and every Morton code is 0;
 // the stable sort then keeps the input order.  spatial == 1 starts the reduction from the
-// empty box instead (the CUDA path's spatial mode), giving real Morton codes.
+// empty box instead, giving real Morton codes (a spatially sorted tree; the pairs found
+// do not depend on the tree).
 template <class T>
 static void build(const T* tri, const T* tri_next, int n, int spatial, T* bboxes_out, int64_t* tree_out,
                   uint32_t* codes_out) {
@@ -1141,6 +1142,141 @@ ORC_API int64_t orc_impulses(int dtype, const void* bboxes, const int64_t* tree,
     c = orc_ccd(dtype, bboxes, tree, x0, x1, n, mask, rows.data(), times.data(), std::min(c, cap), nthreads);
     orc_impulses_from_rows(dtype, x0, x1, masses, n, rows.data(), times.data(), c, dv, dx, cnt);
     return c;
+}
+
+// ---------------------------------------------------------------------------------------
+// Impulse loop of the resident engine (no counterpart in the reference, whose caller owns
+// the loop): collision check with impulses, per-vertex average of the corner corrections,
+// repeat until a check finds no contact or max_iter iterations.  Impulses are summed per
+// vertex in 2^-56 fixed point (int64), so the sums do not depend on contact order and the
+// GPU engine's loop matches this one bit for bit.
+// ---------------------------------------------------------------------------------------
+static const double FIX_SCALE = 72057594037927936.0;   // 2^56
+static const double FIX_INV = 1.3877787807814457e-17;  // 2^-56
+
+static inline bool to_fix(double x, int64_t& q) {
+    if (!(fabs(x) < 64.0)) return false;
+    q = (int64_t)nearbyint(x * FIX_SCALE);
+    return true;
+}
+
+template <class T>
+static void gather_soup(const T* verts, const int32_t* faces, int64_t F, T* soup) {
+    for (int64_t f = 0; f < F; ++f)
+        for (int c = 0; c < 3; ++c)
+            for (int d = 0; d < 3; ++d) soup[f * 9 + c * 3 + d] = verts[(int64_t)faces[f * 3 + c] * 3 + d];
+}
+
+// one contact's four point impulses into the fixed-point vertex sums (8 words per vertex:
+// dx xyz, dv xyz, count); returns false if a value was non-finite or out of range
+template <class T>
+static bool loop_contact(const MTet<T>& tet, int64_t i, int64_t j, int k, T root, const Contact<T>& ct,
+                         const int32_t* faces, int64_t* acc) {
+    T offset;
+    if (fabs((double)ct.vn) < 1e-15) offset = (T)0.1;
+    else offset = (T)((2 * THICKNESS) / (double)(-ct.vn));
+    offset = (T)fmin(fmax((double)offset, 0.), 1.);
+    T msum = ct.m0 + ct.m1;
+    T mf0, mf1;
+    if (fabs((double)msum) < 1e-15) { mf0 = (T)0.5; mf1 = (T)0.5; }
+    else { mf0 = ct.m0 / msum; mf1 = 1 - mf0; }
+    T mag0 = ct.vn * mf1;
+    T mag1 = -ct.vn * mf0;
+    T mags[4];
+    if (k < 9) { mags[0] = mag0; mags[1] = mag0; mags[2] = mag1; mags[3] = mag1; }
+    else if (k < 12) { mags[0] = mag0; mags[1] = mag0; mags[2] = mag0; mags[3] = mag1; }
+    else { mags[0] = mag0; mags[1] = mag1; mags[2] = mag1; mags[3] = mag1; }
+    T keep = 1 - (T)fmax((double)(root - offset), 0.);
+    int side[4], corner[4];
+    type_points(k, side, corner);
+    bool all_ok = true;
+    for (int p = 0; p < 4; ++p) {
+        V3<T> imp = ct.n * mags[p];
+        V3<T> nv = tet.dv[p] + imp;
+        V3<T> idx = (nv - tet.dv[p]) * keep;
+        int64_t q[6];
+        bool ok = to_fix((double)idx.x, q[0]) && to_fix((double)idx.y, q[1]) && to_fix((double)idx.z, q[2]) &&
+                  to_fix((double)imp.x, q[3]) && to_fix((double)imp.y, q[4]) && to_fix((double)imp.z, q[5]);
+        if (!ok) {
+            all_ok = false;
+            continue;
+        }
+        int64_t tri = side[p] ? j : i;
+        int64_t* a = acc + (int64_t)faces[tri * 3 + corner[p]] * 8;
+        for (int c = 0; c < 6; ++c) a[c] = (int64_t)((uint64_t)a[c] + (uint64_t)q[c]);
+        a[6] += 1;
+    }
+    return all_ok;
+}
+
+template <class T>
+static int loop_impl(const T* verts0, T* verts1, T* vel, const int32_t* faces, const T* masses, int64_t F, int64_t V,
+                     int max_iter, int32_t* contacts_per_iter, int nthreads, int* converged) {
+    std::vector<T> x0(F * 9), x1(F * 9), bb((2 * F - 1) * 6);
+    std::vector<int64_t> tree((2 * F - 1) * 4);
+    std::vector<int64_t> acc(V * 8);
+    gather_soup(verts0, faces, F, x0.data());
+    int it = 0;
+    *converged = 0;
+    for (;;) {
+        gather_soup(verts1, faces, F, x1.data());
+        build<T>(x0.data(), x1.data(), (int)F, 1, bb.data(), tree.data(), nullptr);
+        int64_t c = ccd_impl<T>(bb.data(), tree.data(), x0.data(), x1.data(), (int)F, nullptr, nullptr, nullptr, 0,
+                                nthreads, 1);
+        if (c < 0) return -1;
+        if (contacts_per_iter) contacts_per_iter[it] = (int32_t)c;
+        if (c == 0) {
+            *converged = 1;
+            break;
+        }
+        std::vector<int64_t> rows(3 * c);
+        std::vector<double> times(c);
+        ccd_impl<T>(bb.data(), tree.data(), x0.data(), x1.data(), (int)F, nullptr, rows.data(), times.data(), c,
+                    nthreads, 1);
+        std::fill(acc.begin(), acc.end(), 0);
+        for (int64_t r = 0; r < c; ++r) {
+            int64_t i = rows[3 * r], j = rows[3 * r + 1];
+            int k = (int)rows[3 * r + 2];
+            T root = (T)times[r];
+            MTri<T> a = load_mtri(x0.data(), x1.data(), i), b = load_mtri(x0.data(), x1.data(), j);
+            MTet<T> tet = make_tet(a, b, k);
+            T q[4];
+            mass_quad(masses, i, j, k, q);
+            Contact<T> ct = contact(tet, k, root, q);
+            loop_contact(tet, i, j, k, root, ct, faces, acc.data());
+        }
+        for (int64_t v = 0; v < V; ++v) {
+            const int64_t* a = acc.data() + v * 8;
+            if (a[6] == 0) continue;
+            double cnt = (double)a[6];
+            for (int d = 0; d < 3; ++d) {
+                double dx = ((double)a[d] * FIX_INV) / cnt;
+                double dv = ((double)a[3 + d] * FIX_INV) / cnt;
+                verts1[v * 3 + d] = (T)((double)verts1[v * 3 + d] + dx);
+                vel[v * 3 + d] = (T)((double)vel[v * 3 + d] + dv);
+            }
+        }
+        ++it;
+        if (it >= max_iter) break;
+    }
+    return it;
+}
+
+// Impulse loop on one mesh (vertices, faces, per-corner masses); verts1 and vel are updated
+// in place.  Returns the iterations applied (or -1), writes the contact count of every
+// collision check to contacts_per_iter (max_iter + 1 entries) and whether the last check
+// found no contact.
+ORC_API int orc_impulse_loop(int dtype, const void* verts0, void* verts1, void* vel, const int32_t* faces,
+                             const void* masses, int64_t F, int64_t V, int max_iter, int32_t* contacts_per_iter,
+                             int nthreads, int* converged) {
+    if (F < 2 || V < 1 || max_iter < 1) return -1;
+    for (int64_t f = 0; f < 3 * F; ++f)
+        if (faces[f] < 0 || faces[f] >= V) return -1;
+    if (dtype == 0)
+        return loop_impl<float>((const float*)verts0, (float*)verts1, (float*)vel, faces, (const float*)masses, F, V,
+                                max_iter, contacts_per_iter, nthreads, converged);
+    return loop_impl<double>((const double*)verts0, (double*)verts1, (double*)vel, faces, (const double*)masses, F, V,
+                             max_iter, contacts_per_iter, nthreads, converged);
 }
 
 template <class T>

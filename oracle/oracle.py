@@ -88,6 +88,9 @@ def lib():
         L.orc_sat.argtypes = [ctypes.c_int, _P, _P, ctypes.c_double]
         L.orc_sat.restype = ctypes.c_int
         L.orc_num_threads.restype = ctypes.c_int
+        L.orc_impulse_loop.argtypes = [ctypes.c_int, _P, _P, _P, _P, _P, _I64, _I64, ctypes.c_int, _P, ctypes.c_int,
+                                       _P]
+        L.orc_impulse_loop.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -216,6 +219,23 @@ def impulses(bboxes, tree, triangles, triangles_next, masses, mask=None, nthread
     if c < 0:
         raise RuntimeError("oracle impulses failed")
     return dv, dx, cnt, c
+
+
+def impulse_loop(verts0, verts1, vel, faces, masses, max_iter=50, nthreads=0):
+    """The resident engine's impulse loop on one mesh (vertices (V,3), faces (F,3), per-corner
+    masses (F,3)): returns (verts1, vel, iterations, converged, contacts per check)."""
+    v0 = _c(verts0)
+    v1 = _c(verts1, v0.dtype).copy()
+    vl = _c(vel, v0.dtype).copy()
+    fc = _c(faces, np.int32)
+    m = _c(masses, v0.dtype)
+    conv = ctypes.c_int(0)
+    per = np.zeros(max_iter + 1, dtype=np.int32)
+    it = lib().orc_impulse_loop(_dt(v0), _ptr(v0), _ptr(v1), _ptr(vl), _ptr(fc), _ptr(m), fc.shape[0], v0.shape[0],
+                                int(max_iter), _ptr(per), int(nthreads), ctypes.byref(conv))
+    if it < 0:
+        raise RuntimeError("oracle impulse loop failed")
+    return v1, vl, it, bool(conv.value), per[:it + (1 if conv.value else 0)]
 
 
 def proximity(bboxes, tree, triangles, threshold):

@@ -8,9 +8,12 @@ from conftest import ROOT
 
 
 def _declared_functions():
-    src = open(os.path.join(ROOT, "include", "ccc_b200.h")).read()
-    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(ccc_[a-z0-9_]+)\s*\(", src)))
+    names = set()
+    for h in ("ccc_b200.h", "ccc_engine.h"):
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names |= set(re.findall(r"\b(ccc_[a-z0-9_]+)\s*\(", src))
+    return sorted(names)
 
 
 def test_header_declares_the_reference_entry_points():
@@ -42,6 +45,19 @@ def test_pure_host_calls(native_lib):
     assert rc == 1
     rc = native_lib.ccc_find_collisions(0, None, None, None, 1, 1, 0.0, 16, None, None, 0, None)
     assert rc == 1
+
+
+def test_engine_sizes_are_pure_host(native_lib):
+    small = native_lib.ccc_engine_bytes(1, 1000, 500, 4, 16, 16)
+    big = native_lib.ccc_engine_bytes(1, 2000, 500, 4, 16, 16)
+    assert 0 < small < big
+    assert native_lib.ccc_engine_bytes(0, 1000, 500, 4, 16, 16) < small      # fp32 positions
+    assert native_lib.ccc_engine_bytes(2, 1000, 0, 4, 16, 16) == -1          # dtype
+    assert native_lib.ccc_engine_bytes(1, 1, 0, 4, 16, 16) == -1             # F >= 2
+    assert native_lib.ccc_engine_bytes(1, 1 << 27, 0, 4, 16, 16) == -1       # candidate slots > 2^31
+    # argument errors before any device work
+    assert native_lib.ccc_engine_create(1, 1000, 0, 4, 16, 16, None, 0, None, None) == 1
+    assert native_lib.ccc_engine_ccd(None, None) == 1
 
 
 def test_api_mirrors_reference_signatures():
