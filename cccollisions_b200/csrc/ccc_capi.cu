@@ -95,7 +95,9 @@ Layout layout(int64_t B, int64_t F, int64_t maxc, bool need_nodes) {
     return L;
 }
 
-inline int narrow_grid() { return num_sms() * 8; }
+// one wave of resident narrow-phase blocks (the kernels' launch bounds); the kernels loop
+// over their work
+inline int narrow_grid() { return num_sms() * NARROW_MIN_BLOCKS; }
 
 int check_common(int dtype, int64_t B, int64_t F) {
     if (dtype != 0 && dtype != 1) return CCC_ERR_INVALID_ARG;
@@ -225,9 +227,9 @@ int ccd_impl(const void* bboxes, const int64_t* tree, const void* x0, const void
     if (rc) return rc;
     rc = run_broad_phase<T>(bboxes, tree, mask, B, F, (T)0, is_f32<T>(), P, s);
     if (rc) return rc;
-    CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_ROWS, CornerSink<T>><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
+    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
         P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, (long long*)rows, (T*)times,
-        (int)maxcol, P.mesh_cnt, CornerSink<T>{}, g_math_lib));
+        (int)maxcol, P.mesh_cnt, CornerSink<T>{})));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -240,9 +242,9 @@ int mincol_impl(const void* bboxes, const int64_t* tree, const void* x0, const v
     if (rc) return rc;
     rc = run_broad_phase<T>(bboxes, tree, nullptr, B, F, (T)0, is_f32<T>(), P, s);
     if (rc) return rc;
-    CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_MINCOL, CornerSink<T>><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
+    CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_MINCOL, CornerSink<T>, LIB_PORTABLE><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
         P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, (long long*)rows, nullptr,
-        (int)(maxc * 15), P.mesh_cnt, CornerSink<T>{}, g_math_lib));
+        (int)(maxc * 15), P.mesh_cnt, CornerSink<T>{}));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -271,9 +273,9 @@ int impulses_impl(const void* bboxes, const int64_t* tree, const void* x0, const
     if (rc) return rc;
     rc = run_broad_phase<T>(bboxes, tree, mask, B, F, (T)0, is_f32<T>(), P, s);
     if (rc) return rc;
-    CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_IMPULSES, CornerSink<T>><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
+    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_IMPULSES, CornerSink<T>, LIBV><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
         P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, nullptr, nullptr, 0, P.mesh_cnt,
-        CornerSink<T>{(const T*)masses, (T*)dv, (T*)dx, (int*)cnt}, g_math_lib));
+        CornerSink<T>{(const T*)masses, (T*)dv, (T*)dx, (int*)cnt})));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -287,9 +289,9 @@ int from_rows_impl(const int64_t* rows, const void* roots, int64_t B, int64_t N,
     if (rc) return rc;
     if (B * N == 0) return CCC_OK;
     int g = (int)std::min<int64_t>(grid_for(B * N, NARROW_THREADS), (int64_t)narrow_grid());
-    CCC_LAUNCH("k_impulses_from_rows", s, k_impulses_from_rows<T><<<g, NARROW_THREADS, 0, s>>>((const long long*)rows, (const T*)roots, (int)B, N, (int)F,
-                                                         (const T*)x0, (const T*)x1, (const T*)masses, (T*)dv, (T*)dx,
-                                                         (int*)cnt, P.hdr, g_math_lib));
+    CCC_WITH_LIB(CCC_LAUNCH("k_impulses_from_rows", s, k_impulses_from_rows<T, LIBV><<<g, NARROW_THREADS, 0, s>>>(
+        (const long long*)rows, (const T*)roots, (int)B, N, (int)F, (const T*)x0, (const T*)x1, (const T*)masses,
+        (T*)dv, (T*)dx, (int*)cnt, P.hdr)));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }

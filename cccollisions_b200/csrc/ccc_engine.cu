@@ -94,7 +94,7 @@ EngineLayout engine_layout(int64_t tsz, int64_t tc, int64_t vc, int64_t mc, int6
     L.vals0 = take(tc * 4);
     L.vals1 = take(tc * 4);
     L.hist_len = 256 * ((tc + SORT_TILE - 1) / SORT_TILE);
-    L.hist = take(L.hist_len * 4);
+    L.hist = take((L.hist_len + L.hist_len / SCAN_CHUNK + 1) * 4);    // counts, then chunk totals
     L.verts0 = take(vc * 3 * tsz);
     L.verts1 = take(vc * 3 * tsz);
     L.vel = take(vc * 3 * tsz);
@@ -151,11 +151,12 @@ struct Ranges {
     }
 };
 
-// launch shapes: traversal and narrow-phase blocks per SM
+// launch shapes: traversal blocks per SM, narrow-phase blocks per SM in units of one
+// resident wave (NARROW_MIN_BLOCKS)
 struct Shape {
     int trav, narrow;
 };
-constexpr Shape SHAPES[] = {{4, 3}, {8, 3}, {16, 3}, {4, 6}, {8, 6}, {16, 6}, {8, 12}, {16, 12}, {32, 24}};
+constexpr Shape SHAPES[] = {{4, 1}, {8, 1}, {16, 1}, {4, 2}, {8, 2}, {16, 2}, {8, 4}, {16, 4}, {32, 8}};
 constexpr int NSHAPES = sizeof(SHAPES) / sizeof(SHAPES[0]);
 constexpr int DEFAULT_SHAPE = 4;
 
@@ -232,8 +233,14 @@ int upload_table(ccc_engine* e, int which, const int32_t* ids, int64_t n, cudaSt
     return CCC_OK;
 }
 
+// The refit's climbs are chains of dependent L2 round trips, so it runs about one leaf per
+// thread (up to 64 blocks per SM) rather than a grid-stride loop over few threads.
+inline int refit_grid(const ccc_engine* e) {
+    return (int)std::min<int64_t>(grid_for(e->tri_cap, ITEM_THREADS), (int64_t)num_sms() * 64);
+}
+
 template <class T> int refit(ccc_engine* e, const Tables& t, const int* flags, cudaStream_t s) {
-    CCC_LAUNCH("k_engine_refit", s, k_engine_refit<T><<<item_grid(), ITEM_THREADS, 0, s>>>(
+    CCC_LAUNCH("k_engine_refit", s, k_engine_refit<T><<<refit_grid(e), ITEM_THREADS, 0, s>>>(
         t.f, e->at<T>(e->L.x0), e->at<T>(e->L.x1), e->at<int>(e->L.leaf_tri), e->at<int>(e->L.lparent),
         e->at<int>(e->L.nparent), e->at<TNode>(e->L.nodes), e->at<unsigned>(e->L.visits), e->at<T>(e->L.lbox), flags,
         &e->hdr()->status));
@@ -262,11 +269,10 @@ template <class T> int ccd_step(ccc_engine* e, cudaStream_t s) {
     if (rc) return rc;
     rc = traverse<T>(e, t, nullptr, s);
     if (rc) return rc;
-    int g = num_sms() * SHAPES[e->shape].narrow;
-    CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_ROWS, CornerSink<T>><<<g, NARROW_THREADS, 0, s>>>(
+    int g = num_sms() * NARROW_MIN_BLOCKS * SHAPES[e->shape].narrow;
+    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV><<<g, NARROW_THREADS, 0, s>>>(
         e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f,
-        e->at<long long>(e->L.rows), e->at<T>(e->L.times), (int)e->maxcol, e->at<int>(e->L.mesh_cnt), CornerSink<T>{},
-        g_math_lib));
+        e->at<long long>(e->L.rows), e->at<T>(e->L.times), (int)e->maxcol, e->at<int>(e->L.mesh_cnt), CornerSink<T>{})));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -280,11 +286,11 @@ template <class T> int loop_step(ccc_engine* e, int max_iter, cudaStream_t s) {
     if (rc) return rc;
     rc = traverse<T>(e, t, flags, s);
     if (rc) return rc;
-    int g = num_sms() * SHAPES[e->shape].narrow;
+    int g = num_sms() * NARROW_MIN_BLOCKS * SHAPES[e->shape].narrow;
     LoopSink<T> sink{e->at<T>(e->L.masses), e->at<int>(e->L.faces), t.vt, e->at<long long>(e->L.acc), contacts};
-    CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>><<<g, NARROW_THREADS, 0, s>>>(
+    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIBV><<<g, NARROW_THREADS, 0, s>>>(
         e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f, nullptr,
-        nullptr, 0, e->at<int>(e->L.mesh_cnt), sink, g_math_lib));
+        nullptr, 0, e->at<int>(e->L.mesh_cnt), sink)));
     CCC_LAUNCH_CHECK();
     CCC_LAUNCH("k_loop_update", s, k_loop_update<<<grid_for(e->mesh_cap, ITEM_THREADS), ITEM_THREADS, 0, s>>>(
         t.f, contacts, e->at<int>(e->L.iters), flags, max_iter));
@@ -324,7 +330,14 @@ template <class T> int build_trees(ccc_engine* e, int64_t ntri, int64_t nb, cuda
         int shift = 8 * p;
         CCC_LAUNCH("k_radix_hist", s, k_radix_hist<<<nblk, SORT_THREADS, 0, s>>>(keys[cur], n, shift, hist, nblk));
         CCC_LAUNCH_CHECK();
-        CCC_LAUNCH("k_exclusive_scan", s, k_exclusive_scan<<<1, 1024, 0, s>>>(hist, 256 * nblk));
+        int len = 256 * nblk;
+        int nchunk = (len + SCAN_CHUNK - 1) / SCAN_CHUNK;
+        int* part = hist + e->L.hist_len;
+        CCC_LAUNCH("k_scan_chunks", s, k_scan_chunks<<<nchunk, SCAN_THREADS, 0, s>>>(hist, len, part));
+        CCC_LAUNCH_CHECK();
+        CCC_LAUNCH("k_exclusive_scan", s, k_exclusive_scan<<<1, 1024, 0, s>>>(part, nchunk));
+        CCC_LAUNCH_CHECK();
+        CCC_LAUNCH("k_scan_add", s, k_scan_add<<<grid_for(len, 256), 256, 0, s>>>(hist, len, part));
         CCC_LAUNCH_CHECK();
         CCC_LAUNCH("k_radix_scatter", s, k_radix_scatter<<<nblk, SORT_THREADS, 0, s>>>(keys[cur], vals[cur], keys[1 - cur],
                                                                                    vals[1 - cur], n, shift, hist, nblk));

@@ -63,9 +63,28 @@ __global__ void k_mesh_bounds(Forest F, const T* __restrict__ x0, const T* __res
         int m = find_mesh(F.voff, M, v, 0);
         long long slot = (long long)__ldg(F.poff + m) + (v - __ldg(F.voff + m));
         float3 c = swept_centroid(x0, x1, slot);
-        cg::coalesced_group act = cg::coalesced_threads();
-        cg::coalesced_group grp = cg::labeled_partition(act, m);
         float lo[3] = {c.x, c.y, c.z}, hi[3] = {c.x, c.y, c.z};
+        cg::coalesced_group act = cg::coalesced_threads();
+        if (act.size() == 32 && __all_sync(0xffffffffu, m == __shfl_sync(0xffffffffu, m, 0))) {
+            // whole warp in one mesh: butterfly reduction, one atomic per word
+#pragma unroll
+            for (int o = 16; o >= 1; o >>= 1)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+                    hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+                }
+            if ((threadIdx.x & 31) == 0) {
+                unsigned* b = bounds + 6 * __ldg(F.sid + m);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    atomicMin(b + d, f2ord(lo[d]));
+                    atomicMax(b + 3 + d, f2ord(hi[d]));
+                }
+            }
+            continue;
+        }
+        cg::coalesced_group grp = cg::labeled_partition(act, m);
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             lo[d] = cg::reduce(grp, lo[d], cg::less<float>());
@@ -140,7 +159,55 @@ k_radix_hist(const unsigned long long* __restrict__ keys, int n, int shift, int*
     counts[(long long)threadIdx.x * nblk + blockIdx.x] = h[threadIdx.x];
 }
 
-// exclusive prefix sum of len ints in place, one block of 1024 threads
+// Exclusive prefix sum in three passes: each block scans SCAN_CHUNK elements and writes its
+// total, one block scans the totals, and the totals' prefixes are added back.
+static constexpr int SCAN_THREADS = 256;
+static constexpr int SCAN_ITEMS = 8;
+static constexpr int SCAN_CHUNK = SCAN_THREADS * SCAN_ITEMS;
+
+static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_chunks(int* __restrict__ a, int len, int* __restrict__ part) {
+    __shared__ int wsum[SCAN_THREADS / 32];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const long long base = (long long)blockIdx.x * SCAN_CHUNK + (long long)t * SCAN_ITEMS;
+    int v[SCAN_ITEMS];
+    int sum = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        v[i] = base + i < len ? a[base + i] : 0;
+        sum += v[i];
+    }
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    if (t == 0) {
+        int run = 0;
+        for (int i = 0; i < SCAN_THREADS / 32; ++i) {
+            int c = wsum[i];
+            wsum[i] = run;
+            run += c;
+        }
+        part[blockIdx.x] = run;
+    }
+    __syncthreads();
+    int run = wsum[w] + incl - sum;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        if (base + i < len) a[base + i] = run;
+        run += v[i];
+    }
+}
+
+static __global__ void k_scan_add(int* __restrict__ a, int len, const int* __restrict__ part) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < len) a[i] += part[i / SCAN_CHUNK];
+}
+
+// exclusive prefix sum of len ints in place, one block of 1024 threads (short arrays)
 static __global__ void __launch_bounds__(1024) k_exclusive_scan(int* __restrict__ a, int len) {
     __shared__ int part[1024];
     const int t = threadIdx.x;

@@ -374,82 +374,124 @@ template <class T> __device__ __forceinline__ void add_root(T r[3], T x, int& nr
     nr++;
 }
 
-// solveCubic with computeG / computeH (collisions_continuous.cu:472-613); roots start at -1.
-template <class T> __device__ __noinline__ void solve_cubic(double a, double b, double c, double d, T r[3], int lib) {
+// solveCubic with computeG / computeH (collisions_continuous.cu:472-613), in two parts: the
+// prefix classifies (c3, c2, c1, c0) = (a, b, c, d) and computes g and h, and one function
+// per branch produces its roots.  solve_cubic chains them; the continuous narrow phase
+// calls the parts separately so that a warp solves one branch at a time.
+// lib (MathLib) is a template parameter so that each kernel carries one solver variant.
+enum CubicClass {
+    CUBIC_NONE = 0,      // linear: the reference never stores its root
+    CUBIC_QUAD = 1,      // |a| < EPSILON
+    CUBIC_TRIPLE = 2,    // f = g = h = 0
+    CUBIC_THREE = 3,     // h <= 0: three real roots (trigonometric form)
+    CUBIC_ONE = 4,       // h > 0 (or NaN): one real root
+};
+
+template <int lib>
+__device__ __forceinline__ int cubic_prefix(double a, double b, double c, double d, double& g, double& h) {
+    g = h = 0.0;
+    if (a == 0 && b == 0) return CUBIC_NONE;
+    if (fabs(a) < CCC_EPS) return CUBIC_QUAD;
+    double f = ((3.0 * c / a) - ((b * b) / (a * a))) / 3.0;
+    double b3 = 2 * ccc_cube_hi(b);
+    ccc_dd a2dd = ccc_sq_dd(a);
+    double a2 = a2dd.hi;
+    double a3 = ccc_certmul(a2dd.hi, a2dd.lo, 2, a).hi;
+    double p1 = b3 / a3;
+    double p2 = (b * c * 9) / a2;
+    double p3 = 27.0 * d / a;
+    g = (p1 - p2 + p3) / 27.0;
+    double f3 = ccc_cube_hi(f);
+    // the reference's pow(g, 2) resolves (through std::pow's promotion) to CUDA's general
+    // pow(double, double), which is not always the rounded square
+    double g2 = lib == LIB_REFERENCE ? pow(g, 2.0) : g * g;
+    h = g2 / 4.0 + f3 / 27.0;
+    if (f == 0 && g == 0 && h == 0) return CUBIC_TRIPLE;
+    return h <= 0 ? CUBIC_THREE : CUBIC_ONE;
+}
+
+template <class T> __device__ __forceinline__ void quad_roots(double b, double c, double d, T r[3], int& nr) {
+    double D = fmaT(c, c, -(4.0 * b * d));
+    if (D >= 0) {
+        D = ccc_sqrt(D);
+        double x1 = (-c + D) / (2.0 * b);
+        double x2 = (-c - D) / (2.0 * b);
+        add_root<T>(r, (T)x1, nr);
+        add_root<T>(r, (T)x2, nr);
+    }
+}
+
+template <class T, int lib> __device__ __forceinline__ void triple_roots(double a, double d, T r[3], int& nr) {
+    float k = (float)(d / a);
+    double x1;
+    float cr = lib == LIB_REFERENCE ? cbrtf(k >= 0 ? k : -k) : ccc_cbrtf(k >= 0 ? k : -k);
+    if (k >= 0) x1 = (double)(cr * -1);
+    else x1 = (double)cr;
+    add_root<T>(r, (T)x1, nr);
+}
+
+template <class T, int lib>
+__device__ __forceinline__ void three_roots(double a, double b, double g, double h, T r[3], int& nr) {
+    double i = ccc_sqrt(((g * g) / 4.0) - h);
+    double j, k, M, sn;
+    if (lib == LIB_REFERENCE) {
+        j = cbrt(i);
+        k = acos(-(g / (2 * i)));
+        M = cos(k / 3.0);
+        sn = sin(k / 3.0);
+    } else {
+        j = ccc_cbrt(i);
+        k = ccc_acos(-(g / (2 * i)));
+        M = ccc_cos(k / 3.0);
+        sn = ccc_sin(k / 3.0);
+    }
+    // N = sqrt(3) * sin(k/3) is fused into M + N and M - N and each result into
+    // L * (.) + P; the first root 2 j cos(k/3) - b/(3a) is rounded twice (unfused)
+    const double r3 = ccc_sqrt(3.0);
+    double L = j * -1;
+    double P = (b / (3.0 * a)) * -1;
+    double x1 = (2 * j) * M - (b / (3.0 * a));
+    double x2 = fmaT(L, fmaT(r3, sn, M), P);
+    double x3 = fmaT(L, fmaT(-r3, sn, M), P);
+    add_root<T>(r, (T)x1, nr);
+    add_root<T>(r, (T)x2, nr);
+    add_root<T>(r, (T)x3, nr);
+}
+
+template <class T, int lib>
+__device__ __forceinline__ void one_root(double a, double b, double g, double h, T r[3], int& nr) {
+    double R = -(g / 2.0) + ccc_sqrt(h);
+    double S, U;
+    double Ra = R >= 0 ? R : -R;
+    S = lib == LIB_REFERENCE ? cbrt(Ra) : ccc_cbrt(Ra);
+    if (R < 0) S = -S;
+    double V = -(g / 2.0) - ccc_sqrt(h);
+    double Va = V >= 0 ? V : -V;
+    U = lib == LIB_REFERENCE ? cbrt(Va) : ccc_cbrt(Va);
+    if (V < 0) U = -U;
+    double x1 = (S + U) - (b / (3.0 * a));
+    add_root<T>(r, (T)x1, nr);
+}
+
+// roots of one class; r starts at -1
+template <class T, int lib>
+__device__ __forceinline__ void class_roots(int cls, double a, double b, double c, double d, double g, double h,
+                                            T r[3]) {
     r[0] = r[1] = r[2] = (T)-1;
     int nr = 0;
-    if (a == 0 && b == 0) {
-        return;     // linear case: the reference never stores its root
-    } else if (fabs(a) < CCC_EPS) {
-        double D = fmaT(c, c, -(4.0 * b * d));
-        if (D >= 0) {
-            D = ccc_sqrt(D);
-            double x1 = (-c + D) / (2.0 * b);
-            double x2 = (-c - D) / (2.0 * b);
-            add_root<T>(r, (T)x1, nr);
-            add_root<T>(r, (T)x2, nr);
-        }
-    } else {
-        double f = ((3.0 * c / a) - ((b * b) / (a * a))) / 3.0;
-        double b3 = 2 * ccc_cube_hi(b);
-        ccc_dd a2dd = ccc_sq_dd(a);
-        double a2 = a2dd.hi;
-        double a3 = ccc_certmul(a2dd.hi, a2dd.lo, 2, a).hi;
-        double p1 = b3 / a3;
-        double p2 = (b * c * 9) / a2;
-        double p3 = 27.0 * d / a;
-        double g = (p1 - p2 + p3) / 27.0;
-        double f3 = ccc_cube_hi(f);
-        // the reference's pow(g, 2) resolves (through std::pow's promotion) to CUDA's general
-        // pow(double, double), which is not always the rounded square
-        double g2 = lib == LIB_REFERENCE ? pow(g, 2.0) : g * g;
-        double h = g2 / 4.0 + f3 / 27.0;
-        if (f == 0 && g == 0 && h == 0) {
-            float k = (float)(d / a);
-            double x1;
-            float cr = lib == LIB_REFERENCE ? cbrtf(k >= 0 ? k : -k) : ccc_cbrtf(k >= 0 ? k : -k);
-            if (k >= 0) x1 = (double)(cr * -1);
-            else x1 = (double)cr;
-            add_root<T>(r, (T)x1, nr);
-        } else if (h <= 0) {
-            double i = ccc_sqrt(((g * g) / 4.0) - h);
-            double j, k, M, sn;
-            if (lib == LIB_REFERENCE) {
-                j = cbrt(i);
-                k = acos(-(g / (2 * i)));
-                M = cos(k / 3.0);
-                sn = sin(k / 3.0);
-            } else {
-                j = ccc_cbrt(i);
-                k = ccc_acos(-(g / (2 * i)));
-                M = ccc_cos(k / 3.0);
-                sn = ccc_sin(k / 3.0);
-            }
-            // N = sqrt(3) * sin(k/3) is fused into M + N and M - N and each result into
-            // L * (.) + P; the first root 2 j cos(k/3) - b/(3a) is rounded twice (unfused)
-            const double r3 = ccc_sqrt(3.0);
-            double L = j * -1;
-            double P = (b / (3.0 * a)) * -1;
-            double x1 = (2 * j) * M - (b / (3.0 * a));
-            double x2 = fmaT(L, fmaT(r3, sn, M), P);
-            double x3 = fmaT(L, fmaT(-r3, sn, M), P);
-            add_root<T>(r, (T)x1, nr);
-            add_root<T>(r, (T)x2, nr);
-            add_root<T>(r, (T)x3, nr);
-        } else {
-            double R = -(g / 2.0) + ccc_sqrt(h);
-            double S, U;
-            double Ra = R >= 0 ? R : -R;
-            S = lib == LIB_REFERENCE ? cbrt(Ra) : ccc_cbrt(Ra);
-            if (R < 0) S = -S;
-            double V = -(g / 2.0) - ccc_sqrt(h);
-            double Va = V >= 0 ? V : -V;
-            U = lib == LIB_REFERENCE ? cbrt(Va) : ccc_cbrt(Va);
-            if (V < 0) U = -U;
-            double x1 = (S + U) - (b / (3.0 * a));
-            add_root<T>(r, (T)x1, nr);
-        }
+    switch (cls) {
+        case CUBIC_QUAD: quad_roots<T>(b, c, d, r, nr); break;
+        case CUBIC_TRIPLE: triple_roots<T, lib>(a, d, r, nr); break;
+        case CUBIC_THREE: three_roots<T, lib>(a, b, g, h, r, nr); break;
+        case CUBIC_ONE: one_root<T, lib>(a, b, g, h, r, nr); break;
+        default: break;
     }
+}
+
+template <class T, int lib> __device__ __noinline__ void solve_cubic(double a, double b, double c, double d, T r[3]) {
+    double g, h;
+    int cls = cubic_prefix<lib>(a, b, c, d, g, h);
+    class_roots<T, lib>(cls, a, b, c, d, g, h, r);
 }
 
 // is_inside (collisions_continuous.cu:615-637)
@@ -489,11 +531,11 @@ template <class T> __device__ __forceinline__ bool ccd_filter(const MTet<T>& tet
 #define CCC_THICKNESS 2e-3   // collisions_impulses.cu:12-14
 
 // normalize(double3) = a * rsqrt(|a|^2) (utils.cu:91-93); the portable form uses 1 / sqrt
-__device__ __forceinline__ float rsqrt_lib(float n, int lib) { return lib == LIB_REFERENCE ? rsqrtf(n) : 1.0f / sqrtf(n); }
-__device__ __forceinline__ double rsqrt_lib(double n, int lib) { return lib == LIB_REFERENCE ? rsqrt(n) : 1.0 / ccc_sqrt(n); }
-template <class T> __device__ __forceinline__ V3<T> vnormalize(V3<T> a, int lib) {
+template <int lib> __device__ __forceinline__ float rsqrt_lib(float n) { return lib == LIB_REFERENCE ? rsqrtf(n) : 1.0f / sqrtf(n); }
+template <int lib> __device__ __forceinline__ double rsqrt_lib(double n) { return lib == LIB_REFERENCE ? rsqrt(n) : 1.0 / ccc_sqrt(n); }
+template <int lib, class T> __device__ __forceinline__ V3<T> vnormalize(V3<T> a) {
     T n = norm2(a);
-    return a * rsqrt_lib(n, lib);
+    return a * rsqrt_lib<lib>(n);
 }
 
 template <class T> struct Contact { V3<T> n; T vn, m0, m1; };
@@ -502,7 +544,7 @@ template <class T> struct Contact { V3<T> n; T vn, m0, m1; };
 // q holds the masses of the four tetrahedron points.  For vertex-face types the points
 // are first put in (face 0, face 1, face 2, vertex) order with selects: types 9..11 are
 // already in that order, types 12..14 have the vertex first.
-template <class T> __device__ __forceinline__ Contact<T> contact(const MTet<T>& tet, int k, T root, const T q[4], int lib) {
+template <class T, int lib> __device__ __forceinline__ Contact<T> contact(const MTet<T>& tet, int k, T root, const T q[4]) {
     Contact<T> ct;
     if (k < 9) {
         V3<T> th0 = at_time(tet, 0, root), th1 = at_time(tet, 1, root), th2 = at_time(tet, 2, root),
@@ -522,7 +564,7 @@ template <class T> __device__ __forceinline__ Contact<T> contact(const MTet<T>& 
         V3<T> dp0 = axpy(dv[0], dv[1] - dv[0], s);
         V3<T> dp1 = axpy(dv[2], dv[3] - dv[2], t);
         V3<T> c0 = axpy(v[0], dv[0], root), c1 = axpy(v[1], dv[1], root), c2 = axpy(v[2], dv[2], root);
-        V3<T> nd = vnormalize(cross(c1 - c0, c2 - c0), lib);
+        V3<T> nd = vnormalize<lib>(cross(c1 - c0, c2 - c0));
         if (dot(p1 - p0, nd) < 0) nd = nd * (T)-1;
         ct.n = nd;
         ct.vn = dot(dp1 - dp0, nd);
@@ -550,7 +592,7 @@ template <class T> __device__ __forceinline__ Contact<T> contact(const MTet<T>& 
     V3<T> pt = lin3(F0, u, F1, vv, F2, w);
     V3<T> dpt = lin3(D0, u, D1, vv, D2, w);
     V3<T> c0 = axpy(F0, D0, root), c1 = axpy(F1, D1, root), c2 = axpy(F2, D2, root);
-    V3<T> nd = vnormalize(cross(c1 - c0, c2 - c0), lib);
+    V3<T> nd = vnormalize<lib>(cross(c1 - c0, c2 - c0));
     if (dot(FV - pt, nd) < 0) nd = nd * (T)-1;
     ct.vn = dot(DV - dpt, nd);
     if (inv) nd = nd * (T)-1;

@@ -50,6 +50,11 @@ struct __align__(16) TNode {
 static constexpr int TRAV_THREADS = 128;
 static constexpr int STACK_DEPTH = 64;        // STACK_SIZE (flags.h:26-29)
 static constexpr int NARROW_THREADS = 128;
+// resident narrow-phase blocks per SM the register allocation is sized for
+#ifndef CCC_NARROW_MIN_BLOCKS
+#define CCC_NARROW_MIN_BLOCKS 5
+#endif
+static constexpr int NARROW_MIN_BLOCKS = CCC_NARROW_MIN_BLOCKS;
 
 // mesh containing element g where base(m) = off[m] - m * shift (shift 0: triangles,
 // shift 1: internal nodes); off has M + 1 entries
@@ -492,21 +497,32 @@ template <class T> struct CornerSink {
 
 // Continuous narrow phase (collisions_continuous.cu:14-765, collisions_impulses.cu:24-1067),
 // warp-cooperative.  Each warp takes 32 candidate pairs: every lane runs the shared-vertex
-// test and the 15 swept sub-box tests of its pair, the surviving (pair, type) items are
-// staged in shared memory, and then all 32 lanes solve items in lockstep, each loading only
-// the four points its item needs.  A one-thread-per-pair loop leaves most lanes idle, since
-// pairs have 0 to 15 cubic solves each.
-template <class T, int MODE, class Sink>
-__global__ void __launch_bounds__(NARROW_THREADS, 3)
+// test and the 15 swept sub-box tests of its pair, and the surviving (pair, type) items are
+// staged in shared memory.  The warp then works through them in batches of NARROW_BATCH in
+// three uniform phases: (1) cubic coefficients and the solver prefix of every item, which
+// sorts the items by solver branch; (2) the roots of one branch at a time; (3) the root
+// filter and the output of every root in [0, 1].  Items take different branches and have
+// 0 to 3 roots, so solving them in arrival order would leave most lanes idle.
+static constexpr int NARROW_BATCH = 64;
+
+template <class T, int MODE, class Sink, int LIB>
+__global__ void __launch_bounds__(NARROW_THREADS, NARROW_MIN_BLOCKS)
 k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ x0,
              const T* __restrict__ x1, Forest F, long long* __restrict__ rows, T* __restrict__ times, int max_per_tri,
-             int* __restrict__ mesh_counters, Sink sink, int lib) {
+             int* __restrict__ mesh_counters, Sink sink) {
     constexpr int WARPS = NARROW_THREADS / 32;
-    const int M = forest_size(F);
+    constexpr int NB = NARROW_BATCH;
     __shared__ unsigned short items[WARPS][32 * 15];
     __shared__ int2 pairs[WARPS][32];
+    __shared__ double rec[WARPS][6][NB];                 // a, b, c, d, g, h per item of a batch
+    __shared__ unsigned short rec_item[WARPS][NB];
+    __shared__ unsigned char clist[WARPS][4][NB];        // batch positions per class (QUAD..ONE)
+    __shared__ unsigned char root_rec[WARPS][3 * NB];
+    __shared__ T root_val[WARPS][3 * NB];
+    const int M = forest_size(F);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu;
+    const unsigned lt = (1u << lane) - 1u;
     const int n = min(*(volatile int*)&hdr->cand_count, cand_cap);
     for (long long base = ((long long)blockIdx.x * WARPS + warp) * 32; base < n;
          base += (long long)gridDim.x * WARPS * 32) {
@@ -550,19 +566,75 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
         }
         pairs[warp][lane] = pr;
         __syncwarp();
-        for (int it = lane; it < total; it += 32) {
-            int item = items[warp][it];
-            int k = item & 15;
-            int2 q = pairs[warp][item >> 4];
-            MTet<T> tet = load_tet(x0, x1, q.x, q.y, k);
-            T cf[4];
-            cubic_coeffs(tet, cf);
-            T rr[3];
-            solve_cubic<T>((double)cf[0], (double)cf[1], (double)cf[2], (double)cf[3], rr, lib);
+        for (int b0 = 0; b0 < total; b0 += NB) {
+            const int nb = min(NB, total - b0);
+            // (1) coefficients and solver prefix; class lists
+            int ccount[4] = {0, 0, 0, 0};
 #pragma unroll 1
-            for (int s = 0; s < 3; ++s) {
-                T root = rr[s];
-                if (!(root >= 0 && root <= 1)) continue;
+            for (int r0 = 0; r0 < NB; r0 += 32) {
+                const int ri = r0 + lane;
+                int cls = CUBIC_NONE;
+                if (ri < nb) {
+                    int item = items[warp][b0 + ri];
+                    int k = item & 15;
+                    int2 q = pairs[warp][item >> 4];
+                    MTet<T> tet = load_tet(x0, x1, q.x, q.y, k);
+                    T cf[4];
+                    cubic_coeffs(tet, cf);
+                    double g, h;
+                    cls = cubic_prefix<LIB>((double)cf[0], (double)cf[1], (double)cf[2], (double)cf[3], g, h);
+                    rec[warp][0][ri] = (double)cf[0];
+                    rec[warp][1][ri] = (double)cf[1];
+                    rec[warp][2][ri] = (double)cf[2];
+                    rec[warp][3][ri] = (double)cf[3];
+                    rec[warp][4][ri] = g;
+                    rec[warp][5][ri] = h;
+                    rec_item[warp][ri] = (unsigned short)item;
+                }
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc) {
+                    unsigned m = __ballot_sync(FULL, cls == cc + 1);
+                    if (cls == cc + 1) clist[warp][cc][ccount[cc] + __popc(m & lt)] = (unsigned char)ri;
+                    ccount[cc] += __popc(m);
+                }
+            }
+            __syncwarp();
+            // (2) roots, one class at a time; roots in [0, 1] go to the root list
+            int nroots = 0;
+#pragma unroll 1
+            for (int cc = 0; cc < 4; ++cc) {
+#pragma unroll 1
+                for (int j0 = 0; j0 < ccount[cc]; j0 += 32) {
+                    const int j = j0 + lane;
+                    T rr[3] = {(T)-1, (T)-1, (T)-1};
+                    int ri = 0;
+                    if (j < ccount[cc]) {
+                        ri = clist[warp][cc][j];
+                        class_roots<T, LIB>(cc + 1, rec[warp][0][ri], rec[warp][1][ri], rec[warp][2][ri],
+                                            rec[warp][3][ri], rec[warp][4][ri], rec[warp][5][ri], rr);
+                    }
+#pragma unroll
+                    for (int s = 0; s < 3; ++s) {
+                        bool keep = j < ccount[cc] && (rr[s] >= 0 && rr[s] <= 1);
+                        unsigned m = __ballot_sync(FULL, keep);
+                        if (keep) {
+                            int at = nroots + __popc(m & lt);
+                            root_rec[warp][at] = (unsigned char)ri;
+                            root_val[warp][at] = rr[s];
+                        }
+                        nroots += __popc(m);
+                    }
+                }
+            }
+            __syncwarp();
+            // (3) filter and output
+#pragma unroll 1
+            for (int j = lane; j < nroots; j += 32) {
+                int item = rec_item[warp][root_rec[warp][j]];
+                int k = item & 15;
+                int2 q = pairs[warp][item >> 4];
+                T root = root_val[warp][j];
+                MTet<T> tet = load_tet(x0, x1, q.x, q.y, k);
                 if (!ccd_filter(tet, k, root)) continue;
                 if (MODE == CCD_ROWS) {
                     OutRegion R = out_region(F, M, q.x, max_per_tri);
@@ -579,10 +651,11 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
 #pragma unroll
                     for (int pt = 0; pt < 4; ++pt)
                         mq[pt] = sink.masses[(long long)(tet_side(k, pt) ? q.y : q.x) * 3 + tet_corner(k, pt)];
-                    Contact<T> ct = contact(tet, k, root, mq, lib);
+                    Contact<T> ct = contact<T, LIB>(tet, k, root, mq);
                     sink.add(tet, q.x, q.y, k, root, ct, F, M, &hdr->status);
                 }
             }
+            __syncwarp();
         }
         __syncwarp();
     }
@@ -618,11 +691,11 @@ k_prox_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const 
 // compute_impulses_from_collisions (collisions_impulses.cu:1738-1880) on caller rows.
 // Rows with an index outside [0, F) or a type outside [0, 15) are skipped (the reference
 // reads out of bounds on its -1 padding rows).
-template <class T>
+template <class T, int LIB>
 __global__ void __launch_bounds__(NARROW_THREADS)
 k_impulses_from_rows(const long long* __restrict__ rows, const T* __restrict__ roots, int B, long long N, int F,
                      const T* __restrict__ x0, const T* __restrict__ x1, const T* __restrict__ masses,
-                     T* __restrict__ dv_out, T* __restrict__ dx_out, int* __restrict__ cnt_out, WsHeader* hdr, int lib) {
+                     T* __restrict__ dv_out, T* __restrict__ dx_out, int* __restrict__ cnt_out, WsHeader* hdr) {
     long long total = (long long)B * N;
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < total;
          r += (long long)gridDim.x * blockDim.x) {
@@ -635,7 +708,7 @@ k_impulses_from_rows(const long long* __restrict__ rows, const T* __restrict__ r
         MTet<T> tet = load_tet(x0, x1, gi, gj, k);
         T mq[4];
         for (int pt = 0; pt < 4; ++pt) mq[pt] = masses[(tet_side(k, pt) ? gj : gi) * 3 + tet_corner(k, pt)];
-        Contact<T> ct = contact(tet, k, root, mq, lib);
+        Contact<T> ct = contact<T, LIB>(tet, k, root, mq);
         apply_impulse(tet, gi, gj, k, root, ct, dv_out, dx_out, cnt_out);
     }
 }
@@ -662,7 +735,7 @@ static __global__ void k_debug_math(int op, const double* __restrict__ in, doubl
             o[1] = d.lo;
             break;
         }
-        case 5: solve_cubic<double>(a[0], a[1], a[2], a[3], o, LIB_PORTABLE); break;
+        case 5: solve_cubic<double, LIB_PORTABLE>(a[0], a[1], a[2], a[3], o); break;
         case 6: o[0] = cbrt(a[0]); break;
         case 7: o[0] = acos(a[0]); break;
         case 8: o[0] = cos(a[0]); break;
@@ -705,7 +778,8 @@ static __global__ void k_debug_stage(int op, int lib, const double* __restrict__
     if (op == 0) {
         cubic_coeffs(t, o);
     } else if (op == 1) {
-        solve_cubic<double>(a[0], a[1], a[2], a[3], o, lib);
+        if (lib == LIB_REFERENCE) solve_cubic<double, LIB_REFERENCE>(a[0], a[1], a[2], a[3], o);
+        else solve_cubic<double, LIB_PORTABLE>(a[0], a[1], a[2], a[3], o);
     } else if (op == 2) {
         o[0] = ccd_filter(t, (int)a[24], a[25]) ? 1.0 : 0.0;
     } else if (op == 4) {
@@ -729,7 +803,8 @@ static __global__ void k_debug_stage(int op, int lib, const double* __restrict__
         o[2] = x * x;
     } else if (op == 3) {
         double q[4] = {a[26], a[27], a[28], a[29]};
-        Contact<double> ct = contact(t, (int)a[24], a[25], q, lib);
+        Contact<double> ct = lib == LIB_REFERENCE ? contact<double, LIB_REFERENCE>(t, (int)a[24], a[25], q)
+                                                  : contact<double, LIB_PORTABLE>(t, (int)a[24], a[25], q);
         o[0] = ct.n.x; o[1] = ct.n.y; o[2] = ct.n.z; o[3] = ct.vn; o[4] = ct.m0; o[5] = ct.m1;
     }
 }

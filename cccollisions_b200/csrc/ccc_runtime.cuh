@@ -32,6 +32,19 @@ inline int grid_for(int64_t n, int threads) { return (int)((n + threads - 1) / t
         ::ccc::timing_after(slot__, s);           \
     } while (0)
 
+// Run the statement(s) with LIBV bound to the current math library (MathLib) as a
+// compile-time constant, for kernels templated on it.
+#define CCC_WITH_LIB(...)                                              \
+    do {                                                               \
+        if (::ccc::g_math_lib == 0) {                                  \
+            constexpr int LIBV = 0;                                    \
+            __VA_ARGS__;                                               \
+        } else {                                                       \
+            constexpr int LIBV = 1;                                    \
+            __VA_ARGS__;                                               \
+        }                                                              \
+    } while (0)
+
 #define CCC_LAUNCH_CHECK()                                         \
     do {                                                           \
         cudaError_t e__ = cudaGetLastError();                      \
