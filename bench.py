@@ -1,27 +1,35 @@
 """Benchmark of the collision-handling step on B200 (one JSON line on rank 0).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload W]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload (default ``cloth_sphere``): the plain continuous-collision step of the reference's
-API on a 128x128 cloth (32,258 triangles) falling onto a level-5 icosphere (20,480
-triangles), fp64, as one 52,738-triangle soup: ``bvh_motion`` + ``find_collisions_continuous``
-(max 16 candidates / 16 collisions per triangle).  Metric: triangle-steps per second (one
-triangle carried through one full step).
+Metric: triangle-steps per second (one triangle carried through one full collision step of
+its mesh: tree refit, traversal, continuous narrow phase), batched and served against the
+plain per-mesh path, with exact pair sets and p50 / p99 latency.
 
-* ``value``: inputs resident in HBM, outputs and scratch preallocated, C ABI calls on one
-  stream, CUDA events around every step, L2 flushed (256 MiB write) between steps outside
-  the timed events.
-* ``e2e``: the public drop-in API from pinned host buffers: H2D copy of both triangle
-  soups, bvh_motion, find_collisions_continuous (which reads back its status word), a
-  count of valid rows and a D2H copy of those rows and times.
-* ``roofline``: the kernel with the largest share of the timed region, its algorithmic
-  bytes per launch over its CUDA-event duration, against MEASURED_PEAKS.json.
-* ``cpu_baseline``: the same step on the host cores with the C++ oracle (OpenMP).
+* ``value`` — batched form: 64 cloth-over-sphere meshes of log-uniform size (1e3..1e5 cloth
+  triangles plus a level-5 icosphere each, fp64, about 2.6 M triangles) resident in one
+  engine block; one step = one CUDA-graph replay of refit + traversal + continuous narrow
+  phase over all meshes (trees built once beforehand); CUDA events around every step, L2
+  flushed (256 MiB write) between steps outside the events (inputs are larger than L2 too).
+* ``plain`` — the same 64 meshes through the reference-format API one mesh at a time
+  (bvh_motion + find_collisions_continuous, as the reference's caller does); its rows and
+  times are compared with the batched form's as multisets (``pair_sets_equal``).
+* ``served`` — a Poisson stream of impulse-loop requests (rate 2,000/s, meshes of
+  log-uniform 2e3..2e5 triangles as in the impulse workload) under a 40 GB engine budget:
+  throughput (request triangles over the makespan) and p50 / p99 latency (arrival to result
+  on the host).
+* ``e2e`` — the batched step through the public engine API from pinned host buffers: H2D of
+  both soups of every mesh, the graph replay, the per-mesh row counts and a D2H copy of every
+  row and time.
+* ``roofline`` — the dominant kernel (CUDA-event timing of the same step run ungraphed)
+  against MEASURED_PEAKS.json; ``refit_roofline`` / ``build_roofline`` the tree kernels;
+  ``fp64`` the narrow phase's arithmetic rate.
+* ``cpu_baseline`` — the oracle (C++ restatement of the reference pipeline, OpenMP) on a
+  bounded sample of the batched meshes on the host cores.
 
-Multi-GPU: the step does not shard (one mesh, no exchange), so N ranks run N independent
-replicas ("replicas only"); value is the total over ranks divided by the slowest rank.
-``--impl reference`` times the CPU implementation (the oracle restatement of the
-reference's algorithm) on rank 0 only.
+Multi-GPU: meshes are independent and the step has no exchange, so N ranks run N replicas
+("replicas only"); value is the total over ranks divided by the slowest rank.
+``--impl reference`` times the CPU implementation of the path (the oracle) on rank 0 only.
 """
 from __future__ import annotations
 
@@ -32,24 +40,30 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
+from collections import Counter
 
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "triangle-steps/sec"
+METRIC = "triangle-steps/sec batched+served vs plain (exact pair sets); p50/p99 latency"
+UNIT = "triangle-steps/s"
+MAXC, MAXCOL = 32, 16            # no candidate overflow on any of the 64 meshes
+FP64_PEAK_NOMINAL_GFLOPS = 37000.0   # B200 FP64 datasheet figure (not measured here)
+FLOPS_PER_SUBTEST = 252          # coefficients 162 + Cardano and filter 90 (transcendentals as 1)
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cloth_sphere", choices=["cloth_sphere"])
+    ap.add_argument("--meshes", type=int, default=64)
+    ap.add_argument("--served-requests", type=int, default=160)
+    ap.add_argument("--served-plain-sample", type=int, default=12)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     return ap.parse_args()
 
@@ -117,201 +131,326 @@ class ClockSampler:
         return out
 
 
-def cpu_baseline(x0, x1, seconds):
-    """Oracle (C++ restatement of the reference pipeline) on the host cores."""
+def batched_meshes(n):
+    from cccollisions_b200 import workloads as W
+    return W.batched(n)
+
+
+def cpu_sample(meshes, seconds):
+    """Oracle (C++ restatement of the reference pipeline, all host threads) over the meshes
+    in order until `seconds` have passed: (triangle-steps/s, threads, description)."""
     from oracle import oracle as O
     O.build()
     nthreads = O.num_threads()
-    F = x0.shape[1]
-    reps = 0
+    tris, done = 0, 0
     t0 = time.perf_counter()
-    while True:
-        bb, tr = O.bvh(x0[0], x1[0])
-        O.ccd(bb, tr, x0[0], x1[0], nthreads=nthreads)
-        reps += 1
-        if time.perf_counter() - t0 >= seconds or reps >= 200:
+    for x0, x1 in meshes:
+        bb, tr = O.bvh(x0, x1)
+        O.ccd(bb, tr, x0, x1, nthreads=nthreads)
+        tris += x0.shape[0]
+        done += 1
+        if time.perf_counter() - t0 >= seconds:
             break
     dt = time.perf_counter() - t0
-    return {"value": reps * F / dt, "unit": METRIC, "cores": nthreads, "kind": "port",
-            "sample": f"{reps} full steps of the {F}-triangle cloth_sphere workload (bvh_motion + continuous "
-                      f"collisions), {dt:.1f} s"}
+    return tris / dt, nthreads, f"first {done} of the {len(meshes)} batched meshes ({tris} triangles: bvh_motion + " \
+                                f"continuous collisions per mesh), {dt:.1f} s"
 
 
-def alg_bytes(kernel, F, cand, rows):
-    """Algorithmic bytes of one launch (fp64, motion) for the kernels of this step."""
-    tri = 72  # one fp64 triangle (9 doubles)
-    if kernel == "k_leaf_rows":          # read x0, x1; write leaf box (48 B) + 3 tree fields (24 B)
-        return F * (2 * tri + 48 + 24)
-    if kernel == "k_karras_identity":    # write left/right/id of F-1 internal rows + 2F-2 parent fields
-        return (F - 1) * 24 + (2 * F - 2) * 8
-    if kernel == "k_refit":              # read parent links + 2 child boxes, write one box per internal node
-        return (F - 1) * (2 * 48 + 48 + 24) + F * 8
-    if kernel == "k_import_nodes":       # read internal tree rows + child boxes/ids, write 64 B node
-        return (F - 1) * (32 + 2 * 48 + 64) + F * 8
-    if kernel == "k_import_rightmost":   # parent links, node refs, rightmost writes
-        return F * 8 + (F - 1) * (8 + 16 + 4 + 4)
-    if kernel == "k_traverse":           # query box + id per leaf, every node once, candidate pairs out
-        return F * (48 + 8) + (F - 1) * 64 + cand * 8
-    if kernel == "k_ccd_narrow":         # candidate pair in, two moving triangles (x0, x1), rows + times out
-        return cand * (8 + 2 * 2 * tri) + rows * (24 + 8)
-    if kernel == "k_uniform_offsets":
-        return 8
-    return 0
+def refit_bytes(F):
+    """Algorithmic bytes of one refit of a motion tree over F fp64 triangles (fp32 boxes)."""
+    return F * 2 * 72 + (2 * F - 1) * 24 + 2 * (F - 1) * 24 + (F - 1) * 8
+
+
+def build_bytes(F):
+    """Algorithmic bytes of one motion-tree build (positions, keys, 4 radix passes, topology,
+    boxes)."""
+    return F * 2 * 72 + F * 8 + 4 * F * 16 + (F - 1) * 12 + (2 * F - 1) * 24 + 2 * (F - 1) * 24
+
+
+def _ms(rows, times):
+    return Counter(zip(map(tuple, np.asarray(rows).tolist()), np.asarray(times, dtype=np.float64).tolist()))
 
 
 def run_ours(args, rank, world, dev):
-    import ctypes
     import torch
 
-    from cccollisions_b200 import _native as N
-    from cccollisions_b200 import api, workloads as W
+    import cccollisions_b200 as C
+    from cccollisions_b200 import _native as N, api
+    from cccollisions_b200.engine import Engine
 
-    lib = N.lib()
-    x0, x1 = W.cloth_sphere()
-    B, F = x0.shape[0], x0.shape[1]
-    maxc = maxcol = 16
-    X0 = torch.from_numpy(x0).to(dev)
-    X1 = torch.from_numpy(x1).to(dev)
-    bboxes = torch.empty((B, 2 * F - 1, 6), dtype=torch.float64, device=dev)
-    tree = torch.empty((B, 2 * F - 1, 4), dtype=torch.int64, device=dev)
-    rows = torch.empty((B, F * maxcol, 3), dtype=torch.int64, device=dev)
-    times = torch.empty((B, F * maxcol, 1), dtype=torch.float64, device=dev)
-    ws_b = torch.empty(lib.ccc_workspace_size(N.OP_BVH, B, F, 0), dtype=torch.uint8, device=dev)
-    ws_c = torch.empty(lib.ccc_workspace_size(N.OP_CONTINUOUS, B, F, maxc), dtype=torch.uint8, device=dev)
+    meshes = batched_meshes(args.meshes)
+    Fs = [x0.shape[0] for x0, _ in meshes]
+    total = sum(Fs)
+    warm = max(args.warmup, 3)
+    stream = torch.cuda.Stream(dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    stream = torch.cuda.current_stream(dev)
-    sp = ctypes.c_void_p(stream.cuda_stream)
-    P = lambda t: ctypes.c_void_p(t.data_ptr())
+    ev = lambda: torch.cuda.Event(enable_timing=True)
 
-    def step():
-        rows.fill_(-1)
-        times.fill_(-1)
-        rc = lib.ccc_bvh(1, P(X0), P(X1), B, F, P(bboxes), P(tree), P(ws_b), ws_b.numel(), sp)
-        assert rc == 0
-        rc = lib.ccc_find_collisions_continuous(1, P(bboxes), P(tree), P(X0), P(X1), None, B, F, maxc, maxcol,
-                                                P(rows), P(times), P(ws_c), ws_c.numel(), sp)
-        assert rc == 0
-
-    for _ in range(max(args.warmup, 3)):
-        step()
-    torch.cuda.synchronize(dev)
-    st = (ctypes.c_int32 * 3)()
-    lib.ccc_read_status(P(ws_c), 1, st, sp)
-    status, cand, nrows = int(st[0]), int(st[1]), int(st[2])
-
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize(dev)
-    launches0 = N.kernel_launches()
-    N.timing_begin()
-    with ClockSampler(dev.index if dev.index is not None else 0) as clk:
-        for i in range(args.steps):
-            flush.fill_(i & 0xFF)            # evict L2 between steps (outside the events)
-            ev[i][0].record(stream)
-            step()
-            ev[i][1].record(stream)
-        torch.cuda.synchronize(dev)
-    kern = N.timing_end()
-    launches = N.kernel_launches() - launches0
-    step_ms = [a.elapsed_time(b) for a, b in ev]
+    # ---------------- batched form: resident engine, graph replay
+    eng = Engine(tri_capacity=total + 64, mesh_capacity=len(meshes), max_candidates_per_triangle=MAXC,
+                 max_collisions_per_triangle=MAXCOL, device=dev)
+    sids = [eng.add_mesh(f) for f in Fs]
+    for sid, (x0, x1) in zip(sids, meshes):
+        eng.upload_soup(sid, x0, x1)
+    with torch.cuda.stream(stream):
+        eng.set_active(sids)
+        eng.build(sids)
+        a, b = ev(), ev()
+        a.record(stream)
+        eng.build(sids)
+        b.record(stream)
+        stream.synchronize()
+        build_ms = a.elapsed_time(b)
+        shape = eng.autotune()
+        eng.capture(N.ENGINE_OP_CCD, stream=stream)
+        for _ in range(warm):
+            eng.replay(N.ENGINE_OP_CCD)
+        stream.synchronize()
+        cnt = eng.counters()
+        st = eng.state(sids)
+        if world > 1:
+            torch.distributed.barrier()
+        steps = []
+        launches0 = N.kernel_launches()
+        with ClockSampler(dev.index if dev.index is not None else 0) as clk:
+            for i in range(args.steps):
+                flush.fill_(i & 0xFF)
+                a, b = ev(), ev()
+                a.record(stream)
+                eng.replay(N.ENGINE_OP_CCD)
+                b.record(stream)
+                steps.append((a, b))
+            stream.synchronize()
+        launches = N.kernel_launches() - launches0
+        step_ms = [x.elapsed_time(y) for x, y in steps]
+        # per-kernel times of the same step, ungraphed
+        N.timing_begin()
+        for _ in range(3):
+            eng.ccd()
+        kern = N.timing_end()
+        stream.synchronize()
     total_ms = sum(step_ms)
     if world > 1:
         t = torch.tensor([total_ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
-        torch.distributed.barrier()
     ms_per_step = total_ms / args.steps
-    value = world * F * args.steps / (total_ms / 1e3)
+    value = world * total * args.steps / (total_ms / 1e3)
+    batched_rows = {sid: _ms(*[x.cpu().numpy() for x in eng.collisions(sid, int(n))]) for sid, n in
+                    zip(sids, st["rows"])}
 
-    # ---- roofline of the dominant kernel
-    peak, peak_kind = load_peaks()
-    dom = max(kern.items(), key=lambda kv: kv[1][0])
-    dname, (dms, dcount) = dom
-    per_launch_ms = dms / dcount
-    abytes = alg_bytes(dname, F, cand, nrows)
-    achieved = abytes / (per_launch_ms / 1e3) / 1e9
-    share = {k: round(v[0] / max(total_ms, 1e-9), 4) for k, v in kern.items()}
-
-    # ---- end to end through the public API from pinned host memory
-    hx0 = torch.from_numpy(x0).pin_memory()
-    hx1 = torch.from_numpy(x1).pin_memory()
-    api.CHECK_STATUS = True
-    e2e_ev = []
-    d2h = 0
-    for i in range(max(args.warmup, 3) + args.steps):
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        flush.fill_(i & 0xFF)
-        a.record(stream)
-        dX0 = hx0.to(dev, non_blocking=True)
-        dX1 = hx1.to(dev, non_blocking=True)
-        import cccollisions_b200 as C
-        bb, tr = C.bvh_motion(dX0, dX1)
-        r, t = C.find_collisions_continuous(bb, tr, dX0, dX1, maxc, maxcol)
-        n = int((r[0, :, 0] >= 0).sum().item())
-        hr = r[0, :n].cpu()
-        ht = t[0, :n].cpu()
-        b.record(stream)
-        torch.cuda.synchronize(dev)
-        if i >= max(args.warmup, 3):
-            e2e_ev.append(a.elapsed_time(b))
-            d2h = 8 + hr.numel() * 8 + ht.numel() * 8
-    e2e_ms = sum(e2e_ev) / len(e2e_ev)
+    # ---------------- e2e through the engine API from pinned host memory
+    hx = [(torch.from_numpy(x0).pin_memory(), torch.from_numpy(x1).pin_memory()) for x0, x1 in meshes]
+    nrow = [int(n) for n in st["rows"]]
+    hrows = [torch.empty((n, 3), dtype=torch.int64).pin_memory() for n in nrow]
+    htimes = [torch.empty((n,), dtype=torch.float64).pin_memory() for n in nrow]
+    e2e = []
+    with torch.cuda.stream(stream):
+        for i in range(warm + args.steps):
+            flush.fill_(i & 0xFF)
+            stream.synchronize()
+            t0 = time.perf_counter()
+            for sid, (h0, h1) in zip(sids, hx):
+                eng.upload_soup(sid, h0, h1, non_blocking=True)
+            eng.replay(N.ENGINE_OP_CCD)
+            s2 = eng.state(sids)
+            for j, (sid, n) in enumerate(zip(sids, s2["rows"])):
+                r, tt = eng.collisions(sid, int(n))
+                hrows[j][:int(n)].copy_(r, non_blocking=True)
+                htimes[j][:int(n)].copy_(tt, non_blocking=True)
+            stream.synchronize()
+            if i >= warm:
+                e2e.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = statistics.mean(e2e)
     if world > 1:
-        t_ = torch.tensor([e2e_ms], device=dev)
-        torch.distributed.all_reduce(t_, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t_.item())
-    e2e_value = world * F / (e2e_ms / 1e3)
+        t = torch.tensor([e2e_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = sum(x0.nbytes + x1.nbytes for x0, x1 in meshes)
+    d2h = sum(n * 32 for n in nrow) + 4 * len(sids) * 4
+
+    # ---------------- plain per-mesh path through the reference-format API
+    X = [(torch.from_numpy(x0).to(dev), torch.from_numpy(x1).to(dev)) for x0, x1 in meshes]
+    api.CHECK_STATUS = True
+    plain_out = None
+
+    def plain():
+        out = []
+        for X0, X1 in X:
+            bb, tr = C.bvh_motion(X0[None], X1[None])
+            out.append(C.find_collisions_continuous(bb, tr, X0[None], X1[None], MAXC, MAXCOL))
+        return out
+
+    torch.cuda.synchronize(dev)
+    for _ in range(warm):
+        plain_out = plain()
+    torch.cuda.synchronize(dev)
+    pms = []
+    for i in range(args.steps):
+        flush.fill_(i & 0xFF)
+        torch.cuda.synchronize(dev)
+        a, b = ev(), ev()
+        a.record()
+        plain_out = plain()
+        b.record()
+        torch.cuda.synchronize(dev)
+        pms.append(a.elapsed_time(b))
+    plain_ms = statistics.mean(pms)
+    equal = True
+    for sid, (rows, times) in zip(sids, plain_out):
+        r = rows[0].cpu().numpy()
+        k = int((r[:, 0] >= 0).sum())
+        equal &= _ms(r[:k], times[0, :k, 0].cpu().numpy()) == batched_rows[sid]
+
+    # ---------------- rooflines
+    peak, peak_kind = load_peaks()
+    dname, (dms, dcount) = max(kern.items(), key=lambda kv: kv[1][0])
+    per_launch = dms / dcount
+    narrow_bytes = cnt["candidates"] * (8 + 2 * 2 * 72) + int(sum(nrow)) * 32
+    achieved = narrow_bytes / (per_launch / 1e3) / 1e9 if dname == "k_ccd_narrow" else None
+    refit_ms = kern.get("k_engine_refit", (float("nan"), 1))
+    refit_ms = refit_ms[0] / refit_ms[1]
+    rb = sum(refit_bytes(f) for f in Fs)
+    bb_ = sum(build_bytes(f) for f in Fs)
+    fp64_gflops = cnt["subtests"] * FLOPS_PER_SUBTEST / (kern["k_ccd_narrow"][0] / kern["k_ccd_narrow"][1] / 1e3) / 1e9
+    eng.close()
 
     result = None
     if rank == 0:
         clocks = clk.summary()
         result = {
-            "metric": METRIC, "value": value, "unit": "triangle-steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cloth + icosphere)",
-            "config": {"workload": "cloth_sphere: plain CCD step, bvh_motion + find_collisions_continuous",
-                       "triangles": F, "batch": B, "max_candidates_per_triangle": maxc,
-                       "max_collisions_per_triangle": maxcol, "l2": "flushed between steps (256 MiB write)",
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": warm,
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded cloth grids + icospheres)",
+            "config": {"workload": f"batched: {len(meshes)} cloth+icosphere meshes, log-uniform 1e3..1e5 cloth "
+                                   f"triangles + 20,480 sphere triangles each, one CUDA-graph replay per step",
+                       "triangles": total, "meshes": len(meshes), "max_candidates_per_triangle": MAXC,
+                       "max_collisions_per_triangle": MAXCOL, "positions": "fp64", "tree_boxes": "fp32",
+                       "l2": "flushed between steps (256 MiB write); inputs (377 MB) larger than L2",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "candidates": cand, "collision_rows": nrows, "status": status},
-            "e2e": {"value": e2e_value, "unit": "triangle-steps/s", "ms_per_step": e2e_ms,
-                    "h2d_bytes_per_step": int(x0.nbytes + x1.nbytes), "d2h_bytes_per_step": int(d2h)},
+                       "autotuned_shape": shape, "candidates": cnt["candidates"], "subtests": cnt["subtests"],
+                       "roots_in_unit_interval": cnt["roots"], "collision_rows": int(sum(nrow)),
+                       "status": cnt["status"]},
+            "plain": {"value": world * total / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
+                      "path": "per mesh: bvh_motion + find_collisions_continuous (reference-format API)"},
+            "batched_over_plain": plain_ms / ms_per_step,
+            "pair_sets_equal": bool(equal),
+            "e2e": {"value": world * total / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "roofline": {"kernel": dname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
-                         "alg_bytes_per_launch": abytes, "launch_ms": per_launch_ms},
-            "kernel_share": share,
-            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kern.items()},
+                         "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                         "traffic": None, "alg_bytes_per_launch": narrow_bytes, "launch_ms": per_launch,
+                         "note": "the narrow phase is FP64-latency bound; see fp64"},
+            "fp64": {"kernel": "k_ccd_narrow", "achieved_gflops": fp64_gflops,
+                     "peak_gflops": FP64_PEAK_NOMINAL_GFLOPS, "peak_source": "nominal (B200 datasheet)",
+                     "frac": fp64_gflops / FP64_PEAK_NOMINAL_GFLOPS, "flops_per_subtest": FLOPS_PER_SUBTEST},
+            "refit_roofline": {"kernel": "k_engine_refit", "bound": "hbm", "alg_bytes": rb, "launch_ms": refit_ms,
+                               "achieved": rb / (refit_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                               "frac": rb / (refit_ms / 1e3) / 1e9 / peak},
+            "build_roofline": {"kernels": "bounds, Morton, radix sort, Karras, refit", "bound": "hbm",
+                               "alg_bytes": bb_, "ms": build_ms, "achieved": bb_ / (build_ms / 1e3) / 1e9,
+                               "peak": peak, "unit": "GB/s", "frac": bb_ / (build_ms / 1e3) / 1e9 / peak},
+            "kernel_ms_per_step": {k: v[0] / v[1] for k, v in kern.items()},
+            "kernel_share": {k: round(v[0] / sum(x[0] for x in kern.values()), 4) for k, v in kern.items()},
             "gpu_launches": int(launches),
             "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
         }
-        if world == 1:
-            result["cpu_baseline"] = cpu_baseline(x0, x1, args.cpu_seconds)
-    return result
+    return result, meshes
+
+
+def plain_loop(r, dev, max_iter=50):
+    """One impulse-loop request through the reference-format API, as a caller of the reference
+    writes it: per iteration bvh_motion + compute_impulses on the soups, then each vertex moves
+    by the average correction of its corners (torch index_add).  Returns iterations."""
+    import torch
+
+    import cccollisions_b200 as C
+    faces = torch.from_numpy(r.faces.astype(np.int64)).to(dev)
+    v0 = torch.from_numpy(r.verts0).to(dev)
+    v1 = torch.from_numpy(r.verts1).to(dev).clone()
+    vel = torch.from_numpy(r.vel).to(dev).clone()
+    m = torch.from_numpy(r.masses).to(dev)[None].contiguous()
+    x0 = v0[faces][None].contiguous()
+    idx = faces.reshape(-1)
+    V = v0.shape[0]
+    for it in range(max_iter):
+        x1 = v1[faces][None].contiguous()
+        bb, tr = C.bvh_motion(x0, x1)
+        dv, dx, cnt = C.compute_impulses(bb, tr, x0, x1, m, MAXC, MAXCOL)
+        c = cnt[0].reshape(-1).to(v1.dtype)
+        if float(c.sum()) == 0:
+            return it
+        sc = torch.zeros(V, dtype=v1.dtype, device=dev).index_add_(0, idx, c)
+        sdx = torch.zeros((V, 3), dtype=v1.dtype, device=dev).index_add_(0, idx, dx[0].reshape(-1, 3))
+        sdv = torch.zeros((V, 3), dtype=v1.dtype, device=dev).index_add_(0, idx, dv[0].reshape(-1, 3))
+        w = torch.where(sc > 0, 1.0 / sc.clamp(min=1), torch.zeros_like(sc))[:, None]
+        v1 += sdx * w
+        vel += sdv * w
+    return max_iter
+
+
+def run_served(args, dev):
+    import torch
+
+    from cccollisions_b200 import workloads as W
+    from cccollisions_b200.serve import Request, Server, requests_from_stream
+    reqs = requests_from_stream(W.served_stream(num_requests=args.served_requests, rate=2000.0))
+    srv = Server(budget_bytes=40 << 30, device=dev)
+    for r in reqs:
+        srv._pin(r)
+    st = srv.run(reqs)
+    srv.close()
+    # the same sample of requests (every k-th by arrival, so all sizes are represented) through
+    # the engine (all admitted at once) and through the plain per-request path
+    k = max(1, len(reqs) // max(1, args.served_plain_sample))
+    sample = reqs[::k][:max(1, args.served_plain_sample)]
+    copies = [Request(r.verts0, r.verts1, r.vel, r.faces, r.masses, rid=r.rid) for r in sample]
+    srv = Server(budget_bytes=40 << 30, device=dev)
+    for r in copies:
+        srv._pin(r)
+    same = srv.run(copies, realtime=False)
+    srv.close()
+    plain_loop(sample[0], dev, 2)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    its = [plain_loop(r, dev) for r in sample]
+    torch.cuda.synchronize(dev)
+    dt = time.perf_counter() - t0
+    ptris = sum(r.F for r in sample)
+    return {"value": st["throughput"], "unit": UNIT, "requests": st["requests"], "rate_per_s": 2000.0,
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "makespan_s": st["makespan_s"],
+            "request_triangles": st["triangles"], "ticks": st["ticks"], "mean_iterations": st["mean_iterations"],
+            "converged_fraction": st["converged"], "budget_gb": 40,
+            "request": "impulse loop (max 50 iterations) on an impulse-workload mesh of log-uniform 2e3..2e5 "
+                       "triangles, fp64",
+            "same_set": {"requests": len(sample), "triangles": ptris,
+                         "engine": {"value": same["throughput"], "seconds": same["makespan_s"],
+                                    "mean_iterations": same["mean_iterations"]},
+                         "plain": {"value": ptris / dt, "seconds": dt, "mean_iterations": float(np.mean(its)),
+                                   "path": "per request, one after another: bvh_motion + compute_impulses per "
+                                           "iteration, per-vertex averaging with torch"}}}
 
 
 def run_reference(args):
-    from cccollisions_b200 import workloads as W
-    x0, x1 = W.cloth_sphere()
-    F = x0.shape[1]
-    per = max(2.0, args.cpu_seconds / max(args.steps, 1))
+    meshes = batched_meshes(args.meshes)
+    per = max(1.0, args.cpu_seconds / max(args.steps + args.warmup, 1))
     vals = []
-    base = None
-    for i in range(max(args.warmup, 0) + args.steps):
-        base = cpu_baseline(x0, x1, per)
+    desc, threads = "", 0
+    for i in range(args.warmup + args.steps):
+        v, threads, desc = cpu_sample(meshes, per)
         if i >= args.warmup:
-            vals.append(base["value"])
+            vals.append(v)
     v = statistics.median(vals)
-    ms = F / v * 1e3
-    base["value"] = v
-    return {"metric": METRIC, "value": v, "unit": "triangle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cloth + icosphere)",
-            "config": {"workload": "cloth_sphere: plain CCD step, bvh_motion + find_collisions_continuous",
-                       "triangles": F},
-            "impl": "reference", "cpu_baseline": base,
-            "e2e": {"value": v, "unit": "triangle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sum(x0.shape[0] for x0, _ in meshes) / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded cloth grids + icospheres)",
+            "config": {"workload": f"batched: {len(meshes)} cloth+icosphere meshes (CPU sample per step)",
+                       "triangles": sum(x0.shape[0] for x0, _ in meshes)},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"per step: {desc}"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def main():
@@ -328,11 +467,19 @@ def main():
     torch.cuda.set_device(dev)
     if world > 1:
         import datetime
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                             device_id=dev)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
     try:
-        res = run_ours(args, rank, world, dev)
+        res, meshes = run_ours(args, rank, world, dev)
+        if world > 1:
+            torch.distributed.barrier()
         if rank == 0:
+            if world == 1 and args.served_requests > 0:
+                res["served"] = run_served(args, dev)
+                ss = res["served"]["same_set"]
+                res["served_over_plain"] = ss["engine"]["value"] / ss["plain"]["value"]
+            if world == 1:
+                v, threads, desc = cpu_sample(meshes, args.cpu_seconds)
+                res["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
             print(json.dumps(res))
     finally:
         if world > 1:

@@ -40,6 +40,7 @@ SIGNATURES = {
     "ccc_timing_end": (_I, [_I, _P, _I, _P, _P]),
     "ccc_workspace_size": (_I64, [_I, _I64, _I64, _I64]),
     "ccc_read_status": (_I, [_P, _I64, _P, _P]),
+    "ccc_read_counters": (_I, [_P, _P, _P]),
     "ccc_bvh": (_I, [_I, _P, _P, _I64, _I64, _P, _P, _P, _I64, _P]),
     "ccc_find_collisions": (_I, [_I, _P, _P, _P, _I64, _I64, _D, _I64, _P, _P, _I64, _P]),
     "ccc_find_collisions_continuous": (_I, [_I, _P, _P, _P, _P, _P, _I64, _I64, _I64, _I64, _P, _P, _P, _I64, _P]),
@@ -67,6 +68,7 @@ SIGNATURES = {
     "ccc_engine_replay": (_I, [_P, _I, _P]),
     "ccc_engine_autotune": (_I, [_P, _P, _P]),
     "ccc_engine_read_state": (_I, [_P, _P, _I64, _P, _P, _P, _P, _P, _P]),
+    "ccc_engine_counters": (_I, [_P, _P, _P]),
 }
 
 # engine constants (mirrors include/ccc_engine.h)

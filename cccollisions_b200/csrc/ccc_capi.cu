@@ -227,9 +227,11 @@ int ccd_impl(const void* bboxes, const int64_t* tree, const void* x0, const void
     if (rc) return rc;
     rc = run_broad_phase<T>(bboxes, tree, mask, B, F, (T)0, is_f32<T>(), P, s);
     if (rc) return rc;
-    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
-        P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, (long long*)rows, (T*)times,
-        (int)maxcol, P.mesh_cnt, CornerSink<T>{})));
+    cudaError_t le = cudaSuccess;
+    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV>(
+        num_sms() * CCD_MIN_BLOCKS, s, P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, (long long*)rows,
+        (T*)times, (int)maxcol, P.mesh_cnt, CornerSink<T>{})));
+    if (le != cudaSuccess) return CCC_ERR_CUDA;
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -242,9 +244,11 @@ int mincol_impl(const void* bboxes, const int64_t* tree, const void* x0, const v
     if (rc) return rc;
     rc = run_broad_phase<T>(bboxes, tree, nullptr, B, F, (T)0, is_f32<T>(), P, s);
     if (rc) return rc;
-    CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_MINCOL, CornerSink<T>, LIB_PORTABLE><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
-        P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, (long long*)rows, nullptr,
-        (int)(maxc * 15), P.mesh_cnt, CornerSink<T>{}));
+    cudaError_t le = cudaSuccess;
+    CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_MINCOL, CornerSink<T>, LIB_PORTABLE>(
+        num_sms() * CCD_MIN_BLOCKS, s, P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, (long long*)rows,
+        nullptr, (int)(maxc * 15), P.mesh_cnt, CornerSink<T>{}));
+    if (le != cudaSuccess) return CCC_ERR_CUDA;
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -273,9 +277,11 @@ int impulses_impl(const void* bboxes, const int64_t* tree, const void* x0, const
     if (rc) return rc;
     rc = run_broad_phase<T>(bboxes, tree, mask, B, F, (T)0, is_f32<T>(), P, s);
     if (rc) return rc;
-    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_IMPULSES, CornerSink<T>, LIBV><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
-        P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, nullptr, nullptr, 0, P.mesh_cnt,
-        CornerSink<T>{(const T*)masses, (T*)dv, (T*)dx, (int*)cnt})));
+    cudaError_t le = cudaSuccess;
+    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_IMPULSES, CornerSink<T>, LIBV>(
+        num_sms() * CCD_MIN_BLOCKS, s, P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, nullptr, nullptr, 0,
+        P.mesh_cnt, CornerSink<T>{(const T*)masses, (T*)dv, (T*)dx, (int*)cnt})));
+    if (le != cudaSuccess) return CCC_ERR_CUDA;
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -394,6 +400,15 @@ int ccc_read_status(const void* ws, int64_t n_mesh, int32_t* out, void* stream) 
             return CCC_ERR_CUDA;
     }
     if (cudaStreamSynchronize(s) != cudaSuccess) return CCC_ERR_CUDA;
+    return CCC_OK;
+}
+
+int ccc_read_counters(const void* ws, int32_t* out, void* stream) {
+    if (!ws || !out) return CCC_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaMemcpyAsync(out, ws, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return CCC_ERR_CUDA;
     return CCC_OK;
 }
 

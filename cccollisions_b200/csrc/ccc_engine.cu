@@ -151,8 +151,8 @@ struct Ranges {
     }
 };
 
-// launch shapes: traversal blocks per SM, narrow-phase blocks per SM in units of one
-// resident wave (NARROW_MIN_BLOCKS)
+// launch shapes: traversal blocks per SM, narrow-phase blocks per SM (one is resident at
+// a time; more blocks split the work finer)
 struct Shape {
     int trav, narrow;
 };
@@ -269,10 +269,12 @@ template <class T> int ccd_step(ccc_engine* e, cudaStream_t s) {
     if (rc) return rc;
     rc = traverse<T>(e, t, nullptr, s);
     if (rc) return rc;
-    int g = num_sms() * NARROW_MIN_BLOCKS * SHAPES[e->shape].narrow;
-    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV><<<g, NARROW_THREADS, 0, s>>>(
-        e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f,
+    int g = num_sms() * CCD_MIN_BLOCKS * SHAPES[e->shape].narrow;
+    cudaError_t le = cudaSuccess;
+    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV>(
+        g, s, e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f,
         e->at<long long>(e->L.rows), e->at<T>(e->L.times), (int)e->maxcol, e->at<int>(e->L.mesh_cnt), CornerSink<T>{})));
+    if (le != cudaSuccess) return CCC_ERR_CUDA;
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -286,11 +288,13 @@ template <class T> int loop_step(ccc_engine* e, int max_iter, cudaStream_t s) {
     if (rc) return rc;
     rc = traverse<T>(e, t, flags, s);
     if (rc) return rc;
-    int g = num_sms() * NARROW_MIN_BLOCKS * SHAPES[e->shape].narrow;
+    int g = num_sms() * CCD_MIN_BLOCKS * SHAPES[e->shape].narrow;
     LoopSink<T> sink{e->at<T>(e->L.masses), e->at<int>(e->L.faces), t.vt, e->at<long long>(e->L.acc), contacts};
-    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, k_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIBV><<<g, NARROW_THREADS, 0, s>>>(
-        e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f, nullptr,
+    cudaError_t le = cudaSuccess;
+    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIBV>(
+        g, s, e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f, nullptr,
         nullptr, 0, e->at<int>(e->L.mesh_cnt), sink)));
+    if (le != cudaSuccess) return CCC_ERR_CUDA;
     CCC_LAUNCH_CHECK();
     CCC_LAUNCH("k_loop_update", s, k_loop_update<<<grid_for(e->mesh_cap, ITEM_THREADS), ITEM_THREADS, 0, s>>>(
         t.f, contacts, e->at<int>(e->L.iters), flags, max_iter));
@@ -374,6 +378,15 @@ bool active_built(const ccc_engine* e) {
     return true;
 }
 
+// shared-memory attributes of the narrow-phase kernels an engine launches, set before any
+// stream capture
+template <class T> bool prepare_kernels() {
+    return prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_REFERENCE>() == cudaSuccess &&
+           prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_PORTABLE>() == cudaSuccess &&
+           prepare_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIB_REFERENCE>() == cudaSuccess &&
+           prepare_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIB_PORTABLE>() == cudaSuccess;
+}
+
 int run_op(ccc_engine* e, int op, int max_iter, cudaStream_t s) {
     if (!active_built(e)) return CCC_ERR_INVALID_ARG;
     if (op == CCC_ENGINE_OP_CCD) return e->dtype ? ccd_step<double>(e, s) : ccd_step<float>(e, s);
@@ -428,6 +441,7 @@ int ccc_engine_create(int dtype, int64_t tc, int64_t vc, int64_t mc, int64_t max
               cudaHostAlloc((void**)&e->h_state, e->L.state_end, cudaHostAllocDefault) == cudaSuccess &&
               cudaEventCreateWithFlags(&e->stage_ev[0], cudaEventDisableTiming) == cudaSuccess &&
               cudaEventCreateWithFlags(&e->stage_ev[1], cudaEventDisableTiming) == cudaSuccess;
+    if (ok) ok = dtype ? prepare_kernels<double>() : prepare_kernels<float>();
     if (ok) {
         memset(e->h_stage, 0, 2 * words * 4);
         // state, tables (empty), refit counters, topology and accumulators start cleared
@@ -666,6 +680,11 @@ int ccc_engine_autotune(ccc_engine* e, void* stream, int32_t* choice) {
     }
     if (choice) *choice = best;
     return CCC_OK;
+}
+
+int ccc_engine_counters(ccc_engine* e, int32_t* out, void* stream) {
+    if (!e || !out) return CCC_ERR_INVALID_ARG;
+    return ccc_read_counters(e->base + e->L.hdr, out, stream);
 }
 
 int ccc_engine_read_state(ccc_engine* e, const int32_t* ids, int64_t n, int32_t* status, int32_t* rows,

@@ -35,7 +35,9 @@ enum MeshFlags {
 struct WsHeader {
     int status;
     int cand_count;
-    int pad[14];
+    int subtests;      // continuous sub-tests (pair, type) solved
+    int roots;         // roots in [0, 1] filtered
+    int pad[12];
 };
 
 struct __align__(16) TNode {
@@ -50,11 +52,8 @@ struct __align__(16) TNode {
 static constexpr int TRAV_THREADS = 128;
 static constexpr int STACK_DEPTH = 64;        // STACK_SIZE (flags.h:26-29)
 static constexpr int NARROW_THREADS = 128;
-// resident narrow-phase blocks per SM the register allocation is sized for
-#ifndef CCC_NARROW_MIN_BLOCKS
-#define CCC_NARROW_MIN_BLOCKS 5
-#endif
-static constexpr int NARROW_MIN_BLOCKS = CCC_NARROW_MIN_BLOCKS;
+// resident blocks per SM of the static and proximity narrow phases
+static constexpr int NARROW_MIN_BLOCKS = 4;
 
 // mesh containing element g where base(m) = off[m] - m * shift (shift 0: triangles,
 // shift 1: internal nodes); off has M + 1 entries
@@ -496,37 +495,82 @@ template <class T> struct CornerSink {
 };
 
 // Continuous narrow phase (collisions_continuous.cu:14-765, collisions_impulses.cu:24-1067),
-// warp-cooperative.  Each warp takes 32 candidate pairs: every lane runs the shared-vertex
-// test and the 15 swept sub-box tests of its pair, and the surviving (pair, type) items are
-// staged in shared memory.  The warp then works through them in batches of NARROW_BATCH in
-// three uniform phases: (1) cubic coefficients and the solver prefix of every item, which
-// sorts the items by solver branch; (2) the roots of one branch at a time; (3) the root
-// filter and the output of every root in [0, 1].  Items take different branches and have
-// 0 to 3 roots, so solving them in arrival order would leave most lanes idle.
-static constexpr int NARROW_BATCH = 64;
+// block-synchronous.  One block of CCD_BLOCK threads per SM loops over chunks of CCD_BLOCK
+// candidate pairs.  Every thread runs the shared-vertex test and the 15 swept sub-box tests
+// of its pair, and the surviving (pair, type) sub-tests are staged in shared memory.  The
+// block then works through them in batches of CCD_BATCH in three phases, separated by
+// barriers so that every warp of the SM runs the same phase's code at the same time:
+//   (1) cubic coefficients and the solver prefix of every sub-test, which classifies it;
+//   (2) the roots, with the sub-tests ordered by solver branch;
+//   (3) the root filter and the output of every root in [0, 1].
+// Sub-tests take different branches and have 0 to 3 roots: solved in arrival order they
+// leave most lanes idle, and a kernel whose warps are in different phases needs all of its
+// code in the instruction cache at once.
+#ifndef CCC_CCD_BLOCK
+#define CCC_CCD_BLOCK 256
+#endif
+#ifndef CCC_CCD_MIN_BLOCKS
+#define CCC_CCD_MIN_BLOCKS 3
+#endif
+static constexpr int CCD_BLOCK = CCC_CCD_BLOCK;
+static constexpr int CCD_MIN_BLOCKS = CCC_CCD_MIN_BLOCKS;      // resident blocks per SM
+static constexpr int CCD_BATCH = 2 * CCD_BLOCK;
+static constexpr int CCD_ITEMS = 15 * CCD_BLOCK;      // sub-tests of one chunk, worst case
+static_assert(CCD_BLOCK % 32 == 0 && CCD_BLOCK <= 1024 && CCD_BLOCK * 16 <= 65536, "CCD_BLOCK");
+
+constexpr size_t align16(size_t x) { return (x + 15) / 16 * 16; }
+
+// dynamic shared memory of one block (byte offsets)
+template <class T> struct CcdLayout {
+    static constexpr size_t rec = 0;                                                   // double [6][BATCH]
+    static constexpr size_t root_val = rec + 6 * CCD_BATCH * sizeof(double);           // T [3 BATCH]
+    static constexpr size_t pairs = align16(root_val + 3 * CCD_BATCH * sizeof(T));     // int2 [BLOCK]
+    static constexpr size_t items = pairs + CCD_BLOCK * sizeof(int2);                  // u16 [ITEMS]
+    static constexpr size_t rec_item = align16(items + CCD_ITEMS * 2);                 // u16 [BATCH]
+    static constexpr size_t clist = rec_item + CCD_BATCH * 2;                          // u16 [BATCH]
+    static constexpr size_t root_rec = clist + CCD_BATCH * 2;                          // u16 [3 BATCH]
+    static constexpr size_t rec_cls = root_rec + 3 * CCD_BATCH * 2;                    // u8 [BATCH]
+    static constexpr size_t ints = align16(rec_cls + CCD_BATCH);                       // int [64]
+    static constexpr size_t bytes = ints + 64 * sizeof(int);
+};
+
+// slots of the small int area
+enum CcdInts { CI_WARP = 0, CI_TOTAL = 32, CI_COUNT = 33, CI_CURSOR = 37, CI_OFFSET = 41, CI_ROOTS = 46 };
+
+__device__ __forceinline__ int warp_inclusive_scan(int v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += y;
+    }
+    return v;
+}
 
 template <class T, int MODE, class Sink, int LIB>
-__global__ void __launch_bounds__(NARROW_THREADS, NARROW_MIN_BLOCKS)
+__global__ void __launch_bounds__(CCD_BLOCK, CCD_MIN_BLOCKS)
 k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ x0,
              const T* __restrict__ x1, Forest F, long long* __restrict__ rows, T* __restrict__ times, int max_per_tri,
              int* __restrict__ mesh_counters, Sink sink) {
-    constexpr int WARPS = NARROW_THREADS / 32;
-    constexpr int NB = NARROW_BATCH;
-    __shared__ unsigned short items[WARPS][32 * 15];
-    __shared__ int2 pairs[WARPS][32];
-    __shared__ double rec[WARPS][6][NB];                 // a, b, c, d, g, h per item of a batch
-    __shared__ unsigned short rec_item[WARPS][NB];
-    __shared__ unsigned char clist[WARPS][4][NB];        // batch positions per class (QUAD..ONE)
-    __shared__ unsigned char root_rec[WARPS][3 * NB];
-    __shared__ T root_val[WARPS][3 * NB];
+    extern __shared__ __align__(16) unsigned char smem[];
+    using L = CcdLayout<T>;
+    double* rec = reinterpret_cast<double*>(smem + L::rec);
+    T* root_val = reinterpret_cast<T*>(smem + L::root_val);
+    int2* pairs = reinterpret_cast<int2*>(smem + L::pairs);
+    unsigned short* items = reinterpret_cast<unsigned short*>(smem + L::items);
+    unsigned short* rec_item = reinterpret_cast<unsigned short*>(smem + L::rec_item);
+    unsigned short* clist = reinterpret_cast<unsigned short*>(smem + L::clist);
+    unsigned short* root_rec = reinterpret_cast<unsigned short*>(smem + L::root_rec);
+    unsigned char* rec_cls = smem + L::rec_cls;
+    int* ints = reinterpret_cast<int*>(smem + L::ints);
+    constexpr int NW = CCD_BLOCK / 32;
+    constexpr int NB = CCD_BATCH;
     const int M = forest_size(F);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned FULL = 0xffffffffu;
     const unsigned lt = (1u << lane) - 1u;
     const int n = min(*(volatile int*)&hdr->cand_count, cand_cap);
-    for (long long base = ((long long)blockIdx.x * WARPS + warp) * 32; base < n;
-         base += (long long)gridDim.x * WARPS * 32) {
-        long long c = base + lane;
+    for (long long base = (long long)blockIdx.x * CCD_BLOCK; base < n; base += (long long)gridDim.x * CCD_BLOCK) {
+        long long c = base + tid;
         uint32_t bits = 0;
         int2 pr = make_int2(0, 0);
         if (c < n) {
@@ -549,91 +593,107 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
             }
             continue;
         }
-        // stage the work items of the 32 pairs
-        int cnt = __popc(bits);
-        int incl = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int v = __shfl_up_sync(FULL, incl, o);
-            if (lane >= o) incl += v;
+        // stage the sub-tests of the chunk (block-wide exclusive scan of the counts)
+        const int cnt = __popc(bits);
+        const int incl = warp_inclusive_scan(cnt, lane);
+        if (lane == 31) ints[CI_WARP + warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            int v = lane < NW ? ints[CI_WARP + lane] : 0;
+            int sc = warp_inclusive_scan(v, lane);
+            if (lane < NW) ints[CI_WARP + lane] = sc - v;
+            if (lane == 31) ints[CI_TOTAL] = sc;
         }
-        const int total = __shfl_sync(FULL, incl, 31);
-        int pos = incl - cnt;
+        __syncthreads();
+        int pos = ints[CI_WARP + warp] + incl - cnt;
+        const int total = ints[CI_TOTAL];
         while (bits) {
             int k = __ffs(bits) - 1;
             bits &= bits - 1;
-            items[warp][pos++] = (unsigned short)((lane << 4) | k);
+            items[pos++] = (unsigned short)((tid << 4) | k);
         }
-        pairs[warp][lane] = pr;
-        __syncwarp();
+        pairs[tid] = pr;
+        if (tid == 0 && total) atomicAdd(&hdr->subtests, total);
+        __syncthreads();
         for (int b0 = 0; b0 < total; b0 += NB) {
             const int nb = min(NB, total - b0);
-            // (1) coefficients and solver prefix; class lists
-            int ccount[4] = {0, 0, 0, 0};
-#pragma unroll 1
-            for (int r0 = 0; r0 < NB; r0 += 32) {
-                const int ri = r0 + lane;
-                int cls = CUBIC_NONE;
-                if (ri < nb) {
-                    int item = items[warp][b0 + ri];
-                    int k = item & 15;
-                    int2 q = pairs[warp][item >> 4];
-                    MTet<T> tet = load_tet(x0, x1, q.x, q.y, k);
-                    T cf[4];
-                    cubic_coeffs(tet, cf);
-                    double g, h;
-                    cls = cubic_prefix<LIB>((double)cf[0], (double)cf[1], (double)cf[2], (double)cf[3], g, h);
-                    rec[warp][0][ri] = (double)cf[0];
-                    rec[warp][1][ri] = (double)cf[1];
-                    rec[warp][2][ri] = (double)cf[2];
-                    rec[warp][3][ri] = (double)cf[3];
-                    rec[warp][4][ri] = g;
-                    rec[warp][5][ri] = h;
-                    rec_item[warp][ri] = (unsigned short)item;
-                }
-#pragma unroll
-                for (int cc = 0; cc < 4; ++cc) {
-                    unsigned m = __ballot_sync(FULL, cls == cc + 1);
-                    if (cls == cc + 1) clist[warp][cc][ccount[cc] + __popc(m & lt)] = (unsigned char)ri;
-                    ccount[cc] += __popc(m);
-                }
-            }
-            __syncwarp();
-            // (2) roots, one class at a time; roots in [0, 1] go to the root list
-            int nroots = 0;
-#pragma unroll 1
-            for (int cc = 0; cc < 4; ++cc) {
-#pragma unroll 1
-                for (int j0 = 0; j0 < ccount[cc]; j0 += 32) {
-                    const int j = j0 + lane;
-                    T rr[3] = {(T)-1, (T)-1, (T)-1};
-                    int ri = 0;
-                    if (j < ccount[cc]) {
-                        ri = clist[warp][cc][j];
-                        class_roots<T, LIB>(cc + 1, rec[warp][0][ri], rec[warp][1][ri], rec[warp][2][ri],
-                                            rec[warp][3][ri], rec[warp][4][ri], rec[warp][5][ri], rr);
-                    }
-#pragma unroll
-                    for (int s = 0; s < 3; ++s) {
-                        bool keep = j < ccount[cc] && (rr[s] >= 0 && rr[s] <= 1);
-                        unsigned m = __ballot_sync(FULL, keep);
-                        if (keep) {
-                            int at = nroots + __popc(m & lt);
-                            root_rec[warp][at] = (unsigned char)ri;
-                            root_val[warp][at] = rr[s];
-                        }
-                        nroots += __popc(m);
-                    }
-                }
-            }
-            __syncwarp();
-            // (3) filter and output
-#pragma unroll 1
-            for (int j = lane; j < nroots; j += 32) {
-                int item = rec_item[warp][root_rec[warp][j]];
+            if (tid < 8) ints[CI_COUNT + tid] = 0;           // class counts and cursors
+            if (tid == 8) ints[CI_ROOTS] = 0;
+            __syncthreads();
+            // (1) coefficients and solver prefix
+            for (int ri = tid; ri < nb; ri += CCD_BLOCK) {
+                int item = items[b0 + ri];
                 int k = item & 15;
-                int2 q = pairs[warp][item >> 4];
-                T root = root_val[warp][j];
+                int2 q = pairs[item >> 4];
+                MTet<T> tet = load_tet(x0, x1, q.x, q.y, k);
+                T cf[4];
+                cubic_coeffs(tet, cf);
+                double g, h;
+                int cls = cubic_prefix<LIB>((double)cf[0], (double)cf[1], (double)cf[2], (double)cf[3], g, h);
+                rec[0 * NB + ri] = (double)cf[0];
+                rec[1 * NB + ri] = (double)cf[1];
+                rec[2 * NB + ri] = (double)cf[2];
+                rec[3 * NB + ri] = (double)cf[3];
+                rec[4 * NB + ri] = g;
+                rec[5 * NB + ri] = h;
+                rec_item[ri] = (unsigned short)item;
+                rec_cls[ri] = (unsigned char)cls;
+                if (cls != CUBIC_NONE) atomicAdd(&ints[CI_COUNT + cls - 1], 1);
+            }
+            __syncthreads();
+            if (tid == 0) {
+                int o = 0;
+                for (int cc = 0; cc < 4; ++cc) {
+                    ints[CI_OFFSET + cc] = o;
+                    o += ints[CI_COUNT + cc];
+                }
+                ints[CI_OFFSET + 4] = o;
+            }
+            __syncthreads();
+            // sub-tests ordered by class
+            for (int ri = tid; ri < nb; ri += CCD_BLOCK) {
+                int cls = rec_cls[ri];
+                if (cls != CUBIC_NONE) {
+                    int p = atomicAdd(&ints[CI_CURSOR + cls - 1], 1);
+                    clist[ints[CI_OFFSET + cls - 1] + p] = (unsigned short)ri;
+                }
+            }
+            __syncthreads();
+            // (2) roots; the ones in [0, 1] go to the root list
+            const int nsolve = ints[CI_OFFSET + 4];
+            const int o1 = ints[CI_OFFSET + 1], o2 = ints[CI_OFFSET + 2], o3 = ints[CI_OFFSET + 3];
+            for (int j0 = 0; j0 < nsolve; j0 += CCD_BLOCK) {
+                const int j = j0 + tid;
+                T rr[3] = {(T)-1, (T)-1, (T)-1};
+                int ri = 0;
+                if (j < nsolve) {
+                    int cc = (j >= o1) + (j >= o2) + (j >= o3);
+                    ri = clist[j];
+                    class_roots<T, LIB>(cc + 1, rec[0 * NB + ri], rec[1 * NB + ri], rec[2 * NB + ri], rec[3 * NB + ri],
+                                        rec[4 * NB + ri], rec[5 * NB + ri], rr);
+                }
+#pragma unroll
+                for (int s = 0; s < 3; ++s) {
+                    bool keep = j < nsolve && (rr[s] >= 0 && rr[s] <= 1);
+                    unsigned m = __ballot_sync(FULL, keep);
+                    int at = 0;
+                    if (lane == 0 && m) at = atomicAdd(&ints[CI_ROOTS], __popc(m));
+                    at = __shfl_sync(FULL, at, 0) + __popc(m & lt);
+                    if (keep) {
+                        root_rec[at] = (unsigned short)ri;
+                        root_val[at] = rr[s];
+                    }
+                }
+            }
+            __syncthreads();
+            const int nroots = ints[CI_ROOTS];
+            if (tid == 0 && nroots) atomicAdd(&hdr->roots, nroots);
+            // (3) filter and output
+            for (int j = tid; j < nroots; j += CCD_BLOCK) {
+                int item = rec_item[root_rec[j]];
+                int k = item & 15;
+                int2 q = pairs[item >> 4];
+                T root = root_val[j];
                 MTet<T> tet = load_tet(x0, x1, q.x, q.y, k);
                 if (!ccd_filter(tet, k, root)) continue;
                 if (MODE == CCD_ROWS) {
@@ -655,10 +715,33 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                     sink.add(tet, q.x, q.y, k, root, ct, F, M, &hdr->status);
                 }
             }
-            __syncwarp();
+            __syncthreads();
         }
-        __syncwarp();
     }
+}
+
+// Launch of k_ccd_narrow with its dynamic shared memory (the size is raised once per
+// instantiation and device; prepare_ccd_narrow does it ahead of any stream capture).
+template <class T, int MODE, class Sink, int LIB> inline cudaError_t prepare_ccd_narrow() {
+    static bool done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(k_ccd_narrow<T, MODE, Sink, LIB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)CcdLayout<T>::bytes);
+    if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
+    return e;
+}
+
+template <class T, int MODE, class Sink, int LIB>
+inline cudaError_t launch_ccd_narrow(int grid, cudaStream_t s, const int2* cand, int cand_cap, WsHeader* hdr,
+                                     const T* x0, const T* x1, Forest F, long long* rows, T* times, int max_per_tri,
+                                     int* mesh_counters, Sink sink) {
+    cudaError_t e = prepare_ccd_narrow<T, MODE, Sink, LIB>();
+    if (e != cudaSuccess) return e;
+    k_ccd_narrow<T, MODE, Sink, LIB><<<grid, CCD_BLOCK, CcdLayout<T>::bytes, s>>>(
+        cand, cand_cap, hdr, x0, x1, F, rows, times, max_per_tri, mesh_counters, sink);
+    return cudaSuccess;
 }
 
 // proximity (proximity_static.cu:11-508)

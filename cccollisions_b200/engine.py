@@ -194,6 +194,12 @@ class Engine:
                                               _stream(self.device)), "ccc_engine_read_state")
         return {"status": int(st.value), "rows": rows, "contacts": con, "iterations": it, "flags": fl}
 
+    def counters(self) -> dict:
+        """Synchronises; work counters of the last step."""
+        out = (ctypes.c_int32 * 4)()
+        N.check(N.lib().ccc_engine_counters(self.handle, out, _stream(self.device)), "ccc_engine_counters")
+        return {"status": int(out[0]), "candidates": int(out[1]), "subtests": int(out[2]), "roots": int(out[3])}
+
     def collisions(self, sid: int, count: int | None = None):
         """(rows (n, 3) int64, times (n,)) of the last ccd() for one mesh (views)."""
         if count is None:

@@ -95,6 +95,11 @@ int64_t ccc_workspace_size(int op, int64_t B, int64_t F, int64_t max_candidates_
  * the workspace to host memory (synchronises the stream).  out must hold 2 + n_mesh ints. */
 int ccc_read_status(const void* ws, int64_t n_mesh, int32_t* out, void* stream);
 
+/* Work counters of the last operation on a workspace (no counterpart in the reference):
+ * synchronises the stream and writes 4 ints: status word, candidate pairs, continuous
+ * sub-tests solved, roots in [0, 1] filtered. */
+int ccc_read_counters(const void* ws, int32_t* out, void* stream);
+
 /* bvh / bvh_motion — replaces build_bvh(triangles[, triangles_next], &bboxes, &tree)
  * (src/build_bvh.cu:381-449, 570-648; bindings src/cccollisions.cpp:102-132).
  * triangles_next may be NULL (static build).  Writes every row of bboxes and tree in the

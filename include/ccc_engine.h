@@ -115,6 +115,10 @@ int ccc_engine_autotune(ccc_engine* e, void* stream, int32_t* choice);
 int ccc_engine_read_state(ccc_engine* e, const int32_t* slot_ids, int64_t n, int32_t* status, int32_t* rows,
                           int32_t* contacts, int32_t* iterations, int32_t* flags, void* stream);
 
+/* Synchronise the stream and read the work counters of the last step: status word,
+ * candidate pairs, continuous sub-tests solved, roots in [0, 1] filtered. */
+int ccc_engine_counters(ccc_engine* e, int32_t* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
