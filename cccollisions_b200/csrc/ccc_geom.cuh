@@ -243,6 +243,63 @@ template <class T> __device__ __forceinline__ uint32_t ccd_subbox_mask(const MTr
     return m;
 }
 
+// The shared-vertex test and the 15 swept sub-box tests of a candidate pair (i, j), read
+// straight from the soups one axis at a time: both are conjunctions over the axes (equal
+// coordinates; intervals that overlap), so the per-axis results are ANDed.  Same boxes and
+// comparisons as share_vertex + ccd_subbox_mask (v and v + dv with dv = x1 - x0, min / max
+// merges, inclusive bounds), with a third of the live values.  Returns 0 when the
+// triangles share a vertex, else the mask of sub-tests whose swept boxes overlap.
+template <class T>
+__device__ __forceinline__ uint32_t ccd_pair_mask(const T* __restrict__ x0, const T* __restrict__ x1, long long i,
+                                                  long long j) {
+    const T* a0 = x0 + i * 9;
+    const T* a1 = x1 + i * 9;
+    const T* b0 = x0 + j * 9;
+    const T* b1 = x1 + j * 9;
+    uint32_t m = 0x7fffu;
+    uint32_t eq = 0x1ffu;       // vertex pairs (ia, jb) equal on every axis so far: bit 3 ia + jb
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        T av[3], alo[3], ahi[3], bv[3], blo[3], bhi[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            av[c] = __ldg(a0 + 3 * c + ax);
+            T ae = av[c] + (__ldg(a1 + 3 * c + ax) - av[c]);
+            alo[c] = fmn(av[c], ae);
+            ahi[c] = fmx(av[c], ae);
+            bv[c] = __ldg(b0 + 3 * c + ax);
+            T be = bv[c] + (__ldg(b1 + 3 * c + ax) - bv[c]);
+            blo[c] = fmn(bv[c], be);
+            bhi[c] = fmx(bv[c], be);
+        }
+#pragma unroll
+        for (int ia = 0; ia < 3; ++ia)
+#pragma unroll
+            for (int jb = 0; jb < 3; ++jb)
+                if (!(av[ia] == bv[jb])) eq &= ~(1u << (3 * ia + jb));
+        // edges 01, 02, 12 and the face
+        const T ealo[3] = {fmn(alo[0], alo[1]), fmn(alo[0], alo[2]), fmn(alo[1], alo[2])};
+        const T eahi[3] = {fmx(ahi[0], ahi[1]), fmx(ahi[0], ahi[2]), fmx(ahi[1], ahi[2])};
+        const T eblo[3] = {fmn(blo[0], blo[1]), fmn(blo[0], blo[2]), fmn(blo[1], blo[2])};
+        const T ebhi[3] = {fmx(bhi[0], bhi[1]), fmx(bhi[0], bhi[2]), fmx(bhi[1], bhi[2])};
+        const T falo = fmn(fmn(alo[0], alo[1]), alo[2]), fahi = fmx(fmx(ahi[0], ahi[1]), ahi[2]);
+        const T fblo = fmn(fmn(blo[0], blo[1]), blo[2]), fbhi = fmx(fmx(bhi[0], bhi[1]), bhi[2]);
+        uint32_t ma = 0;
+#pragma unroll
+        for (int e0 = 0; e0 < 3; ++e0)
+#pragma unroll
+            for (int e1 = 0; e1 < 3; ++e1)
+                if (ealo[e0] <= ebhi[e1] && eahi[e0] >= eblo[e1]) ma |= 1u << (3 * e0 + e1);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if (falo <= bhi[c] && fahi >= blo[c]) ma |= 1u << (9 + c);
+            if (alo[c] <= fbhi && ahi[c] >= fblo) ma |= 1u << (12 + c);
+        }
+        m &= ma;
+    }
+    return eq ? 0u : m;
+}
+
 // The same table packed into constants, so a runtime type k selects points without
 // indexing local arrays: side(k, p) = bit 4k + p of CCD_SIDE_TABLE, corner(k, p) = the
 // 2-bit field 8 (k % 8) + 2p of CCD_CORNER_TABLE[k / 8].

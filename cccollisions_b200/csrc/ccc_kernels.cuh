@@ -514,7 +514,10 @@ template <class T> struct CornerSink {
 #endif
 static constexpr int CCD_BLOCK = CCC_CCD_BLOCK;
 static constexpr int CCD_MIN_BLOCKS = CCC_CCD_MIN_BLOCKS;      // resident blocks per SM
-static constexpr int CCD_BATCH = 2 * CCD_BLOCK;
+#ifndef CCC_CCD_BATCH_MULT
+#define CCC_CCD_BATCH_MULT 2
+#endif
+static constexpr int CCD_BATCH = CCC_CCD_BATCH_MULT * CCD_BLOCK;
 static constexpr int CCD_ITEMS = 15 * CCD_BLOCK;      // sub-tests of one chunk, worst case
 static_assert(CCD_BLOCK % 32 == 0 && CCD_BLOCK <= 1024 && CCD_BLOCK * 16 <= 65536, "CCD_BLOCK");
 
@@ -575,8 +578,7 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
         int2 pr = make_int2(0, 0);
         if (c < n) {
             pr = cand[c];
-            MTri<T> a = load_mtri(x0, x1, pr.x), b = load_mtri(x0, x1, pr.y);
-            if (!share_vertex(a.v, b.v)) bits = ccd_subbox_mask(a, b);
+            bits = ccd_pair_mask(x0, x1, pr.x, pr.y);
         }
         if (MODE == CCD_MINCOL) {
             while (bits) {
