@@ -256,7 +256,7 @@ template <class T> int traverse(ccc_engine* e, const Tables& t, const int* flags
         CCC_LAUNCH("k_traverse", s, k_traverse<T, false, true><<<g, TRAV_THREADS, 0, s>>>(
             e->at<TNode>(e->L.nodes), lv, t.f, nullptr, (T)0, e->at<int2>(e->L.cand), cap, e->hdr(), flags));
     else
-        CCC_LAUNCH("k_traverse", s, k_traverse<T, false, false><<<g, TRAV_THREADS, 0, s>>>(
+        CCC_LAUNCH("k_traverse", s, k_traverse<T, false, false, SceneLeaves<T>, false><<<g, TRAV_THREADS, 0, s>>>(
             e->at<TNode>(e->L.nodes), lv, t.f, nullptr, (T)0, e->at<int2>(e->L.cand), cap, e->hdr(), flags));
     CCC_LAUNCH_CHECK();
     return CCC_OK;

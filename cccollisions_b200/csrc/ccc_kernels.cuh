@@ -329,7 +329,10 @@ template <class T> struct SceneLeaves {
     }
 };
 
-template <class T, bool MASKED, bool EXACT_F32, class Leaves>
+// RECHECK = false leaves out the exact leaf box test: the candidate set is then the fp32
+// superset, for callers whose narrow phase re-tests every pair exactly (the continuous
+// sub-box tests reject any pair whose swept boxes do not overlap).
+template <class T, bool MASKED, bool EXACT_F32, class Leaves, bool RECHECK = true>
 __global__ void __launch_bounds__(TRAV_THREADS)
 k_traverse(const TNode* __restrict__ nodes, Leaves leaves, Forest F, const uint8_t* __restrict__ mask, T th,
            int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const int* __restrict__ mflags) {
@@ -398,7 +401,7 @@ k_traverse(const TNode* __restrict__ nodes, Leaves leaves, Forest F, const uint8
                     int cpos = ~ref;
                     int cid = s ? D.w : D.z;
                     if (MASKED && mask[po + cid] && !(qid < cid)) hit = false;
-                    if (hit && !EXACT_F32) hit = overlap(q, leaves.box(m, vo, po, n, cpos), th);
+                    if (RECHECK && hit && !EXACT_F32) hit = overlap(q, leaves.box(m, vo, po, n, cpos), th);
                     if (hit) {
                         cg::coalesced_group grp = cg::coalesced_threads();
                         int slot = 0;
@@ -495,31 +498,33 @@ template <class T> struct CornerSink {
 };
 
 // Continuous narrow phase (collisions_continuous.cu:14-765, collisions_impulses.cu:24-1067),
-// block-synchronous.  One block of CCD_BLOCK threads per SM loops over chunks of CCD_BLOCK
-// candidate pairs.  Every thread runs the shared-vertex test and the 15 swept sub-box tests
-// of its pair, and the surviving (pair, type) sub-tests are staged in shared memory.  The
-// block then works through them in batches of CCD_BATCH in three phases, separated by
-// barriers so that every warp of the SM runs the same phase's code at the same time:
+// block-synchronous.  Blocks of CCD_BLOCK threads loop over chunks of CCD_BLOCK candidate
+// pairs.  Every thread runs the shared-vertex test and the 15 swept sub-box tests of its
+// pair, and the surviving (pair, type) sub-tests are appended to a ring queue in shared
+// memory.  Whenever a full batch of CCD_BATCH sub-tests is queued (and once more at the end
+// for the remainder), the block solves it in three phases separated by barriers, so that
+// every warp of the block runs the same phase's code at the same time:
 //   (1) cubic coefficients and the solver prefix of every sub-test, which classifies it;
 //   (2) the roots, with the sub-tests ordered by solver branch;
 //   (3) the root filter and the output of every root in [0, 1].
 // Sub-tests take different branches and have 0 to 3 roots: solved in arrival order they
 // leave most lanes idle, and a kernel whose warps are in different phases needs all of its
-// code in the instruction cache at once.
+// code in the instruction cache at once.  Queued batches are always full, so no phase runs
+// with a partly empty round of threads.
 #ifndef CCC_CCD_BLOCK
 #define CCC_CCD_BLOCK 256
 #endif
 #ifndef CCC_CCD_MIN_BLOCKS
 #define CCC_CCD_MIN_BLOCKS 3
 #endif
+#ifndef CCC_CCD_BATCH_MULT
+#define CCC_CCD_BATCH_MULT 1
+#endif
 static constexpr int CCD_BLOCK = CCC_CCD_BLOCK;
 static constexpr int CCD_MIN_BLOCKS = CCC_CCD_MIN_BLOCKS;      // resident blocks per SM
-#ifndef CCC_CCD_BATCH_MULT
-#define CCC_CCD_BATCH_MULT 2
-#endif
 static constexpr int CCD_BATCH = CCC_CCD_BATCH_MULT * CCD_BLOCK;
-static constexpr int CCD_ITEMS = 15 * CCD_BLOCK;      // sub-tests of one chunk, worst case
-static_assert(CCD_BLOCK % 32 == 0 && CCD_BLOCK <= 1024 && CCD_BLOCK * 16 <= 65536, "CCD_BLOCK");
+static constexpr int CCD_QUEUE = CCD_BATCH + 15 * CCD_BLOCK;  // a partial batch plus a chunk's worst case
+static_assert(CCD_BLOCK % 32 == 0 && CCD_BLOCK <= 1024 && 3 * CCD_BATCH <= 65536, "CCD_BLOCK");
 
 constexpr size_t align16(size_t x) { return (x + 15) / 16 * 16; }
 
@@ -527,10 +532,8 @@ constexpr size_t align16(size_t x) { return (x + 15) / 16 * 16; }
 template <class T> struct CcdLayout {
     static constexpr size_t rec = 0;                                                   // double [6][BATCH]
     static constexpr size_t root_val = rec + 6 * CCD_BATCH * sizeof(double);           // T [3 BATCH]
-    static constexpr size_t pairs = align16(root_val + 3 * CCD_BATCH * sizeof(T));     // int2 [BLOCK]
-    static constexpr size_t items = pairs + CCD_BLOCK * sizeof(int2);                  // u16 [ITEMS]
-    static constexpr size_t rec_item = align16(items + CCD_ITEMS * 2);                 // u16 [BATCH]
-    static constexpr size_t clist = rec_item + CCD_BATCH * 2;                          // u16 [BATCH]
+    static constexpr size_t items = align16(root_val + 3 * CCD_BATCH * sizeof(T));     // int2 [QUEUE]
+    static constexpr size_t clist = items + CCD_QUEUE * sizeof(int2);                  // u16 [BATCH]
     static constexpr size_t root_rec = clist + CCD_BATCH * 2;                          // u16 [3 BATCH]
     static constexpr size_t rec_cls = root_rec + 3 * CCD_BATCH * 2;                    // u8 [BATCH]
     static constexpr size_t ints = align16(rec_cls + CCD_BATCH);                       // int [64]
@@ -539,6 +542,9 @@ template <class T> struct CcdLayout {
 
 // slots of the small int area
 enum CcdInts { CI_WARP = 0, CI_TOTAL = 32, CI_COUNT = 33, CI_CURSOR = 37, CI_OFFSET = 41, CI_ROOTS = 46 };
+
+// a queued sub-test: triangle slots i and j, type k in the top bits of j (slots < 2^28)
+__device__ __forceinline__ int2 pack_subtest(int i, int j, int k) { return make_int2(i, j | (k << 28)); }
 
 __device__ __forceinline__ int warp_inclusive_scan(int v, int lane) {
 #pragma unroll
@@ -558,76 +564,81 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
     using L = CcdLayout<T>;
     double* rec = reinterpret_cast<double*>(smem + L::rec);
     T* root_val = reinterpret_cast<T*>(smem + L::root_val);
-    int2* pairs = reinterpret_cast<int2*>(smem + L::pairs);
-    unsigned short* items = reinterpret_cast<unsigned short*>(smem + L::items);
-    unsigned short* rec_item = reinterpret_cast<unsigned short*>(smem + L::rec_item);
+    int2* items = reinterpret_cast<int2*>(smem + L::items);
     unsigned short* clist = reinterpret_cast<unsigned short*>(smem + L::clist);
     unsigned short* root_rec = reinterpret_cast<unsigned short*>(smem + L::root_rec);
     unsigned char* rec_cls = smem + L::rec_cls;
     int* ints = reinterpret_cast<int*>(smem + L::ints);
     constexpr int NW = CCD_BLOCK / 32;
     constexpr int NB = CCD_BATCH;
+    constexpr int Q = CCD_QUEUE;
     const int M = forest_size(F);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned FULL = 0xffffffffu;
     const unsigned lt = (1u << lane) - 1u;
     const int n = min(*(volatile int*)&hdr->cand_count, cand_cap);
-    for (long long base = (long long)blockIdx.x * CCD_BLOCK; base < n; base += (long long)gridDim.x * CCD_BLOCK) {
-        long long c = base + tid;
-        uint32_t bits = 0;
-        int2 pr = make_int2(0, 0);
-        if (c < n) {
-            pr = cand[c];
-            bits = ccd_pair_mask(x0, x1, pr.x, pr.y);
-        }
-        if (MODE == CCD_MINCOL) {
+    int head = 0, queued = 0;           // ring queue of sub-tests (block-uniform)
+    for (long long base = (long long)blockIdx.x * CCD_BLOCK;; base += (long long)gridDim.x * CCD_BLOCK) {
+        const bool more = base < n;
+        if (!more && queued == 0) break;
+        if (more) {
+            long long c = base + tid;
+            uint32_t bits = 0;
+            int2 pr = make_int2(0, 0);
+            if (c < n) {
+                pr = cand[c];
+                bits = ccd_pair_mask(x0, x1, pr.x, pr.y);
+            }
+            if (MODE == CCD_MINCOL) {
+                while (bits) {
+                    int k = __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    OutRegion R = out_region(F, M, pr.x, max_per_tri);
+                    long long r = append_row(mesh_counters, F, R.m, R.cap, &hdr->status);
+                    if (r >= 0) {
+                        long long o = (long long)R.po * max_per_tri + r;
+                        rows[o * 3 + 0] = pr.x - R.po;
+                        rows[o * 3 + 1] = pr.y - R.po;
+                        rows[o * 3 + 2] = k;
+                    }
+                }
+                continue;
+            }
+            // append the chunk's sub-tests (block-wide exclusive scan of the counts)
+            const int cnt = __popc(bits);
+            const int incl = warp_inclusive_scan(cnt, lane);
+            if (lane == 31) ints[CI_WARP + warp] = incl;
+            __syncthreads();
+            if (warp == 0) {
+                int v = lane < NW ? ints[CI_WARP + lane] : 0;
+                int sc = warp_inclusive_scan(v, lane);
+                if (lane < NW) ints[CI_WARP + lane] = sc - v;
+                if (lane == 31) ints[CI_TOTAL] = sc;
+            }
+            __syncthreads();
+            int pos = head + queued + ints[CI_WARP + warp] + incl - cnt;
+            const int total = ints[CI_TOTAL];
             while (bits) {
                 int k = __ffs(bits) - 1;
                 bits &= bits - 1;
-                OutRegion R = out_region(F, M, pr.x, max_per_tri);
-                long long r = append_row(mesh_counters, F, R.m, R.cap, &hdr->status);
-                if (r >= 0) {
-                    long long o = (long long)R.po * max_per_tri + r;
-                    rows[o * 3 + 0] = pr.x - R.po;
-                    rows[o * 3 + 1] = pr.y - R.po;
-                    rows[o * 3 + 2] = k;
-                }
+                items[pos % Q] = pack_subtest(pr.x, pr.y, k);
+                ++pos;
             }
-            continue;
+            if (tid == 0 && total) atomicAdd(&hdr->subtests, total);
+            queued += total;
+            __syncthreads();
         }
-        // stage the sub-tests of the chunk (block-wide exclusive scan of the counts)
-        const int cnt = __popc(bits);
-        const int incl = warp_inclusive_scan(cnt, lane);
-        if (lane == 31) ints[CI_WARP + warp] = incl;
-        __syncthreads();
-        if (warp == 0) {
-            int v = lane < NW ? ints[CI_WARP + lane] : 0;
-            int sc = warp_inclusive_scan(v, lane);
-            if (lane < NW) ints[CI_WARP + lane] = sc - v;
-            if (lane == 31) ints[CI_TOTAL] = sc;
-        }
-        __syncthreads();
-        int pos = ints[CI_WARP + warp] + incl - cnt;
-        const int total = ints[CI_TOTAL];
-        while (bits) {
-            int k = __ffs(bits) - 1;
-            bits &= bits - 1;
-            items[pos++] = (unsigned short)((tid << 4) | k);
-        }
-        pairs[tid] = pr;
-        if (tid == 0 && total) atomicAdd(&hdr->subtests, total);
-        __syncthreads();
-        for (int b0 = 0; b0 < total; b0 += NB) {
-            const int nb = min(NB, total - b0);
+        // solve full batches (and, after the last chunk, the remainder)
+        while (queued >= NB || (!more && queued > 0)) {
+            const int nb = min(NB, queued);
             if (tid < 8) ints[CI_COUNT + tid] = 0;           // class counts and cursors
             if (tid == 8) ints[CI_ROOTS] = 0;
             __syncthreads();
             // (1) coefficients and solver prefix
             for (int ri = tid; ri < nb; ri += CCD_BLOCK) {
-                int item = items[b0 + ri];
-                int k = item & 15;
-                int2 q = pairs[item >> 4];
-                MTet<T> tet = load_tet(x0, x1, q.x, q.y, k);
+                int2 it = items[(head + ri) % Q];
+                int k = (it.y >> 28) & 15;
+                MTet<T> tet = load_tet(x0, x1, it.x, it.y & 0x0fffffff, k);
                 T cf[4];
                 cubic_coeffs(tet, cf);
                 double g, h;
@@ -638,7 +649,6 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                 rec[3 * NB + ri] = (double)cf[3];
                 rec[4 * NB + ri] = g;
                 rec[5 * NB + ri] = h;
-                rec_item[ri] = (unsigned short)item;
                 rec_cls[ri] = (unsigned char)cls;
                 if (cls != CUBIC_NONE) atomicAdd(&ints[CI_COUNT + cls - 1], 1);
             }
@@ -692,9 +702,9 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
             if (tid == 0 && nroots) atomicAdd(&hdr->roots, nroots);
             // (3) filter and output
             for (int j = tid; j < nroots; j += CCD_BLOCK) {
-                int item = rec_item[root_rec[j]];
-                int k = item & 15;
-                int2 q = pairs[item >> 4];
+                int2 it = items[(head + root_rec[j]) % Q];
+                int k = (it.y >> 28) & 15;
+                int2 q = make_int2(it.x, it.y & 0x0fffffff);
                 T root = root_val[j];
                 MTet<T> tet = load_tet(x0, x1, q.x, q.y, k);
                 if (!ccd_filter(tet, k, root)) continue;
@@ -717,6 +727,8 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                     sink.add(tet, q.x, q.y, k, root, ct, F, M, &hdr->status);
                 }
             }
+            head = (head + nb) % Q;
+            queued -= nb;
             __syncthreads();
         }
     }
