@@ -25,9 +25,10 @@ import sysconfig
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 SHIM = os.path.join(HERE, "ref_shim")
+DEFAULT_SRC = "/root/reference"
 
 
-def build(src="/root/reference", force=False) -> str:
+def build(src=DEFAULT_SRC, force=False) -> str:
     so = os.path.join(OUT, "cccollisions.so")
     if os.path.exists(so) and not force:
         return so
@@ -57,7 +58,7 @@ def build(src="/root/reference", force=False) -> str:
     return so
 
 
-def build_probe(src="/root/reference", force=False) -> str:
+def build_probe(src=DEFAULT_SRC, force=False) -> str:
     """oracle/_ref/libref_probe.so: oracle/ref_probe.cu + the reference sources (stage probe)."""
     so = os.path.join(OUT, "libref_probe.so")
     if os.path.exists(so) and not force:
