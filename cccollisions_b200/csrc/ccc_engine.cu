@@ -50,7 +50,7 @@ struct EngineLayout {
     int64_t hdr, mesh_cnt, contacts, iters, flags, state_end;
     int64_t tab, btab, bounds;
     int64_t x0, x1, masses, faces;
-    int64_t leaf_tri, lparent, nparent, visits, nodes, lbox;
+    int64_t leaf_tri, lparent, nparent, visits, nodes;
     int64_t rows, times, cand;
     int64_t keys0, keys1, vals0, vals1, hist;
     int64_t verts0, verts1, vel, acc, end;
@@ -84,7 +84,6 @@ EngineLayout engine_layout(int64_t tsz, int64_t tc, int64_t vc, int64_t mc, int6
     L.nparent = take(tc * 4);
     L.visits = take(tc * 4);
     L.nodes = take(tc * (int64_t)sizeof(TNode));
-    L.lbox = take(tc * 6 * tsz);
     L.rows = take(tc * maxcol * 3 * 8);
     L.times = take(tc * maxcol * tsz);
     L.cand_cap = tc * maxc;
@@ -242,14 +241,14 @@ inline int refit_grid(const ccc_engine* e) {
 template <class T> int refit(ccc_engine* e, const Tables& t, const int* flags, cudaStream_t s) {
     CCC_LAUNCH("k_engine_refit", s, k_engine_refit<T><<<refit_grid(e), ITEM_THREADS, 0, s>>>(
         t.f, e->at<T>(e->L.x0), e->at<T>(e->L.x1), e->at<int>(e->L.leaf_tri), e->at<int>(e->L.lparent),
-        e->at<int>(e->L.nparent), e->at<TNode>(e->L.nodes), e->at<unsigned>(e->L.visits), e->at<T>(e->L.lbox), flags,
+        e->at<int>(e->L.nparent), e->at<TNode>(e->L.nodes), e->at<unsigned>(e->L.visits), flags,
         &e->hdr()->status));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
 
 template <class T> int traverse(ccc_engine* e, const Tables& t, const int* flags, cudaStream_t s) {
-    SceneLeaves<T> lv{e->at<T>(e->L.lbox), e->at<int>(e->L.leaf_tri)};
+    SceneLeaves<T> lv{e->at<TNode>(e->L.nodes), e->at<int>(e->L.lparent), e->at<int>(e->L.leaf_tri)};
     int g = num_sms() * SHAPES[e->shape].trav;
     int cap = (int)e->L.cand_cap;
     if (sizeof(T) == 4)

@@ -8,9 +8,10 @@
 // swept centroids, normalised by the mesh's own centroid bounds, sorted by a stable LSD
 // radix sort (keys: mesh index above the code, so one sort orders every mesh at once).
 // Topology is built once; every step only refits the boxes, bottom-up, straight into the
-// traversal nodes (TNode, fp32 rounded outward).  The exact (T precision) leaf boxes are
-// kept beside them for the leaf recheck, so the candidate pairs are exactly the pairs
-// whose T-precision swept boxes overlap, as in the reference's traversal.
+// traversal nodes (TNode, fp32 rounded outward); a leaf's query box is its box in its
+// parent's node.  The candidate pairs are therefore a superset of the pairs whose
+// T-precision swept boxes overlap; the continuous narrow phase re-tests every pair's swept
+// sub-boxes exactly, so its output is that of the reference's exact candidate set.
 //
 // The impulse loop adds a vertex arena: faces map triangle corners to vertices, contacts
 // add their impulses to per-vertex fixed-point accumulators (integer atomics, so the sums
@@ -350,7 +351,8 @@ static __global__ void k_karras_build(Forest F, const unsigned long long* __rest
 }
 
 // ---------------------------------------------------------------------------------------
-// Refit: exact swept leaf boxes, then the fp32 child boxes of every node, bottom-up.
+// Refit: swept leaf boxes rounded outward to fp32, then the child boxes of every node,
+// bottom-up.
 
 template <class T> __device__ __forceinline__ void box_outward_f32(const Box<T>& b, float lo[3], float hi[3]) {
     T l[3] = {b.lo.x, b.lo.y, b.lo.z}, h[3] = {b.hi.x, b.hi.y, b.hi.z};
@@ -393,7 +395,7 @@ __device__ __forceinline__ void node_box(const TNode* nd, float lo[3], float hi[
 template <class T>
 __global__ void k_engine_refit(Forest F, const T* __restrict__ x0, const T* __restrict__ x1,
                                const int* __restrict__ leaf_tri, const int* __restrict__ lparent,
-                               const int* __restrict__ nparent, TNode* nodes, unsigned* visits, T* __restrict__ lbox,
+                               const int* __restrict__ nparent, TNode* nodes, unsigned* visits,
                                const int* __restrict__ mflags, int* status) {
     const int M = forest_size(F);
     const int total = __ldg(F.voff + M);
@@ -408,7 +410,6 @@ __global__ void k_engine_refit(Forest F, const T* __restrict__ x0, const T* __re
         if (t < 0 || t >= n) { atomicOr(status, ST_MALFORMED_TREE); continue; }
         long long slot = (long long)po + t;
         Box<T> b = merge(tri_box(load_tri(x0, slot)), tri_box(load_tri(x1, slot)));
-        store_box(lbox + ((long long)po + p) * 6, b);
         float lo[3], hi[3];
         box_outward_f32(b, lo, hi);
         TNode* nd = nodes + po;

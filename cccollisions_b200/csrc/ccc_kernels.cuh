@@ -308,6 +308,7 @@ __device__ __forceinline__ float nudge_up(float x) { return nextafterf(x, INFINI
 template <class T> struct TensorLeaves {
     const T* bboxes;
     const long long* tree;
+    static constexpr bool kSlotQuery = false;
     __device__ __forceinline__ long long row(int m, int vo, int n, int pos) const {
         return 2LL * vo - m + (n - 1) + pos;
     }
@@ -319,10 +320,23 @@ template <class T> struct TensorLeaves {
     }
 };
 template <class T> struct SceneLeaves {
-    const T* lbox;          // 6 values per leaf slot: min xyz, max xyz
+    const TNode* nodes;     // the query box of a leaf is its fp32 box in its parent's node
+    const int* lparent;     // (parent << 1) | side per leaf slot
     const int* leaf_tri;    // mesh-local triangle id per leaf slot
-    __device__ __forceinline__ Box<T> box(int m, int vo, int po, int n, int pos) const {
-        return load_box(lbox + (long long)(po + pos) * 6);
+    static constexpr bool kSlotQuery = true;
+    // fp32 box of leaf pos (rounded outward by the refit); false for a bad parent code
+    __device__ __forceinline__ bool query_f32(int po, int n, int pos, float lo[3], float hi[3]) const {
+        int code = __ldg(lparent + po + pos);
+        int par = code >> 1;
+        if (code < 0 || par >= n - 1) return false;
+        const float4* f = reinterpret_cast<const float4*>(nodes + po + par);
+        float4 A = __ldg(f + 0), B = __ldg(f + 1), C = __ldg(f + 2);
+        if ((code & 1) == 0) {
+            lo[0] = A.x; lo[1] = A.y; lo[2] = A.z; hi[0] = A.w; hi[1] = B.x; hi[2] = B.y;
+        } else {
+            lo[0] = B.z; lo[1] = B.w; lo[2] = C.x; hi[0] = C.y; hi[1] = C.z; hi[2] = C.w;
+        }
+        return true;
     }
     __device__ __forceinline__ long long id(int m, int vo, int po, int n, int pos) const {
         return __ldg(leaf_tri + po + pos);
@@ -349,7 +363,6 @@ k_traverse(const TNode* __restrict__ nodes, Leaves leaves, Forest F, const uint8
         if (MASKED && !mask[po + p]) continue;
         if (mflags && (__ldg(mflags + __ldg(F.sid + m)) & MF_DONE)) continue;
         const TNode* nd = nodes + po;
-        Box<T> q = leaves.box(m, vo, po, n, p);
         long long qid64 = leaves.id(m, vo, po, n, p);
         if (qid64 < 0 || qid64 >= n) {
             atomicOr(&hdr->status, ST_MALFORMED_TREE);
@@ -357,8 +370,17 @@ k_traverse(const TNode* __restrict__ nodes, Leaves leaves, Forest F, const uint8
         }
         int qid = (int)qid64;
         // conservative fp32 query box: threshold folded in, rounded outward, nudged one more ulp
+        // (resident trees: the refit's outward-rounded fp32 box, for threshold 0)
         float qlo[3], qhi[3];
-        {
+        Box<T> q;
+        if constexpr (Leaves::kSlotQuery) {
+            static_assert(!(RECHECK && !EXACT_F32), "the exact leaf test needs exact leaf boxes");
+            if (!leaves.query_f32(po, n, p, qlo, qhi)) {
+                atomicOr(&hdr->status, ST_MALFORMED_TREE);
+                continue;
+            }
+        } else {
+            q = leaves.box(m, vo, po, n, p);
             T lo[3] = {q.lo.x, q.lo.y, q.lo.z}, hi[3] = {q.hi.x, q.hi.y, q.hi.z};
             for (int c = 0; c < 3; ++c) {
                 if (EXACT_F32) {
@@ -401,7 +423,8 @@ k_traverse(const TNode* __restrict__ nodes, Leaves leaves, Forest F, const uint8
                     int cpos = ~ref;
                     int cid = s ? D.w : D.z;
                     if (MASKED && mask[po + cid] && !(qid < cid)) hit = false;
-                    if (RECHECK && hit && !EXACT_F32) hit = overlap(q, leaves.box(m, vo, po, n, cpos), th);
+                    if constexpr (!Leaves::kSlotQuery)
+                        if (RECHECK && hit && !EXACT_F32) hit = overlap(q, leaves.box(m, vo, po, n, cpos), th);
                     if (hit) {
                         cg::coalesced_group grp = cg::coalesced_threads();
                         int slot = 0;
