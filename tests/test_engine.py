@@ -219,3 +219,80 @@ def test_impulse_loop_graph_replay(cuda):
     for sid in sids:
         assert np.array_equal(eng.view(sid)["verts1"].cpu().numpy(), out_direct[sid])
     eng.close()
+
+
+def test_engine_edge_cases_match_oracle(cuda, oracle):
+    """A two-triangle mesh, a flat sheet in rigid translation far from everything and a
+    static mesh (x1 = x0) — both without rows, every root being a dropped linear case — and
+    a slot reused by a different mesh."""
+    from cccollisions_b200 import _native as N
+    from cccollisions_b200 import workloads as W
+    two = W.jittered_fold(40, 2, 3)                      # 2 triangles
+    far = W.jittered_fold(41, 6, 6, noise=0.0, fold=False)      # flat sheet, rigid translation
+    far = (far[0] + 100.0, far[1] + 100.0, far[2])
+    fold = W.jittered_fold(42, 9, 9)
+    static = (fold[0], fold[0].copy(), fold[2])
+    meshes = [two, far, fold, static]
+    with N.math_library(N.LIB_PORTABLE):
+        eng, sids = _engine(meshes + [W.jittered_fold(43, 12, 12)])
+        # replace the last mesh by another of a different size in the freed slots
+        eng.remove_mesh(sids[-1])
+        other = W.jittered_fold(44, 10, 8)
+        sid = eng.add_mesh(other[0].shape[0])
+        eng.upload_soup(sid, other[0], other[1])
+        meshes, sids = meshes + [other], sids[:-1] + [sid]
+        eng.set_active(sids)
+        eng.build(sids)
+        eng.ccd()
+        st = eng.state(sids)
+        assert st["status"] == 0
+        for sid, (x0, x1, _), n in zip(sids, meshes, st["rows"]):
+            rows, times = eng.collisions(sid, int(n))
+            bb, tr = oracle.bvh(x0, x1)
+            er, et = oracle.ccd(bb, tr, x0, x1)
+            assert _ms(rows.cpu().numpy(), times.cpu().numpy()) == _ms(er, et)
+        assert st["rows"][1] == 0 and st["rows"][3] == 0
+        eng.close()
+
+
+def test_engine_rejects_misuse(cuda):
+    from cccollisions_b200.engine import Engine
+    eng = Engine(tri_capacity=256, mesh_capacity=4)
+    with pytest.raises(RuntimeError):
+        eng.add_mesh(1)                                  # a mesh needs two triangles
+    a = eng.add_mesh(20)
+    eng.set_active([a])
+    with pytest.raises(RuntimeError):
+        eng.ccd()                                        # no tree built yet
+    with pytest.raises(RuntimeError):
+        eng.set_active([a, a])                           # duplicate slot
+    with pytest.raises(RuntimeError):
+        eng.set_active([3])                              # unused slot
+    with pytest.raises(RuntimeError):
+        eng.loop_prepare([a])                            # collision-only mesh has no vertices
+    eng.close()
+
+
+def test_engine_full_size_meshes_match_reference_format_path(cuda):
+    """Eight meshes of the batched workload at their real sizes (cloth of log-uniform
+    1e3..1e5 triangles over a 20,480-triangle sphere): rows and times equal, as multisets,
+    to the reference-format path's, in the default math mode."""
+    import cccollisions_b200 as C
+    from cccollisions_b200 import workloads as W
+    meshes = [(x0, x1, None) for x0, x1 in W.batched(8, seed0=2000)]
+    eng, sids = _engine(meshes, max_candidates_per_triangle=32)
+    eng.set_active(sids)
+    eng.build(sids)
+    eng.ccd()
+    st = eng.state(sids)
+    assert st["status"] == 0
+    for sid, (x0, x1, _), n in zip(sids, meshes, st["rows"]):
+        X0 = torch.from_numpy(x0[None]).cuda()
+        X1 = torch.from_numpy(x1[None]).cuda()
+        bb, tr = C.bvh_motion(X0, X1)
+        rows, times = C.find_collisions_continuous(bb, tr, X0, X1, 32, 16)
+        r = rows[0].cpu().numpy()
+        k = int((r[:, 0] >= 0).sum())
+        got = eng.collisions(sid, int(n))
+        assert _ms(got[0].cpu().numpy(), got[1].cpu().numpy()) == _ms(r[:k], times[0, :k, 0].cpu().numpy())
+    eng.close()
