@@ -50,7 +50,7 @@ struct EngineLayout {
     int64_t hdr, mesh_cnt, contacts, iters, flags, state_end;
     int64_t tab, btab, bounds;
     int64_t x0, x1, masses, faces;
-    int64_t leaf_tri, lparent, nparent, visits, nodes;
+    int64_t leaf_tri, lparent, nparent, visits, nodes, qnodes, qcode, qleaf;
     int64_t rows, times, cand;
     int64_t keys0, keys1, vals0, vals1, hist;
     int64_t verts0, verts1, vel, acc, end;
@@ -84,6 +84,9 @@ EngineLayout engine_layout(int64_t tsz, int64_t tc, int64_t vc, int64_t mc, int6
     L.nparent = take(tc * 4);
     L.visits = take(tc * 4);
     L.nodes = take(tc * (int64_t)sizeof(TNode));
+    L.qnodes = take(tc * (int64_t)sizeof(QNode));
+    L.qcode = take(tc * 4);
+    L.qleaf = take(tc * 4);
     L.rows = take(tc * maxcol * 3 * 8);
     L.times = take(tc * maxcol * tsz);
     L.cand_cap = tc * maxc;
@@ -241,22 +244,17 @@ inline int refit_grid(const ccc_engine* e) {
 template <class T> int refit(ccc_engine* e, const Tables& t, const int* flags, cudaStream_t s) {
     CCC_LAUNCH("k_engine_refit", s, k_engine_refit<T><<<refit_grid(e), ITEM_THREADS, 0, s>>>(
         t.f, e->at<T>(e->L.x0), e->at<T>(e->L.x1), e->at<int>(e->L.leaf_tri), e->at<int>(e->L.lparent),
-        e->at<int>(e->L.nparent), e->at<TNode>(e->L.nodes), e->at<unsigned>(e->L.visits), flags,
-        &e->hdr()->status));
+        e->at<int>(e->L.nparent), e->at<int>(e->L.qcode), e->at<int>(e->L.qleaf),
+        e->at<QNode>(e->L.qnodes), e->at<unsigned>(e->L.visits), flags, &e->hdr()->status));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
 
 template <class T> int traverse(ccc_engine* e, const Tables& t, const int* flags, cudaStream_t s) {
-    SceneLeaves<T> lv{e->at<TNode>(e->L.nodes), e->at<int>(e->L.lparent), e->at<int>(e->L.leaf_tri)};
     int g = num_sms() * SHAPES[e->shape].trav;
-    int cap = (int)e->L.cand_cap;
-    if (sizeof(T) == 4)
-        CCC_LAUNCH("k_traverse", s, k_traverse<T, false, true><<<g, TRAV_THREADS, 0, s>>>(
-            e->at<TNode>(e->L.nodes), lv, t.f, nullptr, (T)0, e->at<int2>(e->L.cand), cap, e->hdr(), flags));
-    else
-        CCC_LAUNCH("k_traverse", s, k_traverse<T, false, false, SceneLeaves<T>, false><<<g, TRAV_THREADS, 0, s>>>(
-            e->at<TNode>(e->L.nodes), lv, t.f, nullptr, (T)0, e->at<int2>(e->L.cand), cap, e->hdr(), flags));
+    CCC_LAUNCH("k_traverse", s, k_traverse_q<<<g, TRAV_THREADS, 0, s>>>(
+        e->at<QNode>(e->L.qnodes), e->at<int>(e->L.qleaf), e->at<int>(e->L.leaf_tri), t.f, e->at<int2>(e->L.cand),
+        (int)e->L.cand_cap, e->hdr(), flags));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -350,6 +348,13 @@ template <class T> int build_trees(ccc_engine* e, int64_t ntri, int64_t nb, cuda
     CCC_LAUNCH("k_karras_build", s, k_karras_build<<<item_grid(), ITEM_THREADS, 0, s>>>(
         t.f, keys[cur], vals[cur], e->at<TNode>(e->L.nodes), e->at<int>(e->L.nparent), e->at<int>(e->L.lparent),
         e->at<int>(e->L.leaf_tri), e->at<unsigned>(e->L.visits), &e->hdr()->status));
+    CCC_LAUNCH_CHECK();
+    CCC_LAUNCH("k_qtree_depth", s, k_qtree_depth<<<item_grid(), ITEM_THREADS, 0, s>>>(
+        t.f, e->at<int>(e->L.nparent), e->at<int>(e->L.qcode), &e->hdr()->status));
+    CCC_LAUNCH_CHECK();
+    CCC_LAUNCH("k_qtree_slots", s, k_qtree_slots<<<item_grid(), ITEM_THREADS, 0, s>>>(
+        t.f, e->at<TNode>(e->L.nodes), e->at<int>(e->L.qcode), e->at<int>(e->L.qleaf), e->at<QNode>(e->L.qnodes),
+        &e->hdr()->status));
     CCC_LAUNCH_CHECK();
     return refit<T>(e, t, nullptr, s);
 }

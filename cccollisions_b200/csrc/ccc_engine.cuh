@@ -351,8 +351,111 @@ static __global__ void k_karras_build(Forest F, const unsigned long long* __rest
 }
 
 // ---------------------------------------------------------------------------------------
-// Refit: swept leaf boxes rounded outward to fp32, then the child boxes of every node,
-// bottom-up.
+// Four-wide nodes.  Every even-depth internal node b of the binary tree (the root has depth
+// 0) heads a QNode whose 2 to 4 slots are b's children, where a child that is itself an
+// internal node (odd depth) is replaced by its two children.  A slot holds a child box
+// (fp32, rounded outward), a reference (>= 0: the QNode of an even-depth internal node;
+// ~pos: the leaf at sorted position pos) and an aux word (the rightmost leaf position below
+// an internal slot, the triangle id of a leaf slot).  Unused slots hold an empty box.
+// QNodes are indexed by their binary node.  One QNode visit covers two binary levels, so a
+// tree walk needs half as many dependent node fetches.
+struct __align__(16) QNode {
+    float4 lox, loy, loz, hix, hiy, hiz;
+    int4 ref, aux;
+};
+static constexpr int Q_EMPTY = 0x7fffffff;
+// qcode of an internal node: (QNode << 2) | slot for an even-depth node below the root;
+// QCODE_ROOT for the root; for an odd-depth node, which has no slot of its own,
+// QCODE_ODD - ((QNode << 2) | first slot) locates the two adjacent slots of its children
+static constexpr int QCODE_ROOT = -1;
+static constexpr int QCODE_ODD = -2;
+
+// depth parity of every internal node (a climb to the root); even nodes other than the root
+// get their slot code from k_qtree_slots
+static __global__ void k_qtree_depth(Forest F, const int* __restrict__ nparent, int* __restrict__ qcode,
+                                     int* __restrict__ status) {
+    const int M = forest_size(F);
+    const int total_internal = __ldg(F.voff + M) - M;
+    for (int gi = blockIdx.x * blockDim.x + threadIdx.x; gi < total_internal; gi += gridDim.x * blockDim.x) {
+        int m = find_mesh(F.voff, M, gi, 1);
+        int vo = __ldg(F.voff + m), po = __ldg(F.poff + m);
+        int n = __ldg(F.voff + m + 1) - vo;
+        int i = gi - (vo - m);
+        int depth = 0, x = i;
+        for (int guard = 0; x != 0 && guard < n; ++guard) {
+            int code = __ldg(nparent + po + x);
+            if (code < 0 || (code >> 1) >= n - 1) { atomicOr(status, ST_MALFORMED_TREE); break; }
+            x = code >> 1;
+            ++depth;
+        }
+        qcode[po + i] = i == 0 ? QCODE_ROOT : ((depth & 1) ? QCODE_ODD : 0);
+    }
+}
+
+// slots of every QNode: references, aux words, empty boxes (the refit fills them), and the
+// slot code of every leaf (qleaf) and even-depth internal node (qcode) they hold
+static __global__ void k_qtree_slots(Forest F, const TNode* __restrict__ nodes, int* __restrict__ qcode,
+                                     int* __restrict__ qleaf, QNode* __restrict__ qnodes, int* __restrict__ status) {
+    const int M = forest_size(F);
+    const int total_internal = __ldg(F.voff + M) - M;
+    for (int gi = blockIdx.x * blockDim.x + threadIdx.x; gi < total_internal; gi += gridDim.x * blockDim.x) {
+        int m = find_mesh(F.voff, M, gi, 1);
+        int vo = __ldg(F.voff + m), po = __ldg(F.poff + m);
+        int n = __ldg(F.voff + m + 1) - vo;
+        int i = gi - (vo - m);
+        if (qcode[po + i] <= QCODE_ODD) continue;
+        int4 d = nodes[po + i].d;
+        int ref[4] = {Q_EMPTY, Q_EMPTY, Q_EMPTY, Q_EMPTY}, aux[4] = {0, 0, 0, 0};
+        int ns = 0;
+        bool ok = true;
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            int r = side ? d.y : d.x, a = side ? d.w : d.z;
+            if (r < 0) {
+                ok = ok && ~r < n;
+                ref[ns] = r;
+                aux[ns] = a;
+                ++ns;
+            } else if (r < n - 1) {
+                int4 dc = nodes[po + r].d;     // odd-depth child: its two children take its place
+                qcode[po + r] = QCODE_ODD - ((i << 2) | ns);
+                ref[ns] = dc.x;
+                aux[ns] = dc.z;
+                ++ns;
+                ref[ns] = dc.y;
+                aux[ns] = dc.w;
+                ++ns;
+            } else {
+                ok = false;
+            }
+        }
+        for (int sl = 0; sl < ns && ok; ++sl) {
+            int r = ref[sl];
+            if (r < 0) {
+                if (~r >= n) { ok = false; break; }
+                qleaf[po + ~r] = (i << 2) | sl;
+            } else {
+                if (r >= n - 1) { ok = false; break; }
+                qcode[po + r] = (i << 2) | sl;
+            }
+        }
+        if (!ok) {
+            atomicOr(status, ST_MALFORMED_TREE);
+            continue;
+        }
+        QNode q;
+        const float inf = __int_as_float(0x7f800000);
+        q.lox = q.loy = q.loz = make_float4(inf, inf, inf, inf);
+        q.hix = q.hiy = q.hiz = make_float4(-inf, -inf, -inf, -inf);
+        q.ref = make_int4(ref[0], ref[1], ref[2], ref[3]);
+        q.aux = make_int4(aux[0], aux[1], aux[2], aux[3]);
+        qnodes[po + i] = q;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Refit: swept leaf boxes rounded outward to fp32 into their slots, then bottom-up the box of
+// every even-depth node into its own slot.
 
 template <class T> __device__ __forceinline__ void box_outward_f32(const Box<T>& b, float lo[3], float hi[3]) {
     T l[3] = {b.lo.x, b.lo.y, b.lo.z}, h[3] = {b.hi.x, b.hi.y, b.hi.z};
@@ -368,34 +471,40 @@ template <class T> __device__ __forceinline__ void box_outward_f32(const Box<T>&
     }
 }
 
-// child slot `side` of node: left = a.xyzw b.xy, right = b.zw c.xyzw
-__device__ __forceinline__ void write_child_box(TNode* nd, int side, const float lo[3], const float hi[3]) {
-    float4* f = reinterpret_cast<float4*>(nd);
-    float2* h = reinterpret_cast<float2*>(nd);
-    if (side == 0) {
-        f[0] = make_float4(lo[0], lo[1], lo[2], hi[0]);
-        h[2] = make_float2(hi[1], hi[2]);
-    } else {
-        h[3] = make_float2(lo[0], lo[1]);
-        f[2] = make_float4(lo[2], hi[0], hi[1], hi[2]);
-    }
+__device__ __forceinline__ void write_qslot(QNode* qn, int code, const float lo[3], const float hi[3]) {
+    float* f = reinterpret_cast<float*>(qn + (code >> 2));
+    const int sl = code & 3;
+    f[0 + sl] = lo[0];
+    f[4 + sl] = lo[1];
+    f[8 + sl] = lo[2];
+    f[12 + sl] = hi[0];
+    f[16 + sl] = hi[1];
+    f[20 + sl] = hi[2];
 }
 
-// union of both child boxes of node, read through L2 (written by other blocks)
-__device__ __forceinline__ void node_box(const TNode* nd, float lo[3], float hi[3]) {
-    const float4* f = reinterpret_cast<const float4*>(nd);
-    float4 A = __ldcg(f + 0), B = __ldcg(f + 1), C = __ldcg(f + 2);
-    lo[0] = fminf(A.x, B.z); lo[1] = fminf(A.y, B.w); lo[2] = fminf(A.z, C.x);
-    hi[0] = fmaxf(A.w, C.y); hi[1] = fmaxf(B.x, C.z); hi[2] = fmaxf(B.y, C.w);
+// one slot's box, read through L2 (written by other blocks)
+__device__ __forceinline__ void read_qslot(const QNode* qn, int code, float lo[3], float hi[3]) {
+    const float* f = reinterpret_cast<const float*>(qn + (code >> 2));
+    const int sl = code & 3;
+    lo[0] = __ldcg(f + 0 + sl);
+    lo[1] = __ldcg(f + 4 + sl);
+    lo[2] = __ldcg(f + 8 + sl);
+    hi[0] = __ldcg(f + 12 + sl);
+    hi[1] = __ldcg(f + 16 + sl);
+    hi[2] = __ldcg(f + 20 + sl);
 }
 
-// Every node is reached twice per refit; the refit counters only ever grow, and the
+__device__ __forceinline__ float hmin4(float4 v) { return fminf(fminf(v.x, v.y), fminf(v.z, v.w)); }
+__device__ __forceinline__ float hmax4(float4 v) { return fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)); }
+
+// Every binary node is reached twice per refit; the refit counters only ever grow, and the
 // arrival that finds an odd count is the second one, so nothing has to be cleared between
 // steps.  Meshes with MF_DONE set in mflags (when given) are skipped.
 template <class T>
 __global__ void k_engine_refit(Forest F, const T* __restrict__ x0, const T* __restrict__ x1,
                                const int* __restrict__ leaf_tri, const int* __restrict__ lparent,
-                               const int* __restrict__ nparent, TNode* nodes, unsigned* visits,
+                               const int* __restrict__ nparent, const int* __restrict__ qcode,
+                               const int* __restrict__ qleaf, QNode* qnodes, unsigned* visits,
                                const int* __restrict__ mflags, int* status) {
     const int M = forest_size(F);
     const int total = __ldg(F.voff + M);
@@ -412,17 +521,139 @@ __global__ void k_engine_refit(Forest F, const T* __restrict__ x0, const T* __re
         Box<T> b = merge(tri_box(load_tri(x0, slot)), tri_box(load_tri(x1, slot)));
         float lo[3], hi[3];
         box_outward_f32(b, lo, hi);
-        TNode* nd = nodes + po;
+        QNode* qn = qnodes + po;
+        const int lq = __ldg(qleaf + po + p);
+        if (lq < 0 || (lq >> 2) >= n - 1) { atomicOr(status, ST_MALFORMED_TREE); continue; }
+        write_qslot(qn, lq, lo, hi);
         int code = __ldg(lparent + po + p);
         for (int guard = 0; guard < n; ++guard) {
             int node = code >> 1;
             if (code < 0 || node >= n - 1) { atomicOr(status, ST_MALFORMED_TREE); break; }
-            write_child_box(nd + node, code & 1, lo, hi);
             __threadfence();
             if ((atomicAdd(visits + po + node, 1u) & 1u) == 0u) break;     // first arrival
-            node_box(nd + node, lo, hi);
+            const int qc = __ldg(qcode + po + node);
+            if (qc <= QCODE_ODD) {
+                // its box is the union of its two children's adjacent slots in the QNode above
+                const int c0 = QCODE_ODD - qc;
+                if ((c0 >> 2) >= n - 1 || (c0 & 3) > 2) { atomicOr(status, ST_MALFORMED_TREE); break; }
+                float l2[3], h2[3];
+                read_qslot(qn, c0, lo, hi);
+                read_qslot(qn, c0 + 1, l2, h2);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    lo[c] = fminf(lo[c], l2[c]);
+                    hi[c] = fmaxf(hi[c], h2[c]);
+                }
+            } else {
+                // the union of its QNode's slots (unused slots are empty boxes)
+                const float4* f = reinterpret_cast<const float4*>(qn + node);
+                lo[0] = hmin4(__ldcg(f + 0));
+                lo[1] = hmin4(__ldcg(f + 1));
+                lo[2] = hmin4(__ldcg(f + 2));
+                hi[0] = hmax4(__ldcg(f + 3));
+                hi[1] = hmax4(__ldcg(f + 4));
+                hi[2] = hmax4(__ldcg(f + 5));
+                if (qc == QCODE_ROOT) break;
+                if (qc < 0 || (qc >> 2) >= n - 1) { atomicOr(status, ST_MALFORMED_TREE); break; }
+                write_qslot(qn, qc, lo, hi);
+            }
             code = __ldg(nparent + po + node);
-            if (code < 0) break;                                           // root done
+            if (code < 0) break;
+        }
+    }
+}
+
+// Continuous-collision candidates of resident trees: one query leaf per thread walks the
+// QNodes with an explicit stack in shared memory, tests the 4 slot boxes of a node at once
+// (fp32; the query box is the leaf's own outward-rounded slot box), keeps the reference's
+// order rule (a slot is skipped when its rightmost leaf position is not after the query's,
+// so each unordered pair is found once) and emits (min id, max id) in data slots.  Candidates
+// are the pairs whose fp32 boxes overlap, a superset of the exact ones; the continuous
+// narrow phase re-tests every pair's swept sub-boxes exactly.
+static __global__ void __launch_bounds__(TRAV_THREADS)
+k_traverse_q(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, const int* __restrict__ leaf_tri,
+             Forest F, int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const int* __restrict__ mflags) {
+    __shared__ int stack[STACK_DEPTH][TRAV_THREADS];
+    const int tid = threadIdx.x;
+    const int M = forest_size(F);
+    const int total = __ldg(F.voff + M);
+    for (int v = blockIdx.x * blockDim.x + tid; v < total; v += gridDim.x * blockDim.x) {
+        int m = find_mesh(F.voff, M, v, 0);
+        int vo = __ldg(F.voff + m), po = __ldg(F.poff + m);
+        int n = __ldg(F.voff + m + 1) - vo;
+        int p = v - vo;
+        if (n < 2) continue;
+        if (mflags && (__ldg(mflags + __ldg(F.sid + m)) & MF_DONE)) continue;
+        const QNode* qn = qnodes + po;
+        const int qid = __ldg(leaf_tri + po + p);
+        const int lq = __ldg(qleaf + po + p);
+        if (qid < 0 || qid >= n || lq < 0 || (lq >> 2) >= n - 1) {
+            atomicOr(&hdr->status, ST_MALFORMED_TREE);
+            continue;
+        }
+        float qlo[3], qhi[3];
+        {
+            const float* f = reinterpret_cast<const float*>(qn + (lq >> 2));
+            const int sl = lq & 3;
+            qlo[0] = __ldg(f + 0 + sl);
+            qlo[1] = __ldg(f + 4 + sl);
+            qlo[2] = __ldg(f + 8 + sl);
+            qhi[0] = __ldg(f + 12 + sl);
+            qhi[1] = __ldg(f + 16 + sl);
+            qhi[2] = __ldg(f + 20 + sl);
+        }
+        int sp = 0;
+        int node = 0;
+        const int limit = 2 * n + 64;
+        for (int it = 0;; ++it) {
+            if (it > limit) { atomicOr(&hdr->status, ST_MALFORMED_TREE); break; }
+            const float4* f = reinterpret_cast<const float4*>(qn + node);
+            const float4 LX = __ldg(f + 0), LY = __ldg(f + 1), LZ = __ldg(f + 2);
+            const float4 HX = __ldg(f + 3), HY = __ldg(f + 4), HZ = __ldg(f + 5);
+            const int4 R = __ldg(reinterpret_cast<const int4*>(f + 6));
+            const int4 A = __ldg(reinterpret_cast<const int4*>(f + 7));
+            const float lx[4] = {LX.x, LX.y, LX.z, LX.w}, ly[4] = {LY.x, LY.y, LY.z, LY.w};
+            const float lz[4] = {LZ.x, LZ.y, LZ.z, LZ.w}, hx[4] = {HX.x, HX.y, HX.z, HX.w};
+            const float hy[4] = {HY.x, HY.y, HY.z, HY.w}, hz[4] = {HZ.x, HZ.y, HZ.z, HZ.w};
+            const int rr[4] = {R.x, R.y, R.z, R.w}, aa[4] = {A.x, A.y, A.z, A.w};
+            int next = -1;
+            bool bad = false, deep = false;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const int ref = rr[s];
+                if (ref == Q_EMPTY) continue;
+                if (ref >= n - 1 || (ref < 0 && ~ref >= n)) { bad = true; continue; }
+                bool hit = (qlo[0] <= hx[s]) && (qhi[0] >= lx[s]) && (qlo[1] <= hy[s]) && (qhi[1] >= ly[s]) &&
+                           (qlo[2] <= hz[s]) && (qhi[2] >= lz[s]);
+                const int rightmost = ref < 0 ? ~ref : aa[s];
+                if (p >= rightmost) hit = false;
+                if (!hit) continue;
+                if (ref < 0) {
+                    const int cid = aa[s];
+                    cg::coalesced_group grp = cg::coalesced_threads();
+                    int slot = 0;
+                    if (grp.thread_rank() == 0) slot = atomicAdd(&hdr->cand_count, (int)grp.size());
+                    slot = grp.shfl(slot, 0) + grp.thread_rank();
+                    if (slot < cand_cap) cand[slot] = make_int2(po + min(qid, cid), po + max(qid, cid));
+                    else atomicOr(&hdr->status, ST_CAND_OVERFLOW);
+                } else if (next < 0) {
+                    next = ref;
+                } else if (sp < STACK_DEPTH) {
+                    stack[sp++][tid] = ref;
+                } else {
+                    deep = true;
+                }
+            }
+            if (bad || deep) {
+                atomicOr(&hdr->status, bad ? ST_MALFORMED_TREE : ST_STACK_OVERFLOW);
+                break;
+            }
+            if (next >= 0) {
+                node = next;
+            } else {
+                if (sp == 0) break;
+                node = stack[--sp][tid];
+            }
         }
     }
 }

@@ -301,14 +301,12 @@ static __global__ void k_import_rightmost(const int* __restrict__ moff, int M, i
 __device__ __forceinline__ float nudge_down(float x) { return nextafterf(x, -INFINITY); }
 __device__ __forceinline__ float nudge_up(float x) { return nextafterf(x, INFINITY); }
 
-// Where traversal finds the leaves of mesh m (n triangles): the query's exact box and
-// triangle id, and the exact box of a hit leaf, by sorted leaf position.
-//   TensorLeaves: the reference's exported tensors; mesh m's rows start at 2 voff[m] - m.
-//   SceneLeaves: resident arrays indexed by data slot poff[m] + position.
+// Where traversal finds the leaves of mesh m (n triangles) in the reference's exported
+// tensors (mesh m's rows start at 2 voff[m] - m): the query's exact box and triangle id, and
+// the exact box of a hit leaf, by sorted leaf position.
 template <class T> struct TensorLeaves {
     const T* bboxes;
     const long long* tree;
-    static constexpr bool kSlotQuery = false;
     __device__ __forceinline__ long long row(int m, int vo, int n, int pos) const {
         return 2LL * vo - m + (n - 1) + pos;
     }
@@ -319,34 +317,8 @@ template <class T> struct TensorLeaves {
         return tree[row(m, vo, n, pos) * 4 + 3];
     }
 };
-template <class T> struct SceneLeaves {
-    const TNode* nodes;     // the query box of a leaf is its fp32 box in its parent's node
-    const int* lparent;     // (parent << 1) | side per leaf slot
-    const int* leaf_tri;    // mesh-local triangle id per leaf slot
-    static constexpr bool kSlotQuery = true;
-    // fp32 box of leaf pos (rounded outward by the refit); false for a bad parent code
-    __device__ __forceinline__ bool query_f32(int po, int n, int pos, float lo[3], float hi[3]) const {
-        int code = __ldg(lparent + po + pos);
-        int par = code >> 1;
-        if (code < 0 || par >= n - 1) return false;
-        const float4* f = reinterpret_cast<const float4*>(nodes + po + par);
-        float4 A = __ldg(f + 0), B = __ldg(f + 1), C = __ldg(f + 2);
-        if ((code & 1) == 0) {
-            lo[0] = A.x; lo[1] = A.y; lo[2] = A.z; hi[0] = A.w; hi[1] = B.x; hi[2] = B.y;
-        } else {
-            lo[0] = B.z; lo[1] = B.w; lo[2] = C.x; hi[0] = C.y; hi[1] = C.z; hi[2] = C.w;
-        }
-        return true;
-    }
-    __device__ __forceinline__ long long id(int m, int vo, int po, int n, int pos) const {
-        return __ldg(leaf_tri + po + pos);
-    }
-};
 
-// RECHECK = false leaves out the exact leaf box test: the candidate set is then the fp32
-// superset, for callers whose narrow phase re-tests every pair exactly (the continuous
-// sub-box tests reject any pair whose swept boxes do not overlap).
-template <class T, bool MASKED, bool EXACT_F32, class Leaves, bool RECHECK = true>
+template <class T, bool MASKED, bool EXACT_F32, class Leaves>
 __global__ void __launch_bounds__(TRAV_THREADS)
 k_traverse(const TNode* __restrict__ nodes, Leaves leaves, Forest F, const uint8_t* __restrict__ mask, T th,
            int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const int* __restrict__ mflags) {
@@ -370,17 +342,9 @@ k_traverse(const TNode* __restrict__ nodes, Leaves leaves, Forest F, const uint8
         }
         int qid = (int)qid64;
         // conservative fp32 query box: threshold folded in, rounded outward, nudged one more ulp
-        // (resident trees: the refit's outward-rounded fp32 box, for threshold 0)
         float qlo[3], qhi[3];
-        Box<T> q;
-        if constexpr (Leaves::kSlotQuery) {
-            static_assert(!(RECHECK && !EXACT_F32), "the exact leaf test needs exact leaf boxes");
-            if (!leaves.query_f32(po, n, p, qlo, qhi)) {
-                atomicOr(&hdr->status, ST_MALFORMED_TREE);
-                continue;
-            }
-        } else {
-            q = leaves.box(m, vo, po, n, p);
+        Box<T> q = leaves.box(m, vo, po, n, p);
+        {
             T lo[3] = {q.lo.x, q.lo.y, q.lo.z}, hi[3] = {q.hi.x, q.hi.y, q.hi.z};
             for (int c = 0; c < 3; ++c) {
                 if (EXACT_F32) {
@@ -423,8 +387,7 @@ k_traverse(const TNode* __restrict__ nodes, Leaves leaves, Forest F, const uint8
                     int cpos = ~ref;
                     int cid = s ? D.w : D.z;
                     if (MASKED && mask[po + cid] && !(qid < cid)) hit = false;
-                    if constexpr (!Leaves::kSlotQuery)
-                        if (RECHECK && hit && !EXACT_F32) hit = overlap(q, leaves.box(m, vo, po, n, cpos), th);
+                    if (hit && !EXACT_F32) hit = overlap(q, leaves.box(m, vo, po, n, cpos), th);
                     if (hit) {
                         cg::coalesced_group grp = cg::coalesced_threads();
                         int slot = 0;
