@@ -256,27 +256,38 @@ __device__ __forceinline__ uint32_t ccd_pair_mask(const T* __restrict__ x0, cons
     const T* a1 = x1 + i * 9;
     const T* b0 = x0 + j * 9;
     const T* b1 = x1 + j * 9;
-    uint32_t m = 0x7fffu;
+    // shared vertices first (start positions only): most rejected pairs are mesh neighbours
     uint32_t eq = 0x1ffu;       // vertex pairs (ia, jb) equal on every axis so far: bit 3 ia + jb
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
-        T av[3], alo[3], ahi[3], bv[3], blo[3], bhi[3];
+        T av[3], bv[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             av[c] = __ldg(a0 + 3 * c + ax);
-            T ae = av[c] + (__ldg(a1 + 3 * c + ax) - av[c]);
-            alo[c] = fmn(av[c], ae);
-            ahi[c] = fmx(av[c], ae);
             bv[c] = __ldg(b0 + 3 * c + ax);
-            T be = bv[c] + (__ldg(b1 + 3 * c + ax) - bv[c]);
-            blo[c] = fmn(bv[c], be);
-            bhi[c] = fmx(bv[c], be);
         }
 #pragma unroll
         for (int ia = 0; ia < 3; ++ia)
 #pragma unroll
             for (int jb = 0; jb < 3; ++jb)
                 if (!(av[ia] == bv[jb])) eq &= ~(1u << (3 * ia + jb));
+    }
+    if (eq) return 0u;
+    uint32_t m = 0x7fffu;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        T alo[3], ahi[3], blo[3], bhi[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            T av = __ldg(a0 + 3 * c + ax);
+            T ae = av + (__ldg(a1 + 3 * c + ax) - av);
+            alo[c] = fmn(av, ae);
+            ahi[c] = fmx(av, ae);
+            T bv = __ldg(b0 + 3 * c + ax);
+            T be = bv + (__ldg(b1 + 3 * c + ax) - bv);
+            blo[c] = fmn(bv, be);
+            bhi[c] = fmx(bv, be);
+        }
         // edges 01, 02, 12 and the face
         const T ealo[3] = {fmn(alo[0], alo[1]), fmn(alo[0], alo[2]), fmn(alo[1], alo[2])};
         const T eahi[3] = {fmx(ahi[0], ahi[1]), fmx(ahi[0], ahi[2]), fmx(ahi[1], ahi[2])};
@@ -297,7 +308,7 @@ __device__ __forceinline__ uint32_t ccd_pair_mask(const T* __restrict__ x0, cons
         }
         m &= ma;
     }
-    return eq ? 0u : m;
+    return m;
 }
 
 // The same table packed into constants, so a runtime type k selects points without
