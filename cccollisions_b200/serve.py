@@ -48,6 +48,7 @@ class Request:
     verts1_out: np.ndarray | None = None
     _sid: int = field(default=-1, repr=False)
     _pinned: tuple = field(default=(), repr=False)
+    _result: object = field(default=None, repr=False)    # pinned host buffer for verts1
 
     @property
     def F(self) -> int:
@@ -103,6 +104,8 @@ class Server:
         np_dt = np.float32 if self.dtype == torch.float32 else np.float64
         t = lambda a, dt=np_dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).pin_memory()
         r._pinned = (t(r.verts0), t(r.verts1), t(r.vel), t(r.faces, np.int32), t(r.masses))
+        # page-locking memory is slow, so the result buffer is set up with the inputs
+        r._result = torch.empty((r.V, 3), dtype=self.dtype).pin_memory()
 
     def run(self, requests: list[Request], realtime: bool = True) -> dict:
         """Serve the requests (arrival times in seconds from now when realtime, else all at
@@ -151,13 +154,13 @@ class Server:
                         for sid, it, conv in done:
                             r = active.pop(sid)
                             r.iterations, r.converged = it, conv
-                            host = torch.empty((r.V, 3), dtype=self.dtype).pin_memory()
+                            host = r._result
                             host.copy_(eng.view(sid)["verts1"], non_blocking=True)
                             outs.append((r, host))
                         self.compute.synchronize()
                         t = now()
                         for r, host in outs:
-                            r.verts1_out = host.numpy()
+                            r.verts1_out = host.numpy().copy()
                             r.finished = t
                             eng.remove_mesh(r._sid)
                 changed = bool(done)
