@@ -177,6 +177,7 @@ def run_ours(args, rank, world, dev):
     import cccollisions_b200 as C
     from cccollisions_b200 import _native as N, api
     from cccollisions_b200.engine import Engine
+    from cccollisions_b200.multi import reduce_max
 
     meshes = batched_meshes(args.meshes)
     Fs = [x0.shape[0] for x0, _ in meshes]
@@ -229,11 +230,7 @@ def run_ours(args, rank, world, dev):
             eng.ccd()
         kern = N.timing_end()
         stream.synchronize()
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = reduce_max(sum(step_ms), dev)          # the slowest replica
     ms_per_step = total_ms / args.steps
     value = world * total * args.steps / (total_ms / 1e3)
     batched_rows = {sid: _ms(*[x.cpu().numpy() for x in eng.collisions(sid, int(n))]) for sid, n in
@@ -261,11 +258,7 @@ def run_ours(args, rank, world, dev):
             stream.synchronize()
             if i >= warm:
                 e2e.append((time.perf_counter() - t0) * 1e3)
-    e2e_ms = statistics.mean(e2e)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = reduce_max(statistics.mean(e2e), dev)
     h2d = sum(x0.nbytes + x1.nbytes for x0, x1 in meshes)
     d2h = sum(n * 32 for n in nrow) + 4 * len(sids) * 4
 
