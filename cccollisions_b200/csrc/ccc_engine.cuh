@@ -7,11 +7,12 @@
 // Per mesh, the tree is a Karras radix tree over 30-bit Morton codes of the triangles'
 // swept centroids, normalised by the mesh's own centroid bounds, sorted by a stable LSD
 // radix sort (keys: mesh index above the code, so one sort orders every mesh at once).
-// Topology is built once; every step only refits the boxes, bottom-up, straight into the
-// traversal nodes (TNode, fp32 rounded outward); a leaf's query box is its box in its
-// parent's node.  The candidate pairs are therefore a superset of the pairs whose
-// T-precision swept boxes overlap; the continuous narrow phase re-tests every pair's swept
-// sub-boxes exactly, so its output is that of the reference's exact candidate set.
+// Topology is built once (the binary tree, then four-wide traversal nodes, QNode, over it);
+// every step only refits the boxes, bottom-up, straight into the QNode slots (fp32 rounded
+// outward); a leaf's query box is its own slot box.  The candidate pairs are therefore a
+// superset of the pairs whose T-precision swept boxes overlap; the continuous narrow phase
+// re-tests every pair's swept sub-boxes exactly, so its output is that of the reference's
+// exact candidate set.
 //
 // The impulse loop adds a vertex arena: faces map triangle corners to vertices, contacts
 // add their impulses to per-vertex fixed-point accumulators (integer atomics, so the sums

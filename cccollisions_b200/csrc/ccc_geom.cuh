@@ -248,8 +248,9 @@ template <class T> __device__ __forceinline__ uint32_t ccd_subbox_mask(const MTr
 // coordinates; intervals that overlap), so the per-axis results are ANDed.  Same boxes and
 // comparisons as share_vertex + ccd_subbox_mask (v and v + dv with dv = x1 - x0, min / max
 // merges, inclusive bounds), with a third of the live values.  Returns 0 when the
-// triangles share a vertex, else the mask of sub-tests whose swept boxes overlap.
-template <class T>
+// triangles share a vertex, else the mask of sub-tests whose swept boxes overlap
+// (REJECT_RIGID: 0 as well for a pair whose sub-tests can have no root, see the end).
+template <class T, bool REJECT_RIGID = true>
 __device__ __forceinline__ uint32_t ccd_pair_mask(const T* __restrict__ x0, const T* __restrict__ x1, long long i,
                                                   long long j) {
     const T* a0 = x0 + i * 9;
@@ -274,20 +275,32 @@ __device__ __forceinline__ uint32_t ccd_pair_mask(const T* __restrict__ x0, cons
     }
     if (eq) return 0u;
     uint32_t m = 0x7fffu;
+    bool rigid = true;          // every vertex moves by the same displacement (on all axes so far)
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
-        T alo[3], ahi[3], blo[3], bhi[3];
+        T alo[3], ahi[3], blo[3], bhi[3], dv[6];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             T av = __ldg(a0 + 3 * c + ax);
-            T ae = av + (__ldg(a1 + 3 * c + ax) - av);
+            dv[c] = __ldg(a1 + 3 * c + ax) - av;
+            T ae = av + dv[c];
             alo[c] = fmn(av, ae);
             ahi[c] = fmx(av, ae);
             T bv = __ldg(b0 + 3 * c + ax);
-            T be = bv + (__ldg(b1 + 3 * c + ax) - bv);
+            dv[3 + c] = __ldg(b1 + 3 * c + ax) - bv;
+            T be = bv + dv[3 + c];
             blo[c] = fmn(bv, be);
             bhi[c] = fmx(bv, be);
         }
+        // finite displacement, and start positions below half the largest finite value so that
+        // every difference of two of them is finite too
+        const T half_max = sizeof(T) == 4 ? T(1.7e38) : T(8.9e307);
+        rigid = rigid && fabs(dv[0]) <= half_max;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            rigid = rigid && fabs(__ldg(a0 + 3 * c + ax)) <= half_max && fabs(__ldg(b0 + 3 * c + ax)) <= half_max;
+#pragma unroll
+        for (int c = 1; c < 6; ++c) rigid = rigid && dv[c] == dv[0];
         // edges 01, 02, 12 and the face
         const T ealo[3] = {fmn(alo[0], alo[1]), fmn(alo[0], alo[2]), fmn(alo[1], alo[2])};
         const T eahi[3] = {fmx(ahi[0], ahi[1]), fmx(ahi[0], ahi[2]), fmx(ahi[1], ahi[2])};
@@ -308,7 +321,13 @@ __device__ __forceinline__ uint32_t ccd_pair_mask(const T* __restrict__ x0, cons
         }
         m &= ma;
     }
-    return m;
+    // A pair whose six vertices all move by the same finite displacement (a static or rigidly
+    // translating piece), with finite position differences, has in every sub-test
+    // displacement differences of exactly zero: the t^3 and t^2 coefficients are exactly 0
+    // (every term has such a factor and finite other factors), and the reference drops the
+    // root of that linear case (collisions_continuous.cu:531-535), so no sub-test of the pair
+    // can give a row or a contact.
+    return REJECT_RIGID && rigid ? 0u : m;
 }
 
 // The same table packed into constants, so a runtime type k selects points without

@@ -573,7 +573,7 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
             int2 pr = make_int2(0, 0);
             if (c < n) {
                 pr = cand[c];
-                bits = ccd_pair_mask(x0, x1, pr.x, pr.y);
+                bits = ccd_pair_mask<T, MODE != CCD_MINCOL>(x0, x1, pr.x, pr.y);
             }
             if (MODE == CCD_MINCOL) {
                 while (bits) {

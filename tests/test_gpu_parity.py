@@ -185,6 +185,33 @@ def test_ccd_cloth_sphere_full_size(cuda, oracle):
     _assert_same_rows_times(r[:n], t[:n, 0], er, et)
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_ccd_rigid_pieces(cuda, oracle, dtype):
+    """Triangles that stand still or translate rigidly (all six vertices of a pair with the
+    same displacement) beside deforming ones: the pairs inside a rigid piece give nothing,
+    the pairs across pieces give the oracle's rows."""
+    import cccollisions_b200 as C
+    x0, x1, _ = random_mesh_soup(24, nx=16, ny=14, dtype=dtype)
+    F = x0.shape[0]
+    x1 = x1.copy()
+    x1[: F // 3] = x0[: F // 3]                                   # static piece
+    x1[F // 3: 2 * F // 3] = x0[F // 3: 2 * F // 3] + dtype(0.125)  # translating piece
+    bb, tr = C.bvh_motion(_t(x0[None], cuda), _t(x1[None], cuda))
+    # room for every candidate and row (the pieces overlap after the fold: up to 24 rows a triangle)
+    rows, times = C.find_collisions_continuous(bb, tr, _t(x0[None], cuda), _t(x1[None], cuda), 128, 64)
+    r = rows[0].cpu().numpy()
+    n = _valid_prefix(r)
+    er, et = oracle.ccd(bb[0].cpu().numpy(), tr[0].cpu().numpy(), x0, x1)
+    assert len(er) > 0
+    _assert_same_rows_times(r[:n], times[0].cpu().numpy()[:n, 0], er, et)
+    # the box-only candidate rows still list the rigid pairs' sub-tests
+    mrows = C.find_mincol_cand(bb, tr, _t(x0[None], cuda), _t(x1[None], cuda), 128)
+    mr = mrows[0].cpu().numpy()
+    nm = _valid_prefix(mr)
+    emr = oracle.mincol_cand(bb[0].cpu().numpy(), tr[0].cpu().numpy(), x0, x1)
+    assert _rows_multiset(mr[:nm]) == _rows_multiset(emr)
+
+
 def test_ccd_partial(cuda, oracle):
     import cccollisions_b200 as C
     x0, x1, _ = random_mesh_soup(23, nx=14, ny=12)
