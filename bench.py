@@ -414,6 +414,8 @@ def run_served(args, dev):
             "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "makespan_s": st["makespan_s"],
             "request_triangles": st["triangles"], "ticks": st["ticks"], "mean_iterations": st["mean_iterations"],
             "converged_fraction": st["converged"], "budget_gb": 40,
+            "policy": f"FIFO admission, at most {srv.max_active_triangles} active triangles (a request alone is "
+                      "always admitted)",
             "request": "impulse loop (max 50 iterations) on an impulse-workload mesh of log-uniform 2e3..2e5 "
                        "triangles, fp64",
             "same_set": {"requests": len(sample), "triangles": ptris,

@@ -7,14 +7,19 @@ device-memory budget and works in ticks:
 
 1. one loop iteration for every active request (one CUDA graph replay);
 2. while the GPU runs it, requests that have arrived are admitted in arrival order as long
-   as their slots fit in the block (a request that does not fit waits, and so do the ones
-   behind it), and their inputs are copied to the device on a second stream;
+   as their slots fit in the block and the active triangles stay within
+   ``max_active_triangles`` (a request that does not fit waits, and so do the ones behind
+   it; a request alone is always admitted), and their inputs are copied to the device on a
+   second stream;
 3. the tick's per-mesh flags are read back; finished requests copy their vertices back to
    the host, release their slots and report their latency (arrival to result on the host);
 4. admitted requests get their trees and join the active set before the next tick.
 
 Requests that arrive while others are on the GPU therefore join at the next iteration
-boundary and share its launches.  Each mesh is processed independently and the loop's
+boundary and share its launches.  The active-triangle cap trades nothing in throughput once
+the active set fills the GPU (a few hundred thousand triangles) and bounds the time of a
+tick, so under a backlog the early requests finish early instead of all requests finishing
+together at the end of the backlog.  Each mesh is processed independently and the loop's
 impulse sums are order independent, so a request's result is bit for bit the same alone
 and in any mix.
 """
@@ -82,9 +87,11 @@ def engine_capacity(budget_bytes: int, dtype=torch.float64, mesh_capacity: int =
 
 class Server:
     def __init__(self, budget_bytes: int = 40 << 30, dtype=torch.float64, max_iter: int = 50,
-                 mesh_capacity: int = 4096, maxc: int = 16, device=None, vert_ratio: float = 0.75):
+                 mesh_capacity: int = 4096, maxc: int = 16, device=None, vert_ratio: float = 0.75,
+                 max_active_triangles: int | None = 1 << 20):
         self.dtype = dtype
         self.max_iter = int(max_iter)
+        self.max_active_triangles = max_active_triangles
         tc, vc = engine_capacity(budget_bytes, dtype, mesh_capacity, vert_ratio, maxc)
         self.engine = Engine(tri_capacity=tc, vert_capacity=vc, mesh_capacity=mesh_capacity,
                              max_candidates_per_triangle=maxc, max_collisions_per_triangle=1, dtype=dtype,
@@ -119,14 +126,19 @@ class Server:
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0
         joining: list[tuple[Request, torch.cuda.Event]] = []
+        cap = self.max_active_triangles
+        load = [0]                       # triangles of the active and joining requests
 
         def admit():
             while pending and (not realtime or pending[0].arrival <= now()):
                 r = pending[0]
+                if cap is not None and load[0] > 0 and load[0] + r.F > cap:
+                    break
                 sid = eng.try_add_mesh(r.F, r.V)
                 if sid is None:
                     break
                 pending.popleft()
+                load[0] += r.F
                 r._sid = sid
                 r.admitted = now()
                 with torch.cuda.stream(self.copy):
@@ -163,6 +175,7 @@ class Server:
                             r.verts1_out = host.numpy().copy()
                             r.finished = t
                             eng.remove_mesh(r._sid)
+                            load[0] -= r.F
                 changed = bool(done)
                 if joining:
                     ids = []

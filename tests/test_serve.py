@@ -65,3 +65,28 @@ def test_admission_waits_for_memory(cuda):
     admitted = sorted(r.admitted for r in reqs)
     assert admitted[-1] > admitted[0]                # later requests waited for slots
     srv.close()
+
+
+def test_active_triangle_cap(cuda):
+    """Under a backlog, the cap admits requests in waves: the first finish before the last
+    are admitted, a request larger than the cap still runs alone, and results are those of
+    the uncapped server."""
+    from cccollisions_b200.serve import Server
+    reqs = _requests(8, seed=7, lo=12, hi=16, spacing=0.0)
+    srv = Server(budget_bytes=256 << 20, mesh_capacity=64, max_active_triangles=None)
+    srv.run(reqs, realtime=False)
+    free_out = [r.verts1_out.copy() for r in reqs]
+    srv.close()
+    capped = _requests(8, seed=7, lo=12, hi=16, spacing=0.0)
+    cap = 2 * max(r.F for r in capped)
+    srv = Server(budget_bytes=256 << 20, mesh_capacity=64, max_active_triangles=cap)
+    srv.run(capped, realtime=False)
+    assert min(r.finished for r in capped) <= max(r.admitted for r in capped)
+    for a, b in zip(capped, free_out):
+        assert np.array_equal(a.verts1_out, b)
+    big = _requests(1, seed=8, lo=20, hi=21)[0]
+    small_cap = Server(budget_bytes=256 << 20, mesh_capacity=64, max_active_triangles=big.F // 2)
+    small_cap.run([big], realtime=False)
+    assert big.verts1_out is not None
+    small_cap.close()
+    srv.close()
