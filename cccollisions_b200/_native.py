@@ -46,6 +46,9 @@ SIGNATURES = {
     "ccc_find_collisions_continuous": (_I, [_I, _P, _P, _P, _P, _P, _I64, _I64, _I64, _I64, _P, _P, _P, _I64, _P]),
     "ccc_find_mincol_cand": (_I, [_I, _P, _P, _P, _P, _I64, _I64, _I64, _P, _P, _I64, _P]),
     "ccc_find_proximity": (_I, [_I, _P, _P, _P, _I64, _I64, _D, _I64, _P, _P, _I64, _P]),
+    "ccc_find_triangle_edge_collisions": (_I, [_I, _P, _P, _P, _I64, _I64, _I64, _P, _P, _P, _I64, _P]),
+    "ccc_find_triangle_edge_candidates": (_I, [_I, _P, _P, _P, _I64, _I64, _I64, _P, _P, _I64, _P]),
+    "ccc_find_triangle_edge_candidates2": (_I, [_I, _P, _P, _P, _I64, _I64, _I64, _P, _P, _P, _I64, _P]),
     "ccc_compute_impulses": (_I, [_I, _P, _P, _P, _P, _P, _P, _I64, _I64, _I64, _I64, _P, _P, _P, _P, _I64, _P]),
     "ccc_static_scratch_bytes": (_I64, []),
     "ccc_find_collisions_continuous_static": (_I, [_I, _P, _P, _P, _P, _P, _I64, _I64, _I64, _I64, _P, _P, _P]),

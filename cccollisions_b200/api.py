@@ -266,14 +266,57 @@ def compute_impulses_from_collisions(collisions, roots, triangles, triangles_nex
     return [dv, dx, cnt]
 
 
-def _out_of_scope(name):
-    def f(*args, **kwargs):
-        raise NotImplementedError(
-            f"{name} (ContourCraft triangle-edge contour helper) is not part of this engine's collision path")
-    f.__name__ = name
-    return f
+def _triangle_edge(bboxes, tree, triangles):
+    for t, nme in ((bboxes, "bboxes"), (tree, "tree"), (triangles, "triangles")):
+        _check_input(t, nme)
+    return bboxes.size(0), _num_tris_from_bboxes(bboxes), bboxes.device
 
 
-find_triangle_edge_collisions = _out_of_scope("find_triangle_edge_collisions")
-find_triangle_edge_candidates = _out_of_scope("find_triangle_edge_candidates")
-find_triangle_edge_candidates2 = _out_of_scope("find_triangle_edge_candidates2")
+def find_triangle_edge_collisions(bboxes, tree, triangles, threshold=0., max_collisions=16):
+    """Edges crossing triangles of intersecting pairs (cccollisions.cpp:151-173):
+    [(B, F*mc, 4) int64 (i, j, cid, flag), (B, F*mc, 1) edge coefficients].
+
+    ``threshold`` is accepted and unused, as in the reference (its queries use 0)."""
+    B, F, dev = _triangle_edge(bboxes, tree, triangles)
+    rows = -1 * torch.ones((B, F * max_collisions, 4), dtype=torch.int64, device=dev)
+    coefs = -1 * torch.ones((B, F * max_collisions, 1), dtype=bboxes.dtype, device=dev)
+    with _with_device(bboxes):
+        ws = _workspace(N.OP_FIND_COLLISIONS, B, F, max_collisions, dev)
+        rc = N.lib().ccc_find_triangle_edge_collisions(_dtype_code(bboxes), _ptr(bboxes), _ptr(tree), _ptr(triangles),
+                                                       B, F, max_collisions, _ptr(rows), _ptr(coefs), _ptr(ws),
+                                                       ws.numel(), _stream(dev))
+        N.check(rc, "find_triangle_edge_collisions")
+        _report(ws, dev, B, "find_triangle_edge_collisions")
+    return [rows, coefs]
+
+
+def find_triangle_edge_candidates(bboxes, tree, triangles, threshold=0., max_collisions=16):
+    """Edge / face sub-tests of the pairs sharing at most one vertex (cccollisions.cpp:176-194):
+    (B, F*mc, 4) int64 (i, j, cid, flag).  ``threshold`` is unused, as in the reference."""
+    B, F, dev = _triangle_edge(bboxes, tree, triangles)
+    rows = -1 * torch.ones((B, F * max_collisions, 4), dtype=torch.int64, device=dev)
+    with _with_device(bboxes):
+        ws = _workspace(N.OP_FIND_COLLISIONS, B, F, max_collisions, dev)
+        rc = N.lib().ccc_find_triangle_edge_candidates(_dtype_code(bboxes), _ptr(bboxes), _ptr(tree), _ptr(triangles),
+                                                       B, F, max_collisions, _ptr(rows), _ptr(ws), ws.numel(),
+                                                       _stream(dev))
+        N.check(rc, "find_triangle_edge_candidates")
+        _report(ws, dev, B, "find_triangle_edge_candidates")
+    return rows
+
+
+def find_triangle_edge_candidates2(bboxes, tree, triangles, threshold=0., max_collisions=16):
+    """The pairs of find_triangle_edge_candidates with their sub-test bit masks
+    (cccollisions.cpp:197-218): [(B, F*mc, 2) int64 pairs, (B, F*mc, 2) int32 masks].
+    ``threshold`` is unused, as in the reference."""
+    B, F, dev = _triangle_edge(bboxes, tree, triangles)
+    pairs = -1 * torch.ones((B, F * max_collisions, 2), dtype=torch.int64, device=dev)
+    masks = torch.zeros((B, F * max_collisions, 2), dtype=torch.int32, device=dev)
+    with _with_device(bboxes):
+        ws = _workspace(N.OP_FIND_COLLISIONS, B, F, max_collisions, dev)
+        rc = N.lib().ccc_find_triangle_edge_candidates2(_dtype_code(bboxes), _ptr(bboxes), _ptr(tree),
+                                                        _ptr(triangles), B, F, max_collisions, _ptr(pairs),
+                                                        _ptr(masks), _ptr(ws), ws.numel(), _stream(dev))
+        N.check(rc, "find_triangle_edge_candidates2")
+        _report(ws, dev, B, "find_triangle_edge_candidates2")
+    return [pairs, masks]

@@ -218,6 +218,45 @@ int static_impl(const void* bboxes, const int64_t* tree, const void* tri, int64_
     return CCC_OK;
 }
 
+template <class T, int OP>
+int te_impl(const void* bboxes, const int64_t* tree, const void* tri, int64_t B, int64_t F, int64_t max_collisions,
+            int64_t* rows, void* coefs, int32_t* masks, void* ws, int64_t ws_bytes, cudaStream_t s) {
+    Prepared P;
+    int rc = prepare(ws, ws_bytes, B, F, max_collisions, true, s, P);
+    if (rc) return rc;
+    // the reference's triangle-edge queries traverse and intersect with threshold 0
+    rc = run_broad_phase<T>(bboxes, tree, nullptr, B, F, (T)0, is_f32<T>(), P, s);
+    if (rc) return rc;
+    if (OP == TE_COLLISIONS) {
+        CCC_WITH_LIB(CCC_LAUNCH("k_te_narrow", s, k_te_narrow<T, OP, LIBV><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
+            P.cand, (int)P.L.cand_cap, P.hdr, (const T*)tri, P.forest, (long long*)rows, (T*)coefs, (int*)masks,
+            (int)max_collisions, P.mesh_cnt)));
+    } else {
+        CCC_LAUNCH("k_te_narrow", s, k_te_narrow<T, OP, LIB_PORTABLE><<<narrow_grid(), NARROW_THREADS, 0, s>>>(
+            P.cand, (int)P.L.cand_cap, P.hdr, (const T*)tri, P.forest, (long long*)rows, (T*)coefs, (int*)masks,
+            (int)max_collisions, P.mesh_cnt));
+    }
+    CCC_LAUNCH_CHECK();
+    return CCC_OK;
+}
+
+template <int OP>
+int te_entry(int dtype, const void* bboxes, const int64_t* tree, const void* triangles, int64_t B, int64_t F,
+             int64_t max_collisions, int64_t* rows, void* coefs, int32_t* masks, void* ws, int64_t ws_bytes,
+             void* stream) {
+    int rc = check_common(dtype, B, F);
+    if (rc) return rc;
+    if (!bboxes || !tree || !triangles || !rows || max_collisions < 1) return CCC_ERR_INVALID_ARG;
+    if (OP == TE_COLLISIONS && !coefs) return CCC_ERR_INVALID_ARG;
+    if (OP == TE_CANDIDATES2 && !masks) return CCC_ERR_INVALID_ARG;
+    if (B * F * max_collisions >= ((int64_t)1 << 31)) return CCC_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    return dtype == 0 ? te_impl<float, OP>(bboxes, tree, triangles, B, F, max_collisions, rows, coefs, masks, ws,
+                                           ws_bytes, s)
+                      : te_impl<double, OP>(bboxes, tree, triangles, B, F, max_collisions, rows, coefs, masks, ws,
+                                            ws_bytes, s);
+}
+
 template <class T>
 int ccd_impl(const void* bboxes, const int64_t* tree, const void* x0, const void* x1, const uint8_t* mask, int64_t B,
              int64_t F, int64_t maxc, int64_t maxcol, int64_t* rows, void* times, void* ws, int64_t ws_bytes,
@@ -432,6 +471,27 @@ int ccc_find_collisions(int dtype, const void* bboxes, const int64_t* tree, cons
     cudaStream_t s = (cudaStream_t)stream;
     return dtype == 0 ? static_impl<float>(bboxes, tree, triangles, B, F, threshold, max_collisions, out, ws, ws_bytes, s)
                       : static_impl<double>(bboxes, tree, triangles, B, F, threshold, max_collisions, out, ws, ws_bytes, s);
+}
+
+int ccc_find_triangle_edge_collisions(int dtype, const void* bboxes, const int64_t* tree, const void* triangles,
+                                      int64_t B, int64_t F, int64_t max_collisions, int64_t* out_rows,
+                                      void* out_coefs, void* ws, int64_t ws_bytes, void* stream) {
+    return te_entry<TE_COLLISIONS>(dtype, bboxes, tree, triangles, B, F, max_collisions, out_rows, out_coefs, nullptr,
+                                   ws, ws_bytes, stream);
+}
+
+int ccc_find_triangle_edge_candidates(int dtype, const void* bboxes, const int64_t* tree, const void* triangles,
+                                      int64_t B, int64_t F, int64_t max_collisions, int64_t* out_rows, void* ws,
+                                      int64_t ws_bytes, void* stream) {
+    return te_entry<TE_CANDIDATES>(dtype, bboxes, tree, triangles, B, F, max_collisions, out_rows, nullptr, nullptr,
+                                   ws, ws_bytes, stream);
+}
+
+int ccc_find_triangle_edge_candidates2(int dtype, const void* bboxes, const int64_t* tree, const void* triangles,
+                                       int64_t B, int64_t F, int64_t max_collisions, int64_t* out_pairs,
+                                       int32_t* out_binmasks, void* ws, int64_t ws_bytes, void* stream) {
+    return te_entry<TE_CANDIDATES2>(dtype, bboxes, tree, triangles, B, F, max_collisions, out_pairs, nullptr,
+                                    out_binmasks, ws, ws_bytes, stream);
 }
 
 int ccc_find_collisions_continuous(int dtype, const void* bboxes, const int64_t* tree, const void* triangles,

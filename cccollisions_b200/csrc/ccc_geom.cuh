@@ -25,6 +25,7 @@ __device__ __forceinline__ float fmaT(float a, float b, float c) { return __fmaf
 __device__ __forceinline__ double fmaT(double a, double b, double c) { return __fma_rn(a, b, c); }
 // a.x*b.x + a.y*b.y + a.z*b.z  ->  fma(a.z, b.z, fma(a.x, b.x, a.y*b.y))
 template <class T> __device__ __forceinline__ T dot(V3<T> a, V3<T> b) { return fmaT(a.z, b.z, fmaT(a.x, b.x, a.y * b.y)); }
+template <class T> __device__ __forceinline__ T dot_zyx(V3<T> a, V3<T> b) { return fmaT(a.z, b.z, fmaT(a.y, b.y, a.x * b.x)); }
 // a.y*b.z - a.z*b.y  ->  fma(a.y, b.z, -(a.z*b.y)), and cyclically
 template <class T> __device__ __forceinline__ V3<T> cross(V3<T> a, V3<T> b) {
     return mk<T>(fmaT(a.y, b.z, -(a.z * b.y)), fmaT(a.z, b.x, -(a.x * b.z)), fmaT(a.x, b.y, -(a.y * b.x)));
@@ -58,7 +59,7 @@ template <class T> __device__ __forceinline__ Box<T> merge(const Box<T>& a, cons
     r.hi = mk<T>(fmx(a.hi.x, b.hi.x), fmx(a.hi.y, b.hi.y), fmx(a.hi.z, b.hi.z));
     return r;
 }
-// checkOverlap (aabb.cu:190-200)
+// checkOverlap (aabb.cu:101-111)
 template <class T> __device__ __forceinline__ bool overlap(const Box<T>& a, const Box<T>& b, T th) {
     return (a.lo.x <= (b.hi.x + th)) && (a.hi.x >= (b.lo.x - th)) &&
            (a.lo.y <= (b.hi.y + th)) && (a.hi.y >= (b.lo.y - th)) &&
@@ -688,6 +689,86 @@ template <class T, int lib> __device__ __forceinline__ Contact<T> contact(const 
     ct.m0 = inv ? qv : mface;
     ct.m1 = inv ? mface : qv;
     return ct;
+}
+
+// ------------------------------------------------------------------ triangle-edge helpers
+
+// hasVertex (figures.cu:598-609): exact coordinate equality with one of the corners
+template <class T> __device__ __forceinline__ bool has_vertex(const Tri<T>& t, V3<T> p) {
+    return veq(t.v[0], p) || veq(t.v[1], p) || veq(t.v[2], p);
+}
+
+// Sub-test cid (0..5) of a candidate pair (a, b): cid < 3 takes edge cid % 3 of a against
+// face b, cid >= 3 edge cid % 3 of b against face a; edge e runs from corner e to corner
+// (e + 1) % 3 (collectTEIntersections / collectTECandidates, collisions_static.cu:465-586).
+template <class T>
+__device__ __forceinline__ void te_edge(const Tri<T>& a, const Tri<T>& b, int cid, Tri<T>& face, V3<T>& p0,
+                                        V3<T>& p1, int& e) {
+    const bool first = cid < 3;
+    e = first ? cid : cid - 3;
+    const int e1 = e == 2 ? 0 : e + 1;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) face.v[c] = first ? b.v[c] : a.v[c];
+    const Tri<T>& t1 = first ? a : b;
+    p0 = e == 0 ? t1.v[0] : (e == 1 ? t1.v[1] : t1.v[2]);
+    p1 = e1 == 0 ? t1.v[0] : (e1 == 1 ? t1.v[1] : t1.v[2]);
+}
+
+// addTECollsion (collisions_static.cu:345-462): true, with (flag, coefficient), when edge
+// p0-p1 crosses the face: flag 0 / coefficient 0 for an edge that starts at a corner of
+// the face (cid < 3 only), flag -1 / the edge parameter t of the crossing otherwise.  NaN
+// passes the range tests, as in the reference.
+template <class T, int lib>
+__device__ __forceinline__ bool te_intersect(const Tri<T>& face, V3<T> p0, V3<T> p1, int cid, int& flag, T& coef) {
+    V3<T> e1 = face.v[1] - face.v[0], e2 = face.v[2] - face.v[0];
+    bool s0 = has_vertex(face, p0), s1 = has_vertex(face, p1);
+    if (s0 || s1) {
+        if (cid > 2 || !s0) return false;
+        flag = 0;
+        coef = (T)0;
+        return true;
+    }
+    V3<T> nrm = vnormalize<lib>(cross(e1, e2));
+    V3<T> dir = p1 - p0;
+    T en = dot(dir, nrm);
+    if (en == 0) return false;
+    T d = dot(nrm, face.v[0]);
+    T t = (d - dot(nrm, p0)) / en;
+    if (t < 0 || t > 1) return false;
+    V3<T> x = axpy(p0, dir, t);
+    V3<T> ep = x - face.v[0];
+    // The reference's float build contracts the three dot products of the face's edges the
+    // other way round, fma(z, z', fma(y, y', x x')), and the two with ep as dot() does; its
+    // double build uses dot() for all five.  (Matched against the reference's rows on seeded
+    // folds, where many crossings pass exactly through a triangle edge.)
+    const bool f32 = sizeof(T) == 4;
+    T d00 = f32 ? dot_zyx(e1, e1) : dot(e1, e1), d01 = f32 ? dot_zyx(e1, e2) : dot(e1, e2),
+      d11 = f32 ? dot_zyx(e2, e2) : dot(e2, e2), d20 = dot(ep, e1), d21 = dot(ep, e2);
+    T denom = fms2(d00, d11, d01, d01);
+    if ((double)denom < 1e-15) return false;
+    T v = fms2(d11, d20, d01, d21) / denom;
+    T w = fms2(d00, d21, d01, d20) / denom;
+    T u = (T)(1.0 - (double)v - (double)w);     // `1.0 - v - w`: a double expression for float T
+    if (u < 0 || v < 0 || w < 0) return false;
+    flag = -1;
+    coef = t;
+    return true;
+}
+
+// collectTECandidates / collectTECandidates2 (collisions_static.cu:525-586, icontour.cu:11-110):
+// bit 0 = the sub-test is listed, bit 1 = listed as a loop node (the edge starts at a corner
+// of the face).  The box test compares the face's box with the box of the face's own edge e
+// (not of the tested edge), as the reference does.
+template <class T> __device__ __forceinline__ int te_candidate(const Tri<T>& face, V3<T> p0, V3<T> p1, int cid, int e) {
+    if (has_vertex(face, p0)) return cid < 3 ? 3 : 0;
+    if (has_vertex(face, p1)) return 0;
+    const int e1 = e == 2 ? 0 : e + 1;
+    V3<T> q0 = e == 0 ? face.v[0] : (e == 1 ? face.v[1] : face.v[2]);
+    V3<T> q1 = e1 == 0 ? face.v[0] : (e1 == 1 ? face.v[1] : face.v[2]);
+    Box<T> b1;
+    b1.lo = mk<T>(fmn(q0.x, q1.x), fmn(q0.y, q1.y), fmn(q0.z, q1.z));
+    b1.hi = mk<T>(fmx(q0.x, q1.x), fmx(q0.y, q1.y), fmx(q0.z, q1.z));
+    return overlap(tri_box(face), b1, (T)0) ? 1 : 0;
 }
 
 // extrapolate_impulses + extrapolate_impulses_dv (collisions_impulses.cu:609-1067): impulses of

@@ -103,7 +103,7 @@ static __global__ void k_uniform_offsets(int* nm, int* voff, int* poff, int* sid
 
 // ---------------------------------------------------------------------------------------
 // Build (reference order): leaf boxes, Karras topology, bottom-up box refit.
-// The reference's scene box is reduced from AABB() = (-MAX, +MAX) (aabb.cu:114-122,
+// The reference's scene box is reduced from AABB() = (-MAX, +MAX) (aabb.cu:25-34,
 // build_bvh.cu:243-244), which makes every Morton code 0; with all keys equal the stable
 // sort keeps the input order, so leaf position p holds triangle p and the Karras prefix
 // delta(i, j) reduces to 32 + clz(i ^ j).
@@ -463,6 +463,69 @@ k_static_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, cons
                 long long o = (long long)R.po * max_per_tri + r;
                 rows[o * 2 + 0] = pr.x - R.po;
                 rows[o * 2 + 1] = pr.y - R.po;
+            }
+        }
+    }
+}
+
+// find_triangle_edge_collisions (OP 0), _candidates (OP 1), _candidates2 (OP 2)
+// (collisions_static.cu:588-942, icontour.cu:113-281): candidate pairs that intersect
+// (separating axes, threshold 0) and share at most one vertex (none for OP 0), then the six
+// edge sub-tests of each pair.  OP 0 / 1 append a row (i, j, cid, flag) per listed sub-test
+// (OP 0 with the edge coefficient); OP 2 appends one row (i, j) per pair with its masks
+// (bit cid set in x when the sub-test is listed, in y when it is a loop node).
+enum TeOp { TE_COLLISIONS = 0, TE_CANDIDATES = 1, TE_CANDIDATES2 = 2 };
+
+template <class T, int OP, int LIB>
+__global__ void __launch_bounds__(NARROW_THREADS)
+k_te_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ tri, Forest F,
+            long long* __restrict__ rows, T* __restrict__ coefs, int* __restrict__ masks, int max_per_tri,
+            int* __restrict__ mesh_counters) {
+    const int M = forest_size(F);
+    int n = min(hdr->cand_count, cand_cap);
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        int2 pr = cand[c];
+        Tri<T> a = load_tri(tri, pr.x), b = load_tri(tri, pr.y);
+        if (!(sat(a, b, (T)0) && !(count_shared(a, b) > (OP == TE_COLLISIONS ? 0 : 1)))) continue;
+        OutRegion R = out_region(F, M, pr.x, max_per_tri);
+        int mx = 0, my = 0;
+        for (int cid = 0; cid < 6; ++cid) {
+            Tri<T> face;
+            V3<T> p0, p1;
+            int e;
+            te_edge(a, b, cid, face, p0, p1, e);
+            int flag = -1;
+            T coef = (T)-1;
+            if (OP == TE_COLLISIONS) {
+                if (!te_intersect<T, LIB>(face, p0, p1, cid, flag, coef)) continue;
+            } else {
+                int r = te_candidate(face, p0, p1, cid, e);
+                if (!r) continue;
+                if (OP == TE_CANDIDATES2) {
+                    mx |= 1 << cid;
+                    if (r & 2) my |= 1 << cid;
+                    continue;
+                }
+                flag = (r & 2) ? 0 : -1;
+            }
+            long long r = append_row(mesh_counters, F, R.m, R.cap, &hdr->status);
+            if (r >= 0) {
+                long long o = (long long)R.po * max_per_tri + r;
+                rows[o * 4 + 0] = pr.x - R.po;
+                rows[o * 4 + 1] = pr.y - R.po;
+                rows[o * 4 + 2] = cid;
+                rows[o * 4 + 3] = flag;
+                if (OP == TE_COLLISIONS) coefs[o] = coef;
+            }
+        }
+        if (OP == TE_CANDIDATES2) {
+            long long r = append_row(mesh_counters, F, R.m, R.cap, &hdr->status);
+            if (r >= 0) {
+                long long o = (long long)R.po * max_per_tri + r;
+                rows[o * 2 + 0] = pr.x - R.po;
+                rows[o * 2 + 1] = pr.y - R.po;
+                masks[o * 2 + 0] = mx;
+                masks[o * 2 + 1] = my;
             }
         }
     }

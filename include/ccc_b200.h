@@ -115,6 +115,39 @@ int ccc_find_collisions(int dtype, const void* bboxes, const int64_t* tree, cons
                         int64_t F, double threshold, int64_t max_collisions, int64_t* out, void* ws,
                         int64_t ws_bytes, void* stream);
 
+/* find_triangle_edge_collisions — replaces find_triangle_edge_collisions_from_bbox_tree
+ * (src/collisions_static.cu:588-720, kernels 345-522; binding src/cccollisions.cpp:151-173).
+ * Candidate pairs with threshold 0, kept when they intersect and share no vertex; then six
+ * edge sub-tests per pair (cid 0..2: edge (v0v1, v1v2, v2v0)[cid] of triangle i against
+ * face j; 3..5: edge cid-3 of j against face i).  out_rows (B, F*max_collisions, 4) int64
+ * (i, j, cid, flag) and out_coefs (B, F*max_collisions, 1) of dtype (edge parameter of the
+ * crossing), both pre-filled with -1; rows are packed at the front of each mesh's slice.
+ * The reference copies item b's rows to offset b*F*max_collisions*3 of the 4-wide tensor
+ * (collisions_static.cu:763) and copies 6 rows per intersecting pair even past the tensor's
+ * end; here each item has its own slice, and rows past the capacity are dropped with
+ * CCC_ST_OUT_OVERFLOW in the status word. */
+int ccc_find_triangle_edge_collisions(int dtype, const void* bboxes, const int64_t* tree, const void* triangles,
+                                      int64_t B, int64_t F, int64_t max_collisions, int64_t* out_rows,
+                                      void* out_coefs, void* ws, int64_t ws_bytes, void* stream);
+
+/* find_triangle_edge_candidates — replaces find_triangle_edge_candidates
+ * (src/collisions_static.cu:723-942, kernel 525-586; binding src/cccollisions.cpp:176-194).
+ * Pairs sharing at most one vertex; per sub-test a row (i, j, cid, 0) when the edge starts
+ * at a corner of the face (cid < 3 only), else (i, j, cid, -1) when the face's box overlaps
+ * the box of the face's own edge cid % 3.  out_rows (B, F*max_collisions, 4), pre-filled -1. */
+int ccc_find_triangle_edge_candidates(int dtype, const void* bboxes, const int64_t* tree, const void* triangles,
+                                      int64_t B, int64_t F, int64_t max_collisions, int64_t* out_rows, void* ws,
+                                      int64_t ws_bytes, void* stream);
+
+/* find_triangle_edge_candidates2 — replaces find_triangle_edge_candidates2
+ * (src/icontour.cu:113-281, kernel 11-110; binding src/cccollisions.cpp:197-218).  The
+ * pairs of find_triangle_edge_candidates, one row each: out_pairs (B, F*max_collisions, 2)
+ * int64 pre-filled with -1, out_binmasks (B, F*max_collisions, 2) int32 pre-filled with 0:
+ * bit cid of x when sub-test cid is listed, of y when it is a loop node. */
+int ccc_find_triangle_edge_candidates2(int dtype, const void* bboxes, const int64_t* tree, const void* triangles,
+                                       int64_t B, int64_t F, int64_t max_collisions, int64_t* out_pairs,
+                                       int32_t* out_binmasks, void* ws, int64_t ws_bytes, void* stream);
+
 /* find_collisions_continuous / find_collisions_continuous_partial — replaces
  * find_collisions_from_bbox_tree (CCD overload, src/collisions_continuous.cu:814-1076) and
  * find_collisions_from_bbox_tree_partial (1103-1376); bindings src/cccollisions.cpp:220-273.

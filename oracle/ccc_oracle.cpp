@@ -15,6 +15,7 @@
 //     root flattening and inside/segment filters (src/collisions_continuous.cu:14-765)
 //   * impulses (src/collisions_impulses.cu:24-1067)
 //   * proximity (src/proximity_static.cu:11-508)
+//   * triangle-edge helpers (src/collisions_static.cu:345-942, src/icontour.cu:11-281)
 //
 // Arithmetic: IEEE-754 float/double in the reference's evaluation order, term by term.
 // The reference is compiled by nvcc with its default fused multiply-add contraction, so
@@ -57,6 +58,7 @@ static inline float fmaT(float a, float b, float c) { return fmaf(a, b, c); }
 static inline double fmaT(double a, double b, double c) { return fma(a, b, c); }
 // a.x*b.x + a.y*b.y + a.z*b.z  ->  fma(a.z, b.z, fma(a.x, b.x, a.y*b.y))
 template <class T> static inline T dot(V3<T> a, V3<T> b) { return fmaT(a.z, b.z, fmaT(a.x, b.x, a.y * b.y)); }
+template <class T> static inline T dot_zyx(V3<T> a, V3<T> b) { return fmaT(a.z, b.z, fmaT(a.y, b.y, a.x * b.x)); }
 // a.y*b.z - a.z*b.y  ->  fma(a.y, b.z, -(a.z*b.y)), and cyclically
 template <class T> static inline V3<T> cross(V3<T> a, V3<T> b) {
     return mk<T>(fmaT(a.y, b.z, -(a.z * b.y)), fmaT(a.z, b.x, -(a.x * b.z)), fmaT(a.x, b.y, -(a.y * b.x)));
@@ -78,14 +80,14 @@ template <class T> static inline T fmn(T a, T b) { return (T)fmin(a, b); }
 template <class T> static inline T fmx(T a, T b) { return (T)fmax(a, b); }
 
 template <class T> struct Box { V3<T> lo, hi; };
-// AABB::operator+ (aabb.cu:140-145)
+// AABB::operator+ (aabb.cu:51-56)
 template <class T> static inline Box<T> merge(const Box<T>& a, const Box<T>& b) {
     Box<T> r;
     r.lo = mk<T>(fmn(a.lo.x, b.lo.x), fmn(a.lo.y, b.lo.y), fmn(a.lo.z, b.lo.z));
     r.hi = mk<T>(fmx(a.hi.x, b.hi.x), fmx(a.hi.y, b.hi.y), fmx(a.hi.z, b.hi.z));
     return r;
 }
-// checkOverlap (aabb.cu:190-200): inclusive, threshold widens the second box
+// checkOverlap (aabb.cu:101-111): inclusive, threshold widens the second box
 template <class T> static inline bool overlap(const Box<T>& a, const Box<T>& b, T th) {
     return (a.lo.x <= (b.hi.x + th)) && (a.hi.x >= (b.lo.x - th)) &&
            (a.lo.y <= (b.hi.y + th)) && (a.hi.y >= (b.lo.y - th)) &&
@@ -224,7 +226,7 @@ static void refit(int n, const Topo& tp, std::vector<Box<T>>& box, std::vector<i
 
 // build_bvh (build_bvh.cu:221-306, 381-449) and its motion overload (476-648).
 // spatial == 0 restates the reference literally: the scene box is reduced from the
-// initial AABB() = (-MAX, +MAX) (aabb.cu:114-122, build_bvh.cu:243), so it is unbounded,
+// initial AABB() = (-MAX, +MAX) (aabb.cu:25-34, build_bvh.cu:243), so it is unbounded,
 // every normalised centroid divides by an infinite extent, and every Morton code is 0;
 // the stable sort then keeps the input order.  spatial == 1 starts the reduction from the
 // empty box instead, giving real Morton codes (a spatially sorted tree; the pairs found
@@ -1020,6 +1022,150 @@ ORC_API int64_t orc_find_collisions(int dtype, const void* bboxes, const int64_t
                             int64_t* out, int64_t cap, int nthreads) {
     if (dtype == 0) return static_impl<float>((const float*)bboxes, tree, (const float*)tri, n, th, out, cap, nthreads);
     return static_impl<double>((const double*)bboxes, tree, (const double*)tri, n, th, out, cap, nthreads);
+}
+
+// ---------------------------------------------------------------------------------------
+// Triangle-edge helpers (collisions_static.cu:345-942, icontour.cu:11-281)
+// ---------------------------------------------------------------------------------------
+
+// hasVertex (figures.cu:598-609): exact coordinate equality with one of the corners
+template <class T> static inline bool has_vertex(const Tri<T>& t, V3<T> p) {
+    return veq(t.v[0], p) || veq(t.v[1], p) || veq(t.v[2], p);
+}
+
+// Sub-test cid (0..5) of a pair (a, b): cid < 3 takes edge cid % 3 of a against face b,
+// cid >= 3 edge cid % 3 of b against face a; edge e runs from corner e to corner (e + 1) % 3
+// (collectTEIntersections / collectTECandidates, collisions_static.cu:465-586).
+template <class T>
+static inline void te_edge(const Tri<T>& a, const Tri<T>& b, int cid, Tri<T>& face, V3<T>& p0, V3<T>& p1, int& e) {
+    const Tri<T>& t1 = cid < 3 ? a : b;
+    face = cid < 3 ? b : a;
+    e = cid % 3;
+    p0 = t1.v[e];
+    p1 = t1.v[(e + 1) % 3];
+}
+
+// addTECollsion (collisions_static.cu:345-462): 1 and (flag, coefficient) when edge p0-p1
+// crosses the face; flag 0 / coefficient 0 for an edge that starts at a corner of the face
+// (cid < 3 only), -1 / the edge parameter t of the crossing otherwise.  NaN passes the
+// range tests, as in the reference.
+template <class T>
+static inline int te_intersect(const Tri<T>& face, V3<T> p0, V3<T> p1, int cid, int& flag, T& coef) {
+    V3<T> e1 = face.v[1] - face.v[0], e2 = face.v[2] - face.v[0];
+    V3<T> nrm = vnormalize(cross(e1, e2));
+    bool s0 = has_vertex(face, p0), s1 = has_vertex(face, p1);
+    if (s0 || s1) {
+        if (cid > 2 || !s0) return 0;
+        flag = 0;
+        coef = (T)0;
+        return 1;
+    }
+    V3<T> dir = p1 - p0;
+    T en = dot(dir, nrm);
+    if (en == 0) return 0;
+    T d = dot(nrm, face.v[0]);
+    T t = (d - dot(nrm, p0)) / en;
+    if (t < 0 || t > 1) return 0;
+    V3<T> x = axpy(p0, dir, t);
+    V3<T> ep = x - face.v[0];
+    // the reference's float build contracts the dot products of the face's edges as
+    // fma(z, z', fma(y, y', x x')); its double build, and both builds for the ones with ep,
+    // as dot()
+    const bool f32 = sizeof(T) == 4;
+    T d00 = f32 ? dot_zyx(e1, e1) : dot(e1, e1), d01 = f32 ? dot_zyx(e1, e2) : dot(e1, e2),
+      d11 = f32 ? dot_zyx(e2, e2) : dot(e2, e2), d20 = dot(ep, e1), d21 = dot(ep, e2);
+    T denom = fms2(d00, d11, d01, d01);
+    if ((double)denom < 1e-15) return 0;
+    T v = fms2(d11, d20, d01, d21) / denom;
+    T w = fms2(d00, d21, d01, d20) / denom;
+    T u = (T)(1.0 - (double)v - (double)w);  // `1.0 - v - w`: a double expression for float T
+    if (u < 0 || v < 0 || w < 0) return 0;
+    flag = -1;
+    coef = t;
+    return 1;
+}
+
+// collectTECandidates / collectTECandidates2 (collisions_static.cu:525-586, icontour.cu:11-110):
+// bit 0 = the sub-test is listed, bit 1 = it is listed as a loop node (edge starting at a
+// corner of the face).  The box test compares the face's box with the box of the face's
+// own edge e (not the tested edge), as the reference does.
+template <class T> static inline int te_candidate(const Tri<T>& face, V3<T> p0, V3<T> p1, int cid, int e) {
+    if (has_vertex(face, p0)) return cid < 3 ? 3 : 0;
+    if (has_vertex(face, p1)) return 0;
+    const V3<T>& q0 = face.v[e];
+    const V3<T>& q1 = face.v[(e + 1) % 3];
+    Box<T> b1;
+    b1.lo = mk<T>(fmn(q0.x, q1.x), fmn(q0.y, q1.y), fmn(q0.z, q1.z));
+    b1.hi = mk<T>(fmx(q0.x, q1.x), fmx(q0.y, q1.y), fmx(q0.z, q1.z));
+    return overlap(tri_box(face), b1, (T)0) ? 1 : 0;
+}
+
+// find_triangle_edge_collisions (op 0), _candidates (op 1), _candidates2 (op 2)
+// (collisions_static.cu:588-942, icontour.cu:113-281): candidate pairs that intersect
+// (separating axes, threshold 0) sharing at most `allow` vertices (0 for op 0, 1 otherwise),
+// then the six edge sub-tests of each.  Ops 0 / 1 write rows (i, j, cid, flag) (+ the
+// coefficient, op 0) and return the row count; op 2 writes (i, j) and (mask_x, mask_y) per
+// pair and returns the pair count.  At most `cap` rows are written.
+template <class T>
+static int64_t te_impl(const T* bboxes, const int64_t* tree, const T* tri, int n, int op, int64_t* rows, T* coefs,
+                       int32_t* masks, int64_t cap, int nthreads) {
+    Forest<T> f;
+    import_tree(bboxes, tree, n, f);
+    if (!f.ok) return -1;
+    std::vector<int64_t> pairs;
+    if (candidates(f, (T)0, nullptr, pairs, nthreads) < 0) return -1;
+    const int allow = op == 0 ? 0 : 1;
+    int64_t nc = (int64_t)pairs.size() / 2;
+    int64_t w = 0;
+    for (int64_t c = 0; c < nc; ++c) {
+        int64_t i = pairs[2 * c], j = pairs[2 * c + 1];
+        Tri<T> a = load_tri(tri, i), b = load_tri(tri, j);
+        if (!(sat(a, b, (T)0) && !(count_shared(a, b) > allow))) continue;
+        int32_t mx = 0, my = 0;
+        for (int cid = 0; cid < 6; ++cid) {
+            Tri<T> face;
+            V3<T> p0, p1;
+            int e;
+            te_edge(a, b, cid, face, p0, p1, e);
+            int flag = -1;
+            T coef = (T)-1;
+            if (op == 0) {
+                if (!te_intersect(face, p0, p1, cid, flag, coef)) continue;
+            } else {
+                int r = te_candidate(face, p0, p1, cid, e);
+                if (!r) continue;
+                flag = (r & 2) ? 0 : -1;
+                if (op == 2) {
+                    mx |= 1 << cid;
+                    if (r & 2) my |= 1 << cid;
+                    continue;
+                }
+            }
+            if (w < cap) {
+                rows[4 * w + 0] = i; rows[4 * w + 1] = j; rows[4 * w + 2] = cid; rows[4 * w + 3] = flag;
+                if (coefs) coefs[w] = coef;
+            }
+            ++w;
+        }
+        if (op == 2) {
+            if (w < cap) {
+                rows[2 * w] = i; rows[2 * w + 1] = j;
+                masks[2 * w] = mx; masks[2 * w + 1] = my;
+            }
+            ++w;
+        }
+    }
+    return w;
+}
+
+ORC_API int64_t orc_triangle_edge(int dtype, const void* bboxes, const int64_t* tree, const void* tri, int n, int op,
+                                  int64_t* rows, void* coefs, int32_t* masks, int64_t cap, int nthreads) {
+    if (op < 0 || op > 2) return -1;
+    if (dtype == 0)
+        return te_impl<float>((const float*)bboxes, tree, (const float*)tri, n, op, rows, (float*)coefs, masks, cap,
+                              nthreads);
+    return te_impl<double>((const double*)bboxes, tree, (const double*)tri, n, op, rows, (double*)coefs, masks, cap,
+                           nthreads);
 }
 
 template <class T>

@@ -88,6 +88,9 @@ def lib():
         L.orc_sat.argtypes = [ctypes.c_int, _P, _P, ctypes.c_double]
         L.orc_sat.restype = ctypes.c_int
         L.orc_num_threads.restype = ctypes.c_int
+        L.orc_triangle_edge.argtypes = [ctypes.c_int, _P, _P, _P, ctypes.c_int, ctypes.c_int, _P, _P, _P, _I64,
+                                        ctypes.c_int]
+        L.orc_triangle_edge.restype = _I64
         L.orc_impulse_loop.argtypes = [ctypes.c_int, _P, _P, _P, _P, _P, _I64, _I64, ctypes.c_int, _P, ctypes.c_int,
                                        _P]
         L.orc_impulse_loop.restype = ctypes.c_int
@@ -155,6 +158,40 @@ def find_collisions(bboxes, tree, triangles, threshold=0.0, nthreads=1):
     if cnt < 0 or cnt > cap:
         raise RuntimeError("oracle find_collisions failed")
     return out[:cnt].copy()
+
+
+def _triangle_edge(bboxes, tree, triangles, op, nthreads):
+    bb = _c(bboxes)
+    tr = _c(tree, np.int64)
+    t = _c(triangles, bb.dtype)
+    n = t.shape[0]
+    L = lib()
+    cnt = L.orc_triangle_edge(_dt(bb), _ptr(bb), _ptr(tr), _ptr(t), n, op, None, None, None, 0, nthreads)
+    if cnt < 0:
+        raise RuntimeError("oracle triangle-edge query failed (malformed tree or stack overflow)")
+    w = 2 if op == 2 else 4
+    rows = np.zeros((max(cnt, 1), w), dtype=np.int64)
+    coefs = np.zeros(max(cnt, 1), dtype=bb.dtype) if op == 0 else None
+    masks = np.zeros((max(cnt, 1), 2), dtype=np.int32) if op == 2 else None
+    cnt = L.orc_triangle_edge(_dt(bb), _ptr(bb), _ptr(tr), _ptr(t), n, op, _ptr(rows), _ptr(coefs), _ptr(masks), cnt,
+                              nthreads)
+    return rows[:cnt], (coefs[:cnt] if op == 0 else masks[:cnt] if op == 2 else None)
+
+
+def triangle_edge_collisions(bboxes, tree, triangles, nthreads=1):
+    """find_triangle_edge_collisions for one mesh: rows (N, 4) int64 (i, j, cid, flag) and
+    the edge coefficients (N,)."""
+    return _triangle_edge(bboxes, tree, triangles, 0, nthreads)
+
+
+def triangle_edge_candidates(bboxes, tree, triangles, nthreads=1):
+    """find_triangle_edge_candidates for one mesh: rows (N, 4) int64 (i, j, cid, flag)."""
+    return _triangle_edge(bboxes, tree, triangles, 1, nthreads)[0]
+
+
+def triangle_edge_candidates2(bboxes, tree, triangles, nthreads=1):
+    """find_triangle_edge_candidates2 for one mesh: pairs (N, 2) int64 and their masks (N, 2) int32."""
+    return _triangle_edge(bboxes, tree, triangles, 2, nthreads)
 
 
 def ccd(bboxes, tree, triangles, triangles_next, mask=None, nthreads=1):

@@ -146,3 +146,35 @@ def test_static_and_proximity_match_reference(cuda, oracle):
         p = p[0].cpu().numpy()
         n = int((p[:, 0] >= 0).sum())
         assert Counter(map(tuple, p[:n].tolist())) == Counter(map(tuple, d["prox_rows"].tolist()))
+
+
+TE_CASES = ["te_fold_60_float64", "te_fold_61_float32", "te_fold_70_float32", "te_fold_75_float32",
+            "te_fold_75_float64", "te_static_fold"]
+
+
+@pytest.mark.parametrize("name", TE_CASES)
+def test_triangle_edge_queries_match_reference(cuda, name):
+    """find_triangle_edge_collisions / _candidates / _candidates2 in the default mode
+    (CUDA's rsqrt in the face normal, as the reference) against the reference's own rows:
+    equal multisets, edge coefficients bit for bit.  Many crossings of these folds pass
+    exactly through a triangle edge (a barycentric coordinate of exactly 0), so the rows
+    depend on every rounding of the reference's expressions."""
+    import cccollisions_b200 as C
+    from cccollisions_b200 import _native as N
+    d = _load(name)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    Bb, Tr, X = T(d["bboxes"][None]), T(d["tree"][None]), T(d["x"][None])
+    assert N.lib().ccc_get_math_library() == N.LIB_REFERENCE
+    rows, coefs = C.find_triangle_edge_collisions(Bb, Tr, X, 0.0, 32)
+    r = rows[0].cpu().numpy()
+    n = int((r[:, 0] >= 0).sum())
+    got = Counter(zip(map(tuple, r[:n].tolist()), coefs[0, :n, 0].cpu().tolist()))
+    assert got == Counter(zip(map(tuple, d["te_rows"].tolist()), d["te_coefs"].tolist()))
+    c = C.find_triangle_edge_candidates(Bb, Tr, X, 0.0, 32)[0].cpu().numpy()
+    c = c[c[:, 0] >= 0]
+    assert Counter(map(tuple, c.tolist())) == Counter(map(tuple, d["cand_rows"].tolist()))
+    pairs, masks = C.find_triangle_edge_candidates2(Bb, Tr, X, 0.0, 32)
+    p, m = pairs[0].cpu().numpy(), masks[0].cpu().numpy()
+    k = p[:, 0] >= 0
+    assert Counter(zip(map(tuple, p[k].tolist()), map(tuple, m[k].tolist()))) == \
+        Counter(zip(map(tuple, d["cand2_pairs"].tolist()), map(tuple, d["cand2_masks"].tolist())))

@@ -77,8 +77,12 @@ def test_api_mirrors_reference_signatures():
                                                     "max_candidates_per_triangle"]
     assert [k for k, _ in sig(C.compute_impulses_from_collisions)] == ["collisions", "roots", "triangles",
                                                                       "triangles_next", "triangles_mass"]
-    with pytest.raises(NotImplementedError):
-        C.find_triangle_edge_collisions(None, None, None)
+    for f in (C.find_triangle_edge_collisions, C.find_triangle_edge_candidates, C.find_triangle_edge_candidates2):
+        p = sig(f)
+        assert [k for k, _ in p] == ["bboxes", "tree", "triangles", "threshold", "max_collisions"]
+        assert p[3][1].default == 0.0 and p[4][1].default == 16
+        with pytest.raises(RuntimeError, match="torch.Tensor"):
+            f(None, None, None)
 
 
 def test_api_rejects_cpu_tensors():

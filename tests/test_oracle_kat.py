@@ -52,7 +52,7 @@ def test_karras_identity_topology_n8(oracle):
 
 
 def test_reference_scene_box_gives_zero_codes(oracle):
-    # AABB() is (-MAX, +MAX) (aabb.cu:114-122) and seeds the scene-box reduction
+    # AABB() is (-MAX, +MAX) (aabb.cu:25-34) and seeds the scene-box reduction
     # (build_bvh.cu:243), so every normalised centroid is 0 and every code is 0
     x0, x1, _ = random_mesh_soup(3)
     _, _, codes = oracle.bvh(x0, return_codes=True)
