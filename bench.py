@@ -18,9 +18,10 @@ plain per-mesh path, with exact pair sets and p50 / p99 latency.
   log-uniform 2e3..2e5 triangles as in the impulse workload) under a 40 GB engine budget:
   throughput (request triangles over the makespan) and p50 / p99 latency (arrival to result
   on the host).
-* ``e2e`` — the batched step through the public engine API from pinned host buffers: H2D of
-  both soups of every mesh, the graph replay, the per-mesh row counts and a D2H copy of every
-  row and time.
+* ``e2e`` — the batched step through the public engine API from pinned host buffers
+  (``engine.StepPipeline``): every step's H2D of both soups of every mesh, the graph replay,
+  the rows packed on the device and one D2H copy of every row and time, with each step's
+  copies overlapping the neighbouring steps' kernels.
 * ``roofline`` — the dominant kernel (CUDA-event timing of the same step run ungraphed)
   against MEASURED_PEAKS.json; ``refit_roofline`` / ``build_roofline`` the tree kernels;
   ``fp64`` the narrow phase's arithmetic rate.
@@ -176,7 +177,7 @@ def run_ours(args, rank, world, dev):
 
     import cccollisions_b200 as C
     from cccollisions_b200 import _native as N, api
-    from cccollisions_b200.engine import Engine
+    from cccollisions_b200.engine import Engine, StepPipeline
     from cccollisions_b200.multi import reduce_max
 
     meshes = batched_meshes(args.meshes)
@@ -236,31 +237,29 @@ def run_ours(args, rank, world, dev):
     batched_rows = {sid: _ms(*[x.cpu().numpy() for x in eng.collisions(sid, int(n))]) for sid, n in
                     zip(sids, st["rows"])}
 
-    # ---------------- e2e through the engine API from pinned host memory
-    hx = [(torch.from_numpy(x0).pin_memory(), torch.from_numpy(x1).pin_memory()) for x0, x1 in meshes]
+    # ---------------- e2e through the engine API from pinned host memory: StepPipeline streams
+    # the steps, so step k's soups go up and step k-1's rows come down while step k runs;
+    # every step's copies are inside the timed region
     nrow = [int(n) for n in st["rows"]]
-    hrows = [torch.empty((n, 3), dtype=torch.int64).pin_memory() for n in nrow]
-    htimes = [torch.empty((n,), dtype=torch.float64).pin_memory() for n in nrow]
-    e2e = []
-    with torch.cuda.stream(stream):
-        for i in range(warm + args.steps):
-            flush.fill_(i & 0xFF)
-            stream.synchronize()
-            t0 = time.perf_counter()
-            for sid, (h0, h1) in zip(sids, hx):
-                eng.upload_soup(sid, h0, h1, non_blocking=True)
-            eng.replay(N.ENGINE_OP_CCD)
-            s2 = eng.state(sids)
-            for j, (sid, n) in enumerate(zip(sids, s2["rows"])):
-                r, tt = eng.collisions(sid, int(n))
-                hrows[j][:int(n)].copy_(r, non_blocking=True)
-                htimes[j][:int(n)].copy_(tt, non_blocking=True)
-            stream.synchronize()
-            if i >= warm:
-                e2e.append((time.perf_counter() - t0) * 1e3)
-    e2e_ms = reduce_max(statistics.mean(e2e), dev)
+    hx = [(torch.from_numpy(x0).pin_memory(), torch.from_numpy(x1).pin_memory()) for x0, x1 in meshes]
+    pipe = StepPipeline(eng, sids)
+    houts = [pipe.host_outputs(), pipe.host_outputs()]
+    pipe.run([hx] * warm, [houts[k % 2] for k in range(warm)])
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    e2e_totals = pipe.run([hx] * args.steps, [houts[k % 2] for k in range(args.steps)])
+    torch.cuda.synchronize(dev)
+    e2e_ms = reduce_max((time.perf_counter() - t0) * 1e3 / args.steps, dev)
+    # the streamed rows of the last step, split by mesh, are the batched step's rows
+    rows_h, times_h, meta_h = [o.numpy() for o in houts[(args.steps - 1) % 2]]
+    M = len(sids)
+    e2e_equal = all(_ms(rows_h[meta_h[m]:meta_h[m + 1]], times_h[meta_h[m]:meta_h[m + 1]]) ==
+                    batched_rows[int(meta_h[M + 1 + m])] for m in range(M))
+    e2e_equal &= all(t == sum(nrow) for t in e2e_totals)
     h2d = sum(x0.nbytes + x1.nbytes for x0, x1 in meshes)
-    d2h = sum(n * 32 for n in nrow) + 4 * len(sids) * 4
+    d2h = sum(n * 32 for n in nrow) + 4 * (2 * len(sids) + 2)
 
     # ---------------- plain per-mesh path through the reference-format API
     X = [(torch.from_numpy(x0).to(dev), torch.from_numpy(x1).to(dev)) for x0, x1 in meshes]
@@ -329,7 +328,11 @@ def run_ours(args, rank, world, dev):
             "batched_over_plain": plain_ms / ms_per_step,
             "pair_sets_equal": bool(equal),
             "e2e": {"value": world * total / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
-                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "path": "engine.StepPipeline: per step, H2D of both soups of every mesh from page-locked "
+                            "memory, graph replay, device packing of the rows, D2H of rows + times; copies of "
+                            "step k overlap the kernels of steps k-1 / k+1",
+                    "rows_equal_batched": bool(e2e_equal)},
             "roofline": {"kernel": dname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
                          "traffic": None, "alg_bytes_per_launch": narrow_bytes, "launch_ms": per_launch,

@@ -71,6 +71,7 @@ SIGNATURES = {
     "ccc_engine_replay": (_I, [_P, _I, _P]),
     "ccc_engine_autotune": (_I, [_P, _P, _P]),
     "ccc_engine_read_state": (_I, [_P, _P, _I64, _P, _P, _P, _P, _P, _P]),
+    "ccc_engine_pack_rows": (_I, [_P, _P, _P, _I64, _P, _P]),
     "ccc_engine_counters": (_I, [_P, _P, _P]),
 }
 

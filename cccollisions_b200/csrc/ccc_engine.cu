@@ -686,6 +686,30 @@ int ccc_engine_autotune(ccc_engine* e, void* stream, int32_t* choice) {
     return CCC_OK;
 }
 
+int ccc_engine_pack_rows(ccc_engine* e, int64_t* out_rows, void* out_times, int64_t capacity, int32_t* out_meta,
+                         void* stream) {
+    if (!e || !out_rows || !out_times || !out_meta || capacity < 0) return CCC_ERR_INVALID_ARG;
+    if (e->tri_cap * e->maxcol >= ((int64_t)1 << 31)) return CCC_ERR_INVALID_ARG;   // int32 offsets
+    cudaStream_t s = (cudaStream_t)stream;
+    Forest F = e->active().f;
+    CCC_LAUNCH("k_pack_offsets", s, k_pack_offsets<<<1, PACK_SCAN_THREADS, 0, s>>>(
+        F, e->at<int>(e->L.mesh_cnt), (int)e->maxcol, &e->hdr()->status, out_meta));
+    CCC_LAUNCH_CHECK();
+    if (capacity == 0) return CCC_OK;
+    int64_t work = std::min<int64_t>(capacity, e->active_tris * e->maxcol);
+    int g = (int)std::max<int64_t>(1, std::min<int64_t>(grid_for(work, 256), (int64_t)num_sms() * 8));
+    if (e->dtype)
+        CCC_LAUNCH("k_pack_rows", s, k_pack_rows<double><<<g, 256, 0, s>>>(
+            F, out_meta, e->at<long long>(e->L.rows), e->at<double>(e->L.times), (int)e->maxcol, (long long*)out_rows,
+            (double*)out_times, capacity, &e->hdr()->status));
+    else
+        CCC_LAUNCH("k_pack_rows", s, k_pack_rows<float><<<g, 256, 0, s>>>(
+            F, out_meta, e->at<long long>(e->L.rows), e->at<float>(e->L.times), (int)e->maxcol, (long long*)out_rows,
+            (float*)out_times, capacity, &e->hdr()->status));
+    CCC_LAUNCH_CHECK();
+    return CCC_OK;
+}
+
 int ccc_engine_counters(ccc_engine* e, int32_t* out, void* stream) {
     if (!e || !out) return CCC_ERR_INVALID_ARG;
     return ccc_read_counters(e->base + e->L.hdr, out, stream);

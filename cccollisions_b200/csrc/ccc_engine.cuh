@@ -830,4 +830,68 @@ static __global__ void k_zero_acc(Forest F, VertTable vt, long long* __restrict_
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// Packed copy of the active meshes' collision rows, for one device-to-host copy per step.
+// meta = [offsets (M + 1) | slot ids (M) | status word] in table order: offsets[m] = rows of
+// the active meshes before m, each mesh's count capped at its capacity F_m * maxcol.  One block.
+static constexpr int PACK_SCAN_THREADS = 1024;
+static __global__ void __launch_bounds__(PACK_SCAN_THREADS)
+k_pack_offsets(Forest F, const int* __restrict__ mesh_cnt, int maxcol, const int* status, int* __restrict__ meta) {
+    __shared__ int warp_sum[PACK_SCAN_THREADS / 32];
+    __shared__ int carry;
+    const int M = forest_size(F);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < M; base += PACK_SCAN_THREADS) {
+        const int m = base + threadIdx.x;
+        int n = 0;
+        if (m < M) {
+            int sid = __ldg(F.sid + m);
+            long long cap = (long long)(__ldg(F.voff + m + 1) - __ldg(F.voff + m)) * maxcol;
+            n = (int)min((long long)max(mesh_cnt[sid], 0), cap);
+            meta[M + 1 + m] = sid;
+        }
+        int incl = warp_inclusive_scan(n, lane);
+        if (lane == 31) warp_sum[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            int v = warp_sum[lane];
+            int sc = warp_inclusive_scan(v, lane);
+            warp_sum[lane] = sc - v;
+        }
+        __syncthreads();
+        const int c0 = carry;
+        if (m < M) meta[m] = c0 + warp_sum[warp] + incl - n;
+        __syncthreads();
+        if (threadIdx.x == PACK_SCAN_THREADS - 1) carry = c0 + warp_sum[warp] + incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        meta[M] = carry;
+        meta[2 * M + 1] = *(volatile const int*)status;
+    }
+}
+
+// rows and times of every active mesh, back to back in table order (the first `capacity`
+// rows; ST_OUT_OVERFLOW when there are more)
+template <class T>
+static __global__ void k_pack_rows(Forest F, const int* __restrict__ meta, const long long* __restrict__ rows,
+                                   const T* __restrict__ times, int maxcol, long long* __restrict__ out_rows,
+                                   T* __restrict__ out_times, long long capacity, int* status) {
+    const int M = forest_size(F);
+    const long long total = __ldg(meta + M);
+    const long long n = min(total, capacity);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && total > capacity) atomicOr(status, ST_OUT_OVERFLOW);
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
+         r += (long long)gridDim.x * blockDim.x) {
+        int m = find_mesh(meta, M, r, 0);
+        long long src = (long long)__ldg(F.poff + m) * maxcol + (r - __ldg(meta + m));
+        out_rows[r * 3 + 0] = __ldg(rows + src * 3 + 0);
+        out_rows[r * 3 + 1] = __ldg(rows + src * 3 + 1);
+        out_rows[r * 3 + 2] = __ldg(rows + src * 3 + 2);
+        out_times[r] = __ldg(times + src);
+    }
+}
+
 }  // namespace ccc

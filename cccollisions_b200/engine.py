@@ -16,6 +16,9 @@ and runs each step over all active meshes at once:
 ``capture``/``replay`` turn a step into one CUDA graph launch that follows the active set;
 ``loop_prepare``/``loop_step`` run the impulse loop on meshes given as vertices + faces.
 The block is an ordinary torch allocation, and every per-mesh array is a tensor view of it.
+
+``StepPipeline`` streams collision steps from page-locked host inputs to page-locked host
+outputs, overlapping each step's copies with the kernels of its neighbours.
 """
 from __future__ import annotations
 
@@ -200,9 +203,156 @@ class Engine:
         N.check(N.lib().ccc_engine_counters(self.handle, out, _stream(self.device)), "ccc_engine_counters")
         return {"status": int(out[0]), "candidates": int(out[1]), "subtests": int(out[2]), "roots": int(out[3])}
 
+    def pack_rows(self, out_rows: torch.Tensor, out_times: torch.Tensor, out_meta: torch.Tensor):
+        """Packs the last ccd()'s rows of every active mesh back to back on the device (no
+        synchronisation): out_rows (capacity, 3) int64, out_times (capacity,), out_meta
+        (2 M + 2,) int32 = [row offset of each mesh in slot order, total, slot ids, status]."""
+        if out_rows.dtype != torch.int64 or out_times.dtype != self.dtype or out_meta.dtype != torch.int32:
+            raise RuntimeError("pack_rows: int64 rows, engine-dtype times and int32 meta expected")
+        if not (out_rows.is_contiguous() and out_times.is_contiguous() and out_meta.is_contiguous()):
+            raise RuntimeError("pack_rows: contiguous outputs expected")
+        cap = min(out_rows.shape[0], out_times.shape[0])
+        N.check(N.lib().ccc_engine_pack_rows(self.handle, ctypes.c_void_p(out_rows.data_ptr()),
+                                             ctypes.c_void_p(out_times.data_ptr()), int(cap),
+                                             ctypes.c_void_p(out_meta.data_ptr()), _stream(self.device)),
+                "ccc_engine_pack_rows")
+
     def collisions(self, sid: int, count: int | None = None):
         """(rows (n, 3) int64, times (n,)) of the last ccd() for one mesh (views)."""
         if count is None:
             count = int(self.state([sid])["rows"][0])
         v = self.view(sid)
         return v["rows"][:count], v["times"][:count]
+
+
+def _ranges(views, key):
+    """Byte ranges of the given arrays in the engine block, adjacent ones merged."""
+    spans = sorted((v[key].data_ptr(), v[key].data_ptr() + v[key].numel() * v[key].element_size()) for v in views)
+    out = []
+    for a, b in spans:
+        if out and out[-1][1] == a:
+            out[-1][1] = b
+        else:
+            out.append([a, b])
+    return out
+
+
+class StepPipeline:
+    """Collision steps of a fixed active set, streamed from page-locked host memory to
+    page-locked host memory.
+
+    Step k's soups go up on one copy stream while step k-1 runs; step k's rows, packed on
+    the device (``Engine.pack_rows``), come down on a second copy stream while step k+1
+    runs.  The kernels of consecutive steps therefore run back to back, and a step's
+    host-device traffic costs time only where it exceeds a step's kernel time.
+
+    Device staging: one copy of the active meshes' soups and two packed-row buffers of
+    (active triangles x max_collisions_per_triangle) rows.  The engine's step must have been
+    captured (``Engine.capture(ENGINE_OP_CCD)``) for ``graph=True``; the active set and
+    trees must be those of ``sids``.
+    """
+
+    def __init__(self, engine: Engine, sids: Sequence[int], graph: bool = True):
+        self.e = engine
+        self.sids = list(sids)
+        self.graph = graph
+        dev = engine.device
+        views = [engine.view(s) for s in self.sids]
+        self.M = len(self.sids)
+        self.capacity = sum(v["F"] for v in views) * engine.maxcol
+        base = engine.block.data_ptr()
+        # device staging of the soups, laid out like the engine's slot ranges
+        self._stage, self._pairs, self._slices = {}, [], []
+        for key in ("x0", "x1"):
+            for a, b in _ranges(views, key):
+                st = torch.empty(b - a, dtype=torch.uint8, device=dev)
+                self._pairs.append((engine.block[a - base:b - base], st))
+                self._stage[(key, a)] = st
+        for v in views:
+            sl = []
+            for key in ("x0", "x1"):
+                p = v[key].data_ptr()
+                a = max(k[1] for k in self._stage if k[0] == key and k[1] <= p)
+                st = self._stage[(key, a)]
+                n = v[key].numel() * v[key].element_size()
+                sl.append(st[p - a:p - a + n].view(engine.dtype).view(v[key].shape))
+            self._slices.append(tuple(sl))
+        self._rows = [torch.empty((max(self.capacity, 1), 3), dtype=torch.int64, device=dev) for _ in range(2)]
+        self._times = [torch.empty(max(self.capacity, 1), dtype=engine.dtype, device=dev) for _ in range(2)]
+        self._meta = [torch.empty(2 * self.M + 2, dtype=torch.int32, device=dev) for _ in range(2)]
+        self.compute = torch.cuda.Stream(dev)
+        self.copy_in = torch.cuda.Stream(dev)
+        self.copy_out = torch.cuda.Stream(dev)
+
+    def host_outputs(self):
+        """Page-locked (rows, times, meta) host buffers sized for one step."""
+        return (torch.empty((max(self.capacity, 1), 3), dtype=torch.int64).pin_memory(),
+                torch.empty(max(self.capacity, 1), dtype=self.e.dtype).pin_memory(),
+                torch.empty(2 * self.M + 2, dtype=torch.int32).pin_memory())
+
+    def run(self, inputs, outputs) -> list[int]:
+        """inputs[k]: one (x0, x1) pair of page-locked host tensors per mesh (order of sids)
+        for step k; outputs[k]: (rows, times, meta) page-locked host tensors from
+        host_outputs() that receive step k's rows (the same buffers may serve several steps
+        when the caller does not need the earlier ones).  meta = [row offset of each mesh in
+        slot order, total, slot ids, status word].  Returns the row count of every step;
+        raises if a step's status word reports an error."""
+        e, K = self.e, len(inputs)
+        if len(outputs) != K:
+            raise ValueError("one output triple per step")
+        ev = lambda: torch.cuda.Event()
+        up, in_free, done, down = [ev() for _ in range(K)], [ev() for _ in range(K)], [ev() for _ in range(K)], \
+            [ev() for _ in range(K)]
+        totals, status = [0] * K, [0] * K
+
+        def upload(k):
+            with torch.cuda.stream(self.copy_in):
+                if k > 0:
+                    self.copy_in.wait_event(in_free[k - 1])
+                for (d0, d1), (h0, h1) in zip(self._slices, inputs[k]):
+                    d0.copy_(h0.view(d0.shape), non_blocking=True)
+                    d1.copy_(h1.view(d1.shape), non_blocking=True)
+                up[k].record(self.copy_in)
+
+        def download(k):
+            done[k].synchronize()
+            rows_h, times_h, meta_h = outputs[k]
+            n = min(int(meta_h[self.M]), self.capacity)
+            totals[k] = int(meta_h[self.M])
+            status[k] = int(meta_h[2 * self.M + 1])
+            with torch.cuda.stream(self.copy_out):
+                self.copy_out.wait_event(done[k])
+                if n:
+                    rows_h[:n].copy_(self._rows[k % 2][:n], non_blocking=True)
+                    times_h[:n].copy_(self._times[k % 2][:n], non_blocking=True)
+                down[k].record(self.copy_out)
+
+        self.compute.wait_stream(torch.cuda.current_stream(e.device))
+        if K:
+            upload(0)
+        for k in range(K):
+            with torch.cuda.stream(self.compute):
+                self.compute.wait_event(up[k])
+                for dst, src in self._pairs:
+                    dst.copy_(src, non_blocking=True)
+                in_free[k].record(self.compute)
+                if self.graph:
+                    e.replay(N.ENGINE_OP_CCD)
+                else:
+                    e.ccd()
+                if k >= 2:
+                    self.compute.wait_event(down[k - 2])
+                e.pack_rows(self._rows[k % 2], self._times[k % 2], self._meta[k % 2])
+                outputs[k][2].copy_(self._meta[k % 2], non_blocking=True)
+                done[k].record(self.compute)
+            if k + 1 < K:
+                upload(k + 1)
+            if k >= 1:
+                download(k - 1)
+        if K:
+            download(K - 1)
+        self.copy_out.synchronize()
+        bad = [(k, st) for k, st in enumerate(status) if st & ~N.CCC_ST_NONFINITE]
+        if bad:
+            raise RuntimeError(f"engine status {bad[0][1]:#x} in step {bad[0][0]}")
+        return totals

@@ -115,6 +115,18 @@ int ccc_engine_autotune(ccc_engine* e, void* stream, int32_t* choice);
 int ccc_engine_read_state(ccc_engine* e, const int32_t* slot_ids, int64_t n, int32_t* status, int32_t* rows,
                           int32_t* contacts, int32_t* iterations, int32_t* flags, void* stream);
 
+/* Pack the rows and times of the last ccc_engine_ccd of every active mesh back to back into
+ * out_rows (capacity x 3 int64) and out_times (capacity, of the engine's dtype), so that one
+ * device-to-host copy fetches a whole step (no counterpart in the reference, which returns
+ * one fixed-size tensor per call).  Device-only, no synchronisation.  out_meta (device,
+ * 2 * M + 2 int32 for M active meshes) receives, in the engine's table order (ascending
+ * triangle slot), the row offset of each mesh, the total at [M], the mesh slot ids at
+ * [M + 1 .. 2M] and the step's status word at [2M + 1].  Rows past capacity are dropped
+ * with CCC_ST_OUT_OVERFLOW; a capacity of the active triangles x
+ * max_collisions_per_triangle always suffices. */
+int ccc_engine_pack_rows(ccc_engine* e, int64_t* out_rows, void* out_times, int64_t capacity, int32_t* out_meta,
+                         void* stream);
+
 /* Synchronise the stream and read the work counters of the last step: status word,
  * candidate pairs, continuous sub-tests solved, roots in [0, 1] filtered. */
 int ccc_engine_counters(ccc_engine* e, int32_t* out, void* stream);
