@@ -31,8 +31,11 @@ CCC_HD ccc_dd ccc_fast_two_sum(double a, double b) {
     return r;
 }
 
-// (x0 (+ x1 when k == 2)) * y rounded to a 2-term expansion: bins of 45 bits, 4 live bins.
-CCC_HD_CALL ccc_dd ccc_certmul(double x0, double x1, int k, double y) {
+// (x0 (+ x1 when K == 2)) * y rounded to a 2-term expansion: bins of 45 bits, 4 live bins.
+// K is a template parameter so that the solver's six products a call compile to straight
+// code (the first partial product always lands at bin offset 0).
+template <int K> CCC_HD ccc_dd ccc_certmul_k(double x0, double x1, double y) {
+    const int k = K;
     const int BIN = 45;
     double b0, b1, b2, b3, b4, b5;           // bins (6 slots, the last two spill targets)
     double s0, s1, s2, s3;                   // biases of the live bins
@@ -116,9 +119,14 @@ CCC_HD_CALL ccc_dd ccc_certmul(double x0, double x1, int k, double y) {
     return r;
 }
 
+// the same with the number of terms K in {1, 2} given at run time
+CCC_HD_CALL ccc_dd ccc_certmul(double x0, double x1, int k, double y) {
+    return k > 1 ? ccc_certmul_k<2>(x0, x1, y) : ccc_certmul_k<1>(x0, x1, y);
+}
+
 // Leading terms the solver uses: x^2 (as a 2-term expansion) and x^3 = (x^2) * x.
-CCC_HD ccc_dd ccc_sq_dd(double x) { return ccc_certmul(x, 0.0, 1, x); }
+CCC_HD ccc_dd ccc_sq_dd(double x) { return ccc_certmul_k<1>(x, 0.0, x); }
 CCC_HD double ccc_cube_hi(double x) {
     ccc_dd s = ccc_sq_dd(x);
-    return ccc_certmul(s.hi, s.lo, 2, x).hi;
+    return ccc_certmul_k<2>(s.hi, s.lo, x).hi;
 }
