@@ -799,8 +799,11 @@ __device__ __forceinline__ void impulse_point(const MTet<T>& tet, int k, int pt,
                                               const ImpulseScale<T>& sc, V3<T>& imp, V3<T>& idx) {
     T mag = (k < 9) ? (pt < 2 ? sc.mag0 : sc.mag1) : (k < 12 ? (pt < 3 ? sc.mag0 : sc.mag1) : (pt < 1 ? sc.mag0 : sc.mag1));
     imp = ct.n * mag;
-    V3<T> nv = tet.dv[pt] + imp;
-    idx = (nv - tet.dv[pt]) * sc.keep;
+    // the point's displacement by value selects: a run-time index into tet would move the
+    // whole tetrahedron to local memory
+    const V3<T> d = pt == 0 ? tet.dv[0] : (pt == 1 ? tet.dv[1] : (pt == 2 ? tet.dv[2] : tet.dv[3]));
+    V3<T> nv = d + imp;
+    idx = (nv - d) * sc.keep;
 }
 
 // extrapolate_impulses + extrapolate_impulses_dv (collisions_impulses.cu:609-1067): impulses of
