@@ -124,9 +124,79 @@ CCC_HD_CALL ccc_dd ccc_certmul(double x0, double x1, int k, double y) {
     return k > 1 ? ccc_certmul_k<2>(x0, x1, y) : ccc_certmul_k<1>(x0, x1, y);
 }
 
+// ---- Short paths with the same results --------------------------------------------------
+//
+// With x, y finite and non-zero, e0 = exponent(x) + exponent(y) (frexp exponents), the bins
+// of ccc_certmul_k hold, after the un-biasing, b0 = the partial products rounded to the grid
+// 2^(e0-45), b1 = the rest rounded to the grid 2^(e0-90), b2, b3 = the remainder; each bin
+// is exact for these magnitudes as long as the bias constants are normal numbers.  Then:
+//
+//  * K = 1 (x * y = p + e exactly, p = RN(x y), e = fma(x, y, -p)): b0 + b1 = p + E with E = e
+//    rounded to the grid 2^(e0-90), so |E| <= ulp(p) / 2, and the renormalisation returns
+//    (p, e) unless |E| = ulp(p) / 2 exactly, where RN(p + E) may tie away from p.  That
+//    needs |e| within 2^(e0-91) of ulp(p) / 2.
+//  * K = 2, leading term only (V = (x0 + x1) y exactly, |x1| <= ulp(x0) / 2): b0 + b1
+//    differs from V by less than 2^(e0-88), and the leading term is RN(b0 + b1) (or, when
+//    that sum is exact, the rounded sum with the next bins), so it is RN(V) whenever V is
+//    farther than 2^(e0-88) from the midpoint of two neighbouring doubles.
+//
+// The short paths compute (p, e) and RN(V) with TwoProd and a compensated sum (error far
+// below 2^(e0-100)) and use them when the distance to the critical point exceeds 2^(e0-80)
+// and the operands are in the range where every bias constant is normal; anything else
+// (zeros, ties and near-ties, powers of two, extreme exponents, non-finite values) takes
+// the bin algorithm itself.  The CPU test suite checks both paths against each other on
+// random, short-mantissa (exact and tied products) and special operands.
+CCC_HD int ccc_bexp(double x) { return (int)((ccc_dbits(x) >> 52) & 0x7ff); }
+CCC_HD bool ccc_pow2_or_special(double x) {
+    uint64_t u = ccc_dbits(x);
+    int be = (int)((u >> 52) & 0x7ff);
+    return (u & 0x000fffffffffffffull) == 0 || be == 0 || be == 0x7ff;
+}
+
+// certifiedMul<1,1,2>(x, y)
+CCC_HD ccc_dd ccc_certmul1(double x, double y) {
+    const int bx = ccc_bexp(x), by = ccc_bexp(y);
+    const int e0 = (bx - 1022) + (by - 1022);
+    const double p = x * y;
+    const double e = ccc_fma(x, y, -p);
+    bool easy = x != 0.0 && y != 0.0 && bx != 0 && bx != 0x7ff && by != 0 && by != 0x7ff && e0 >= -700 &&
+                e0 <= 1000 && !ccc_pow2_or_special(p);
+    if (easy) {
+        const double half_ulp = ccc_pow2i(ccc_bexp(p) - 1023 - 53);
+        easy = half_ulp - fabs(e) > ccc_pow2i(e0 - 80);
+    }
+    if (easy) {
+        ccc_dd r;
+        r.hi = p;
+        r.lo = e;
+        return r;
+    }
+    return ccc_certmul_k<1>(x, 0.0, y);
+}
+
+// certifiedMul<2,1,2>((x0, x1), y), leading term
+CCC_HD double ccc_certmul2_hi(double x0, double x1, double y) {
+    const int b0 = ccc_bexp(x0), by = ccc_bexp(y);
+    const int e0 = (b0 - 1022) + (by - 1022);
+    const double p0 = x0 * y;
+    const double er = ccc_fma(x0, y, -p0);
+    const double rest = er + x1 * y;
+    const double c = p0 + rest;
+    bool easy = x0 != 0.0 && y != 0.0 && b0 != 0 && b0 != 0x7ff && by != 0 && by != 0x7ff && e0 >= -700 &&
+                e0 <= 1000 && !ccc_pow2_or_special(c) && ccc_bexp(x1) != 0x7ff &&
+                fabs(x1) <= ccc_pow2i(b0 - 1023 - 53);
+    if (easy) {
+        const double res = (p0 - c) + rest;
+        const double half_ulp = ccc_pow2i(ccc_bexp(c) - 1023 - 53);
+        easy = fabs(fabs(res) - half_ulp) > ccc_pow2i(e0 - 80);
+    }
+    if (easy) return c;
+    return ccc_certmul_k<2>(x0, x1, y).hi;
+}
+
 // Leading terms the solver uses: x^2 (as a 2-term expansion) and x^3 = (x^2) * x.
-CCC_HD ccc_dd ccc_sq_dd(double x) { return ccc_certmul_k<1>(x, 0.0, x); }
+CCC_HD ccc_dd ccc_sq_dd(double x) { return ccc_certmul1(x, x); }
 CCC_HD double ccc_cube_hi(double x) {
     ccc_dd s = ccc_sq_dd(x);
-    return ccc_certmul_k<2>(s.hi, s.lo, x).hi;
+    return ccc_certmul2_hi(s.hi, s.lo, x);
 }

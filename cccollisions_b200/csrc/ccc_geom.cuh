@@ -484,7 +484,7 @@ __device__ __forceinline__ int cubic_prefix(double a, double b, double c, double
     double b3 = 2 * ccc_cube_hi(b);
     ccc_dd a2dd = ccc_sq_dd(a);
     double a2 = a2dd.hi;
-    double a3 = ccc_certmul_k<2>(a2dd.hi, a2dd.lo, a).hi;
+    double a3 = ccc_certmul2_hi(a2dd.hi, a2dd.lo, a);
     double p1 = b3 / a3;
     double p2 = (b * c * 9) / a2;
     double p3 = 27.0 * d / a;

@@ -641,7 +641,7 @@ template <class T> static void solve_cubic(double a, double b, double c, double 
         double b3 = 2 * ccc_cube_hi(b);
         ccc_dd a2dd = ccc_sq_dd(a);
         double a2 = a2dd.hi;
-        double a3 = ccc_certmul(a2dd.hi, a2dd.lo, 2, a).hi;
+        double a3 = ccc_certmul2_hi(a2dd.hi, a2dd.lo, a);
         double p1 = b3 / a3;
         double p2 = (b * c * 9) / a2;
         double p3 = 27.0 * d / a;
@@ -960,6 +960,67 @@ using namespace orc;
 // Return values >= 0 are counts; -1 = capacity overflow or malformed tree.
 // =======================================================================================
 #define ORC_API extern "C"
+
+// Self-check of the double-double short paths (ccc_ddmul.h): n operand sets drawn by a
+// splitmix64 stream from `seed` in one of four families (0: random significands over
+// exponents +-600; 1: significands of 1..30 bits, which make exact and tied products;
+// 2: neighbours of powers of two; 3: zeros, signed zeros, subnormals, huge values, inf and
+// NaN mixed in).  Each set checks certifiedMul<1,1,2> (both terms) and the leading term of
+// certifiedMul<2,1,2> against the bin algorithm.  out: [mismatches, short-path uses].
+static uint64_t sm64(uint64_t& s) {
+    uint64_t z = (s += 0x9e3779b97f4a7c15ull);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+static double draw(uint64_t& st, int family) {
+    uint64_t r = sm64(st);
+    int sign = (int)(r & 1);
+    int ex = (int)((r >> 1) % 1201) - 600;
+    uint64_t mant = sm64(st) & 0x000fffffffffffffull;
+    if (family == 1) {
+        int bits = 1 + (int)((r >> 20) % 30);
+        mant &= ~((1ull << (52 - bits + 1)) - 1) & 0x000fffffffffffffull;
+    } else if (family == 2) {
+        uint64_t k = (r >> 24) % 4;
+        mant = (r >> 40) & 1 ? k : (0x000fffffffffffffull - k);
+        ex = (int)((r >> 28) % 401) - 200;
+    } else if (family == 3) {
+        switch ((r >> 30) % 8) {
+            case 0: return sign ? -0.0 : 0.0;
+            case 1: return ccc_dfrombits(sm64(st) & 0x000fffffffffffffull);          // subnormal
+            case 2: return ccc_dfrombits(((uint64_t)(2000 + (r >> 33) % 46) << 52) | mant);
+            case 3: return sign ? -INFINITY : INFINITY;
+            case 4: return NAN;
+            default: ex = (int)((r >> 1) % 2001) - 1000;
+        }
+    }
+    uint64_t u = ((uint64_t)sign << 63) | ((uint64_t)(ex + 1023) << 52) | mant;
+    return ccc_dfrombits(u);
+}
+static bool same(double a, double b) { return ccc_dbits(a) == ccc_dbits(b) || (a != a && b != b); }
+
+ORC_API int orc_ddmul_check(int64_t n, uint64_t seed, int family, int64_t* out) {
+    int64_t bad = 0, fast = 0;
+#pragma omp parallel for reduction(+ : bad, fast) schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        uint64_t st = seed * 0x100000001b3ull + (uint64_t)i * 0x9e3779b97f4a7c15ull;
+        double x = draw(st, family), y = draw(st, family), z = draw(st, family);
+        ccc_dd g = ccc_certmul_k<1>(x, 0.0, y);
+        ccc_dd f = ccc_certmul1(x, y);
+        if (!same(g.hi, f.hi) || !same(g.lo, f.lo)) ++bad;
+        if (ccc_dbits(f.hi) == ccc_dbits(x * y) && !(x == 0.0 || y == 0.0)) ++fast;
+        // K = 2 on a normalised expansion (a square, as in the solver) and on (x, lo) pairs
+        ccc_dd sq = ccc_certmul_k<1>(x, 0.0, x);
+        if (!same(ccc_certmul_k<2>(sq.hi, sq.lo, z).hi, ccc_certmul2_hi(sq.hi, sq.lo, z))) ++bad;
+        ccc_dd pr = ccc_certmul_k<1>(y, 0.0, z);
+        if (!same(ccc_certmul_k<2>(pr.hi, pr.lo, x).hi, ccc_certmul2_hi(pr.hi, pr.lo, x))) ++bad;
+        if (!same(ccc_cube_hi(x), ccc_certmul_k<2>(sq.hi, sq.lo, x).hi)) ++bad;
+    }
+    out[0] = bad;
+    out[1] = fast;
+    return 0;
+}
 
 ORC_API int orc_bvh(int dtype, const void* tri, const void* tri_next, int n, int spatial, void* bboxes, int64_t* tree,
             uint32_t* codes) {

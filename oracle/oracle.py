@@ -91,6 +91,8 @@ def lib():
         L.orc_triangle_edge.argtypes = [ctypes.c_int, _P, _P, _P, ctypes.c_int, ctypes.c_int, _P, _P, _P, _I64,
                                         ctypes.c_int]
         L.orc_triangle_edge.restype = _I64
+        L.orc_ddmul_check.argtypes = [_I64, ctypes.c_uint64, ctypes.c_int, _P]
+        L.orc_ddmul_check.restype = ctypes.c_int
         L.orc_impulse_loop.argtypes = [ctypes.c_int, _P, _P, _P, _P, _P, _I64, _I64, ctypes.c_int, _P, ctypes.c_int,
                                        _P]
         L.orc_impulse_loop.restype = ctypes.c_int
@@ -299,6 +301,14 @@ def morton(x, y, z, single=False):
     if single:
         return lib().orc_morton_f(x, y, z)
     return lib().orc_morton(x, y, z)
+
+
+def ddmul_check(n, seed, family):
+    """(mismatches, short-path uses) of the double-double short paths against the bin
+    algorithm on n generated operand sets (orc_ddmul_check)."""
+    out = np.zeros(2, dtype=np.int64)
+    lib().orc_ddmul_check(int(n), int(seed), int(family), _ptr(out))
+    return int(out[0]), int(out[1])
 
 
 def certmul(x, y):

@@ -308,3 +308,14 @@ def test_impulses_from_rows_match_full(oracle):
     assert np.allclose(dx, dx2, rtol=1e-12, atol=1e-15)
     # every contact touches exactly four corners
     assert cnt.sum() == 4 * nc
+
+
+@pytest.mark.parametrize("family", [0, 1, 2, 3])
+def test_double_double_short_paths_match_the_bin_algorithm(oracle, family):
+    """The short paths of certifiedMul<1,1,2> and of the leading term of certifiedMul<2,1,2>
+    (TwoProd and a compensated sum away from ties) give the bin algorithm's bits: random
+    significands, 1..30-bit significands (exact and tied products), neighbours of powers of
+    two, and zeros / subnormals / huge / non-finite operands."""
+    bad, fast = oracle.ddmul_check(4_000_000, 77 + family, family)
+    assert bad == 0
+    assert fast > (3_000_000 if family < 3 else 1_000_000)
