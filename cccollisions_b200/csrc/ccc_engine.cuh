@@ -571,10 +571,28 @@ __global__ void k_engine_refit(Forest F, const T* __restrict__ x0, const T* __re
 // so each unordered pair is found once) and emits (min id, max id) in data slots.  Candidates
 // are the pairs whose fp32 boxes overlap, a superset of the exact ones; the continuous
 // narrow phase re-tests every pair's swept sub-boxes exactly.
+static constexpr int TRAV_BUF = 8;
+
+// the first n buffered pairs of thread tid to cand[base ..]; pairs past the capacity are
+// dropped and reported
+__device__ __forceinline__ void flush_candidates(int2 (*cbuf)[TRAV_THREADS], int tid, int n, int base,
+                                                 int2* __restrict__ cand, int cand_cap, WsHeader* hdr) {
+    for (int i = 0; i < n; ++i) {
+        const long long slot = (long long)base + i;
+        if (base >= 0 && slot < cand_cap) cand[slot] = cbuf[i][tid];
+        else atomicOr(&hdr->status, ST_CAND_OVERFLOW);
+    }
+}
+
 static __global__ void __launch_bounds__(TRAV_THREADS)
 k_traverse_q(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, const int* __restrict__ leaf_tri,
              Forest F, int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const int* __restrict__ mflags) {
     __shared__ int stack[STACK_DEPTH][TRAV_THREADS];
+    // Candidates go through a per-thread buffer of TRAV_BUF pairs and reach the global list
+    // TRAV_BUF at a time, so one atomic on the shared counter serves TRAV_BUF pairs of every
+    // thread of a coalesced group (the counter is contended by every SM).
+    __shared__ int2 cbuf[TRAV_BUF][TRAV_THREADS];
+    int nbuf = 0;
     const int tid = threadIdx.x;
     const int M = forest_size(F);
     const int total = __ldg(F.voff + M);
@@ -631,12 +649,15 @@ k_traverse_q(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, co
                 if (!hit) continue;
                 if (ref < 0) {
                     const int cid = aa[s];
-                    cg::coalesced_group grp = cg::coalesced_threads();
-                    int slot = 0;
-                    if (grp.thread_rank() == 0) slot = atomicAdd(&hdr->cand_count, (int)grp.size());
-                    slot = grp.shfl(slot, 0) + grp.thread_rank();
-                    if (slot < cand_cap) cand[slot] = make_int2(po + min(qid, cid), po + max(qid, cid));
-                    else atomicOr(&hdr->status, ST_CAND_OVERFLOW);
+                    cbuf[nbuf++][tid] = make_int2(po + min(qid, cid), po + max(qid, cid));
+                    if (nbuf == TRAV_BUF) {
+                        cg::coalesced_group grp = cg::coalesced_threads();
+                        int base = 0;
+                        if (grp.thread_rank() == 0) base = atomicAdd(&hdr->cand_count, TRAV_BUF * (int)grp.size());
+                        base = grp.shfl(base, 0) + TRAV_BUF * (int)grp.thread_rank();
+                        flush_candidates(cbuf, tid, TRAV_BUF, base, cand, cand_cap, hdr);
+                        nbuf = 0;
+                    }
                 } else if (next < 0) {
                     next = ref;
                 } else if (sp < STACK_DEPTH) {
@@ -657,6 +678,7 @@ k_traverse_q(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, co
             }
         }
     }
+    if (nbuf > 0) flush_candidates(cbuf, tid, nbuf, atomicAdd(&hdr->cand_count, nbuf), cand, cand_cap, hdr);
 }
 
 // ---------------------------------------------------------------------------------------
