@@ -571,27 +571,11 @@ __global__ void k_engine_refit(Forest F, const T* __restrict__ x0, const T* __re
 // so each unordered pair is found once) and emits (min id, max id) in data slots.  Candidates
 // are the pairs whose fp32 boxes overlap, a superset of the exact ones; the continuous
 // narrow phase re-tests every pair's swept sub-boxes exactly.
-static constexpr int TRAV_BUF = 8;
-
-// the first n buffered pairs of thread tid to cand[base ..]; pairs past the capacity are
-// dropped and reported
-__device__ __forceinline__ void flush_candidates(int2 (*cbuf)[TRAV_THREADS], int tid, int n, int base,
-                                                 int2* __restrict__ cand, int cand_cap, WsHeader* hdr) {
-    for (int i = 0; i < n; ++i) {
-        const long long slot = (long long)base + i;
-        if (base >= 0 && slot < cand_cap) cand[slot] = cbuf[i][tid];
-        else atomicOr(&hdr->status, ST_CAND_OVERFLOW);
-    }
-}
-
 static __global__ void __launch_bounds__(TRAV_THREADS)
 k_traverse_q(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, const int* __restrict__ leaf_tri,
              Forest F, int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const int* __restrict__ mflags) {
     __shared__ int stack[STACK_DEPTH][TRAV_THREADS];
-    // Candidates go through a per-thread buffer of TRAV_BUF pairs and reach the global list
-    // TRAV_BUF at a time, so one atomic on the shared counter serves TRAV_BUF pairs of every
-    // thread of a coalesced group (the counter is contended by every SM).
-    __shared__ int2 cbuf[TRAV_BUF][TRAV_THREADS];
+    __shared__ int2 cbuf[TRAV_BUF][TRAV_THREADS];     // candidate buffer (see flush_candidates)
     int nbuf = 0;
     const int tid = threadIdx.x;
     const int M = forest_size(F);
@@ -678,7 +662,7 @@ k_traverse_q(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, co
             }
         }
     }
-    if (nbuf > 0) flush_candidates(cbuf, tid, nbuf, atomicAdd(&hdr->cand_count, nbuf), cand, cand_cap, hdr);
+    if (nbuf > 0) flush_rest(cbuf, tid, nbuf, cand, cand_cap, hdr);
 }
 
 // ---------------------------------------------------------------------------------------

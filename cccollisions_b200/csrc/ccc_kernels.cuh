@@ -318,11 +318,46 @@ template <class T> struct TensorLeaves {
     }
 };
 
+// Traversal kernels pass candidates through a per-thread buffer of TRAV_BUF pairs and
+// reserve TRAV_BUF slots per thread of a coalesced group with one atomic on the shared
+// counter, which every SM contends for.
+static constexpr int TRAV_BUF = 16;
+
+// the first n buffered pairs of thread tid to cand[base ..]; pairs past the capacity are
+// dropped and reported
+__device__ __forceinline__ void flush_candidates(int2 (*cbuf)[TRAV_THREADS], int tid, int n, int base,
+                                                 int2* __restrict__ cand, int cand_cap, WsHeader* hdr) {
+    for (int i = 0; i < n; ++i) {
+        const long long slot = (long long)base + i;
+        if (base >= 0 && slot < cand_cap) cand[slot] = cbuf[i][tid];
+        else atomicOr(&hdr->status, ST_CAND_OVERFLOW);
+    }
+}
+
+// the remaining buffered pairs of every thread of the calling coalesced group, with one
+// atomic for the group (exclusive scan of the counts)
+__device__ __forceinline__ void flush_rest(int2 (*cbuf)[TRAV_THREADS], int tid, int n, int2* __restrict__ cand,
+                                           int cand_cap, WsHeader* hdr) {
+    cg::coalesced_group grp = cg::coalesced_threads();
+    int incl = n;
+    for (int o = 1; o < (int)grp.size(); o <<= 1) {
+        int y = grp.shfl_up(incl, o);
+        if ((int)grp.thread_rank() >= o) incl += y;
+    }
+    int total = grp.shfl(incl, grp.size() - 1);
+    int base = 0;
+    if (grp.thread_rank() == 0) base = atomicAdd(&hdr->cand_count, total);
+    base = grp.shfl(base, 0) + incl - n;
+    flush_candidates(cbuf, tid, n, base, cand, cand_cap, hdr);
+}
+
 template <class T, bool MASKED, bool EXACT_F32, class Leaves>
 __global__ void __launch_bounds__(TRAV_THREADS)
 k_traverse(const TNode* __restrict__ nodes, Leaves leaves, Forest F, const uint8_t* __restrict__ mask, T th,
            int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const int* __restrict__ mflags) {
     __shared__ int stack[STACK_DEPTH][TRAV_THREADS];
+    __shared__ int2 cbuf[TRAV_BUF][TRAV_THREADS];
+    int nbuf = 0;
     const int tid = threadIdx.x;
     const int M = forest_size(F);
     const int total = __ldg(F.voff + M);
@@ -389,12 +424,15 @@ k_traverse(const TNode* __restrict__ nodes, Leaves leaves, Forest F, const uint8
                     if (MASKED && mask[po + cid] && !(qid < cid)) hit = false;
                     if (hit && !EXACT_F32) hit = overlap(q, leaves.box(m, vo, po, n, cpos), th);
                     if (hit) {
-                        cg::coalesced_group grp = cg::coalesced_threads();
-                        int slot = 0;
-                        if (grp.thread_rank() == 0) slot = atomicAdd(&hdr->cand_count, (int)grp.size());
-                        slot = grp.shfl(slot, 0) + grp.thread_rank();
-                        if (slot < cand_cap) cand[slot] = make_int2(po + min(qid, cid), po + max(qid, cid));
-                        else atomicOr(&hdr->status, ST_CAND_OVERFLOW);
+                        cbuf[nbuf++][tid] = make_int2(po + min(qid, cid), po + max(qid, cid));
+                        if (nbuf == TRAV_BUF) {
+                            cg::coalesced_group grp = cg::coalesced_threads();
+                            int base = 0;
+                            if (grp.thread_rank() == 0) base = atomicAdd(&hdr->cand_count, TRAV_BUF * (int)grp.size());
+                            base = grp.shfl(base, 0) + TRAV_BUF * (int)grp.thread_rank();
+                            flush_candidates(cbuf, tid, TRAV_BUF, base, cand, cand_cap, hdr);
+                            nbuf = 0;
+                        }
                     }
                 }
             }
@@ -411,6 +449,7 @@ k_traverse(const TNode* __restrict__ nodes, Leaves leaves, Forest F, const uint8
             }
         }
     }
+    if (nbuf > 0) flush_rest(cbuf, tid, nbuf, cand, cand_cap, hdr);
 }
 
 // ---------------------------------------------------------------------------------------
