@@ -574,7 +574,7 @@ __global__ void k_engine_refit(Forest F, const T* __restrict__ x0, const T* __re
 static __global__ void __launch_bounds__(TRAV_THREADS)
 k_traverse_q(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, const int* __restrict__ leaf_tri,
              Forest F, int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const int* __restrict__ mflags) {
-    __shared__ int stack[STACK_DEPTH][TRAV_THREADS];
+    int stack[STACK_DEPTH];          // per-thread, in local memory (L1): shared memory holds the buffer
     __shared__ int2 cbuf[TRAV_BUF][TRAV_THREADS];     // candidate buffer (see flush_candidates)
     int nbuf = 0;
     const int tid = threadIdx.x;
@@ -645,7 +645,7 @@ k_traverse_q(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, co
                 } else if (next < 0) {
                     next = ref;
                 } else if (sp < STACK_DEPTH) {
-                    stack[sp++][tid] = ref;
+                    stack[sp++] = ref;
                 } else {
                     deep = true;
                 }
@@ -658,7 +658,7 @@ k_traverse_q(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, co
                 node = next;
             } else {
                 if (sp == 0) break;
-                node = stack[--sp][tid];
+                node = stack[--sp];
             }
         }
     }

@@ -355,7 +355,7 @@ template <class T, bool MASKED, bool EXACT_F32, class Leaves>
 __global__ void __launch_bounds__(TRAV_THREADS)
 k_traverse(const TNode* __restrict__ nodes, Leaves leaves, Forest F, const uint8_t* __restrict__ mask, T th,
            int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const int* __restrict__ mflags) {
-    __shared__ int stack[STACK_DEPTH][TRAV_THREADS];
+    int stack[STACK_DEPTH];          // per-thread, in local memory (L1): shared memory holds the buffer
     __shared__ int2 cbuf[TRAV_BUF][TRAV_THREADS];
     int nbuf = 0;
     const int tid = threadIdx.x;
@@ -439,12 +439,12 @@ k_traverse(const TNode* __restrict__ nodes, Leaves leaves, Forest F, const uint8
             bool tl = ol && D.x >= 0, tr = orr && D.y >= 0;
             if (!tl && !tr) {
                 if (sp == 0) break;
-                node = stack[--sp][tid];
+                node = stack[--sp];
             } else {
                 node = tl ? D.x : D.y;
                 if (tl && tr) {
                     if (sp >= STACK_DEPTH) { atomicOr(&hdr->status, ST_STACK_OVERFLOW); break; }
-                    stack[sp++][tid] = D.y;
+                    stack[sp++] = D.y;
                 }
             }
         }
