@@ -119,7 +119,9 @@ template <int K> CCC_HD ccc_dd ccc_certmul_k(double x0, double x1, double y) {
     return r;
 }
 
-// the same with the number of terms K in {1, 2} given at run time
+
+// the same with the number of terms K in {1, 2} given at run time (kept out of line: the
+// short paths below call it only for their rare fallback cases)
 CCC_HD_CALL ccc_dd ccc_certmul(double x0, double x1, int k, double y) {
     return k > 1 ? ccc_certmul_k<2>(x0, x1, y) : ccc_certmul_k<1>(x0, x1, y);
 }
@@ -171,7 +173,7 @@ CCC_HD ccc_dd ccc_certmul1(double x, double y) {
         r.lo = e;
         return r;
     }
-    return ccc_certmul_k<1>(x, 0.0, y);
+    return ccc_certmul(x, 0.0, 1, y);
 }
 
 // certifiedMul<2,1,2>((x0, x1), y), leading term
@@ -191,7 +193,7 @@ CCC_HD double ccc_certmul2_hi(double x0, double x1, double y) {
         easy = fabs(fabs(res) - half_ulp) > ccc_pow2i(e0 - 80);
     }
     if (easy) return c;
-    return ccc_certmul_k<2>(x0, x1, y).hi;
+    return ccc_certmul(x0, x1, 2, y).hi;
 }
 
 // Leading terms the solver uses: x^2 (as a 2-term expansion) and x^3 = (x^2) * x.
