@@ -624,12 +624,14 @@ template <class T> struct CcdLayout {
     static constexpr size_t clist = items + CCD_QUEUE * sizeof(int2);                  // u16 [BATCH]
     static constexpr size_t root_rec = clist + CCD_BATCH * 2;                          // u16 [3 BATCH]
     static constexpr size_t rec_cls = root_rec + 3 * CCD_BATCH * 2;                    // u8 [BATCH]
-    static constexpr size_t ints = align16(rec_cls + CCD_BATCH);                       // int [64]
+    static constexpr size_t rec_pos = align16(rec_cls + CCD_BATCH);                    // u16 [BATCH]
+    static constexpr size_t ints = align16(rec_pos + CCD_BATCH * 2);                   // int [64]
     static constexpr size_t bytes = ints + 64 * sizeof(int);
 };
 
 // slots of the small int area
-enum CcdInts { CI_WARP = 0, CI_TOTAL = 32, CI_COUNT = 33, CI_CURSOR = 37, CI_OFFSET = 41, CI_ROOTS = 46 };
+// (class counts and root count come in two sets, used by alternate batches)
+enum CcdInts { CI_WARP = 0, CI_TOTAL = 32, CI_COUNT = 33, CI_ROOTS = 41 };
 
 // a queued sub-test: triangle slots i and j, type k in the top bits of j (slots < 2^28)
 __device__ __forceinline__ int2 pack_subtest(int i, int j, int k) { return make_int2(i, j | (k << 28)); }
@@ -656,6 +658,7 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
     unsigned short* clist = reinterpret_cast<unsigned short*>(smem + L::clist);
     unsigned short* root_rec = reinterpret_cast<unsigned short*>(smem + L::root_rec);
     unsigned char* rec_cls = smem + L::rec_cls;
+    unsigned short* rec_pos = reinterpret_cast<unsigned short*>(smem + L::rec_pos);
     int* ints = reinterpret_cast<int*>(smem + L::ints);
     constexpr int NW = CCD_BLOCK / 32;
     constexpr int NB = CCD_BATCH;
@@ -666,6 +669,12 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
     const unsigned lt = (1u << lane) - 1u;
     const int n = min(*(volatile int*)&hdr->cand_count, cand_cap);
     int head = 0, queued = 0;           // ring queue of sub-tests (block-uniform)
+    // class counts and root count of a batch, two sets used by alternate batches: a batch
+    // clears the other set at its end, when every read of that set is two barriers back
+    // (the staging barriers order the initial clearing before the first batch)
+    int par = 0;
+    if (tid < 8) ints[CI_COUNT + tid] = 0;
+    if (tid < 2) ints[CI_ROOTS + tid] = 0;
     for (long long base = (long long)blockIdx.x * CCD_BLOCK;; base += (long long)gridDim.x * CCD_BLOCK) {
         const bool more = base < n;
         if (!more && queued == 0) break;
@@ -719,10 +728,7 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
         // solve full batches (and, after the last chunk, the remainder)
         while (queued >= NB || (!more && queued > 0)) {
             const int nb = min(NB, queued);
-            if (tid < 8) ints[CI_COUNT + tid] = 0;           // class counts and cursors
-            if (tid == 8) ints[CI_ROOTS] = 0;
-            __syncthreads();
-            // (1) coefficients and solver prefix
+            // (1) coefficients and solver prefix; each sub-test takes its place in its class
             for (int ri = tid; ri < nb; ri += CCD_BLOCK) {
                 int2 it = items[(head + ri) % Q];
                 int k = (it.y >> 28) & 15;
@@ -738,30 +744,24 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                 rec[4 * NB + ri] = g;
                 rec[5 * NB + ri] = h;
                 rec_cls[ri] = (unsigned char)cls;
-                if (cls != CUBIC_NONE) atomicAdd(&ints[CI_COUNT + cls - 1], 1);
+                if (cls != CUBIC_NONE) rec_pos[ri] = (unsigned short)atomicAdd(&ints[CI_COUNT + 4 * par + cls - 1], 1);
             }
             __syncthreads();
-            if (tid == 0) {
-                int o = 0;
-                for (int cc = 0; cc < 4; ++cc) {
-                    ints[CI_OFFSET + cc] = o;
-                    o += ints[CI_COUNT + cc];
-                }
-                ints[CI_OFFSET + 4] = o;
-            }
-            __syncthreads();
-            // sub-tests ordered by class
+            // sub-tests ordered by class (every thread forms the class offsets itself)
+            const int* counts = ints + CI_COUNT + 4 * par;
+            const int o1 = counts[0];
+            const int o2 = o1 + counts[1];
+            const int o3 = o2 + counts[2];
+            const int nsolve = o3 + counts[3];
             for (int ri = tid; ri < nb; ri += CCD_BLOCK) {
                 int cls = rec_cls[ri];
                 if (cls != CUBIC_NONE) {
-                    int p = atomicAdd(&ints[CI_CURSOR + cls - 1], 1);
-                    clist[ints[CI_OFFSET + cls - 1] + p] = (unsigned short)ri;
+                    int off = cls == 1 ? 0 : (cls == 2 ? o1 : (cls == 3 ? o2 : o3));
+                    clist[off + rec_pos[ri]] = (unsigned short)ri;
                 }
             }
             __syncthreads();
             // (2) roots; the ones in [0, 1] go to the root list
-            const int nsolve = ints[CI_OFFSET + 4];
-            const int o1 = ints[CI_OFFSET + 1], o2 = ints[CI_OFFSET + 2], o3 = ints[CI_OFFSET + 3];
             for (int j0 = 0; j0 < nsolve; j0 += CCD_BLOCK) {
                 const int j = j0 + tid;
                 T rr[3] = {(T)-1, (T)-1, (T)-1};
@@ -777,7 +777,7 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                     bool keep = j < nsolve && (rr[s] >= 0 && rr[s] <= 1);
                     unsigned m = __ballot_sync(FULL, keep);
                     int at = 0;
-                    if (lane == 0 && m) at = atomicAdd(&ints[CI_ROOTS], __popc(m));
+                    if (lane == 0 && m) at = atomicAdd(&ints[CI_ROOTS + par], __popc(m));
                     at = __shfl_sync(FULL, at, 0) + __popc(m & lt);
                     if (keep) {
                         root_rec[at] = (unsigned short)ri;
@@ -786,7 +786,7 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                 }
             }
             __syncthreads();
-            const int nroots = ints[CI_ROOTS];
+            const int nroots = ints[CI_ROOTS + par];
             if (tid == 0 && nroots) atomicAdd(&hdr->roots, nroots);
             // (3) filter and output
             for (int j = tid; j < nroots; j += CCD_BLOCK) {
@@ -815,6 +815,9 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                     sink.add(tet, q.x, q.y, k, root, ct, F, M, &hdr->status);
                 }
             }
+            if (tid < 4) ints[CI_COUNT + 4 * (par ^ 1) + tid] = 0;
+            if (tid == 4) ints[CI_ROOTS + (par ^ 1)] = 0;
+            par ^= 1;
             head = (head + nb) % Q;
             queued -= nb;
             __syncthreads();
