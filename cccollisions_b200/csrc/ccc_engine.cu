@@ -50,7 +50,7 @@ struct EngineLayout {
     int64_t hdr, mesh_cnt, contacts, iters, flags, state_end;
     int64_t tab, btab, bounds;
     int64_t x0, x1, masses, faces;
-    int64_t leaf_tri, lparent, nparent, visits, nodes, qnodes, qcode, qleaf;
+    int64_t leaf_tri, lparent, nparent, visits, nodes, qnodes, qcode, qleaf, nrange, front;
     int64_t rows, times, cand;
     int64_t keys0, keys1, vals0, vals1, hist;
     int64_t verts0, verts1, vel, acc, end;
@@ -87,6 +87,8 @@ EngineLayout engine_layout(int64_t tsz, int64_t tc, int64_t vc, int64_t mc, int6
     L.qnodes = take(tc * (int64_t)sizeof(QNode));
     L.qcode = take(tc * 4);
     L.qleaf = take(tc * 4);
+    L.nrange = take(tc * 8);
+    L.front = take(tc * 8);
     L.rows = take(tc * maxcol * 3 * 8);
     L.times = take(tc * maxcol * tsz);
     L.cand_cap = tc * maxc;
@@ -238,14 +240,19 @@ int upload_table(ccc_engine* e, int which, const int32_t* ids, int64_t n, cudaSt
 // The refit's climbs are chains of dependent L2 round trips, so it runs about one leaf per
 // thread (up to 64 blocks per SM) rather than a grid-stride loop over few threads.
 inline int refit_grid(const ccc_engine* e) {
-    return (int)std::min<int64_t>(grid_for(e->tri_cap, ITEM_THREADS), (int64_t)num_sms() * 64);
+    return (int)std::min<int64_t>(grid_for(e->tri_cap, REFIT_THREADS), (int64_t)num_sms() * 64);
 }
 
 template <class T> int refit(ccc_engine* e, const Tables& t, const int* flags, cudaStream_t s) {
-    CCC_LAUNCH("k_engine_refit", s, k_engine_refit<T><<<refit_grid(e), ITEM_THREADS, 0, s>>>(
+    if (cudaMemsetAsync(&e->hdr()->front, 0, sizeof(int), s) != cudaSuccess) return CCC_ERR_CUDA;
+    CCC_LAUNCH("k_engine_refit", s, k_engine_refit_local<T><<<refit_grid(e), REFIT_THREADS, 0, s>>>(
         t.f, e->at<T>(e->L.x0), e->at<T>(e->L.x1), e->at<int>(e->L.leaf_tri), e->at<int>(e->L.lparent),
-        e->at<int>(e->L.nparent), e->at<int>(e->L.qcode), e->at<int>(e->L.qleaf),
-        e->at<QNode>(e->L.qnodes), e->at<unsigned>(e->L.visits), flags, &e->hdr()->status));
+        e->at<int>(e->L.nparent), e->at<int>(e->L.qcode), e->at<int>(e->L.qleaf), e->at<int2>(e->L.nrange),
+        e->at<QNode>(e->L.qnodes), e->at<int2>(e->L.front), (int)e->tri_cap, flags, e->hdr()));
+    CCC_LAUNCH_CHECK();
+    CCC_LAUNCH("k_engine_refit_front", s, k_engine_refit_front<<<num_sms() * 8, 256, 0, s>>>(
+        t.f, e->at<int>(e->L.nparent), e->at<int>(e->L.qcode), e->at<QNode>(e->L.qnodes),
+        e->at<unsigned>(e->L.visits), e->at<int2>(e->L.front), (int)e->tri_cap, e->hdr()));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -347,7 +354,7 @@ template <class T> int build_trees(ccc_engine* e, int64_t ntri, int64_t nb, cuda
     }
     CCC_LAUNCH("k_karras_build", s, k_karras_build<<<item_grid(), ITEM_THREADS, 0, s>>>(
         t.f, keys[cur], vals[cur], e->at<TNode>(e->L.nodes), e->at<int>(e->L.nparent), e->at<int>(e->L.lparent),
-        e->at<int>(e->L.leaf_tri), e->at<unsigned>(e->L.visits), &e->hdr()->status));
+        e->at<int>(e->L.leaf_tri), e->at<unsigned>(e->L.visits), e->at<int2>(e->L.nrange), &e->hdr()->status));
     CCC_LAUNCH_CHECK();
     CCC_LAUNCH("k_qtree_depth", s, k_qtree_depth<<<item_grid(), ITEM_THREADS, 0, s>>>(
         t.f, e->at<int>(e->L.nparent), e->at<int>(e->L.qcode), &e->hdr()->status));

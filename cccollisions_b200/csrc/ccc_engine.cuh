@@ -294,7 +294,7 @@ static __global__ void k_karras_build(Forest F, const unsigned long long* __rest
                                       const int* __restrict__ vals, TNode* __restrict__ nodes,
                                       int* __restrict__ nparent, int* __restrict__ lparent,
                                       int* __restrict__ leaf_tri, unsigned* __restrict__ visits,
-                                      int* __restrict__ status) {
+                                      int2* __restrict__ nrange, int* __restrict__ status) {
     const int M = forest_size(F);
     const int total_internal = __ldg(F.voff + M) - M;
     for (int gi = blockIdx.x * blockDim.x + threadIdx.x; gi < total_internal; gi += gridDim.x * blockDim.x) {
@@ -346,6 +346,7 @@ static __global__ void k_karras_build(Forest F, const unsigned long long* __rest
             nparent[po + split + 1] = (i << 1) | 1;
         }
         nodes[po + i].d = make_int4(lref, rref, laux, raux);
+        nrange[po + i] = make_int2(lo, hi);
         visits[po + i] = 0u;
         if (i == 0) nparent[po] = -1;
     }
@@ -498,45 +499,136 @@ __device__ __forceinline__ void read_qslot(const QNode* qn, int code, float lo[3
 __device__ __forceinline__ float hmin4(float4 v) { return fminf(fminf(v.x, v.y), fminf(v.z, v.w)); }
 __device__ __forceinline__ float hmax4(float4 v) { return fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)); }
 
-// Every binary node is reached twice per refit; the refit counters only ever grow, and the
-// arrival that finds an odd count is the second one, so nothing has to be cleared between
-// steps.  Meshes with MF_DONE set in mflags (when given) are skipped.
+// Refit: every leaf writes its swept box (fp32, rounded outward) into its QNode slot and
+// climbs; at each binary node the second arrival (the one that finds the node's other
+// subtree done) unions the children and goes on, the first stops.  Two passes:
+//  * pass 1 (k_engine_refit_local): a block takes REFIT_THREADS consecutive leaf positions
+//    and refits every node whose leaf range lies inside them, with arrival counters in
+//    shared memory and block-scope fences; a climb that reaches a node reaching outside the
+//    block stops and hands that arrival to pass 2 through the frontier list;
+//  * pass 2 (k_engine_refit_front) finishes those climbs with device-scope fences, global
+//    arrival counters and L2 reads.  The global counters only ever grow and the arrival
+//    that finds an odd count is the second one, so they are never cleared (a node refit in
+//    pass 1 leaves its counter alone).  The kernel boundary makes every box written in
+//    pass 1 visible to pass 2.
+// Most nodes lie inside one block's range, so most arrivals cost a shared-memory atomic
+// instead of a device fence and an L2 round trip.  Meshes with MF_DONE set in mflags (when
+// given) are skipped.
+static constexpr int REFIT_THREADS = 256;
+
 template <class T>
-__global__ void k_engine_refit(Forest F, const T* __restrict__ x0, const T* __restrict__ x1,
-                               const int* __restrict__ leaf_tri, const int* __restrict__ lparent,
-                               const int* __restrict__ nparent, const int* __restrict__ qcode,
-                               const int* __restrict__ qleaf, QNode* qnodes, unsigned* visits,
-                               const int* __restrict__ mflags, int* status) {
+__device__ __forceinline__ void refit_leaf_local(int v, int base, const Forest& F, int M, const T* __restrict__ x0,
+                                                 const T* __restrict__ x1, const int* __restrict__ leaf_tri,
+                                                 const int* __restrict__ lparent, const int* __restrict__ nparent,
+                                                 const int* __restrict__ qcode, const int* __restrict__ qleaf,
+                                                 const int2* __restrict__ nrange, QNode* qnodes, unsigned* scnt,
+                                                 int2* __restrict__ front, int front_cap,
+                                                 const int* __restrict__ mflags, WsHeader* hdr) {
+    const int m = find_mesh(F.voff, M, v, 0);
+    const int vo = __ldg(F.voff + m), po = __ldg(F.poff + m);
+    const int n = __ldg(F.voff + m + 1) - vo;
+    if (n < 2) return;
+    if (mflags && (__ldg(mflags + __ldg(F.sid + m)) & MF_DONE)) return;
+    const int p = v - vo;
+    const int t = __ldg(leaf_tri + po + p);
+    if (t < 0 || t >= n) { atomicOr(&hdr->status, ST_MALFORMED_TREE); return; }
+    const long long slot = (long long)po + t;
+    Box<T> b = merge(tri_box(load_tri(x0, slot)), tri_box(load_tri(x1, slot)));
+    float lo[3], hi[3];
+    box_outward_f32(b, lo, hi);
+    QNode* qn = qnodes + po;
+    const int lq = __ldg(qleaf + po + p);
+    if (lq < 0 || (lq >> 2) >= n - 1) { atomicOr(&hdr->status, ST_MALFORMED_TREE); return; }
+    write_qslot(qn, lq, lo, hi);
+    // the block's leaf positions in this mesh
+    const int blo = base - vo, bhi = base + REFIT_THREADS - 1 - vo;
+    int code = __ldg(lparent + po + p);
+    for (int guard = 0; guard < n; ++guard) {
+        const int node = code >> 1;
+        if (code < 0 || node >= n - 1) { atomicOr(&hdr->status, ST_MALFORMED_TREE); return; }
+        const int2 r = __ldg(nrange + po + node);
+        if (r.x < blo || r.y > bhi) {
+            // the node reaches outside the block: pass 2 takes this arrival
+            const int f = atomicAdd(&hdr->front, 1);
+            if (f < front_cap) front[f] = make_int2(m, code);
+            else atomicOr(&hdr->status, ST_MALFORMED_TREE);
+            return;
+        }
+        __threadfence_block();
+        if (atomicAdd(scnt + (node - blo), 1u) == 0u) return;           // first arrival
+        __threadfence_block();
+        const int qc = __ldg(qcode + po + node);
+        if (qc <= QCODE_ODD) {
+            const int c0 = QCODE_ODD - qc;
+            if ((c0 >> 2) >= n - 1 || (c0 & 3) > 2) { atomicOr(&hdr->status, ST_MALFORMED_TREE); return; }
+            // slots written by threads of this block: plain loads after the block fence
+            const float* f = reinterpret_cast<const float*>(qn + (c0 >> 2));
+            const int sl = c0 & 3;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                lo[c] = fminf(f[4 * c + sl], f[4 * c + sl + 1]);
+                hi[c] = fmaxf(f[12 + 4 * c + sl], f[12 + 4 * c + sl + 1]);
+            }
+        } else {
+            const float4* f = reinterpret_cast<const float4*>(qn + node);
+            lo[0] = hmin4(f[0]);
+            lo[1] = hmin4(f[1]);
+            lo[2] = hmin4(f[2]);
+            hi[0] = hmax4(f[3]);
+            hi[1] = hmax4(f[4]);
+            hi[2] = hmax4(f[5]);
+            if (qc == QCODE_ROOT) return;
+            if (qc < 0 || (qc >> 2) >= n - 1) { atomicOr(&hdr->status, ST_MALFORMED_TREE); return; }
+            write_qslot(qn, qc, lo, hi);
+        }
+        code = __ldg(nparent + po + node);
+        if (code < 0) return;
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(REFIT_THREADS)
+k_engine_refit_local(Forest F, const T* __restrict__ x0, const T* __restrict__ x1, const int* __restrict__ leaf_tri,
+                     const int* __restrict__ lparent, const int* __restrict__ nparent,
+                     const int* __restrict__ qcode, const int* __restrict__ qleaf, const int2* __restrict__ nrange,
+                     QNode* qnodes, int2* __restrict__ front, int front_cap, const int* __restrict__ mflags,
+                     WsHeader* hdr) {
+    __shared__ unsigned scnt[REFIT_THREADS];
     const int M = forest_size(F);
     const int total = __ldg(F.voff + M);
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
-        int m = find_mesh(F.voff, M, v, 0);
-        int vo = __ldg(F.voff + m), po = __ldg(F.poff + m);
-        int n = __ldg(F.voff + m + 1) - vo;
-        if (n < 2) continue;
-        if (mflags && (__ldg(mflags + __ldg(F.sid + m)) & MF_DONE)) continue;
-        int p = v - vo;
-        int t = __ldg(leaf_tri + po + p);
-        if (t < 0 || t >= n) { atomicOr(status, ST_MALFORMED_TREE); continue; }
-        long long slot = (long long)po + t;
-        Box<T> b = merge(tri_box(load_tri(x0, slot)), tri_box(load_tri(x1, slot)));
-        float lo[3], hi[3];
-        box_outward_f32(b, lo, hi);
+    for (int base = blockIdx.x * REFIT_THREADS; base < total; base += gridDim.x * REFIT_THREADS) {
+        scnt[threadIdx.x] = 0u;
+        __syncthreads();
+        const int v = base + threadIdx.x;
+        if (v < total)
+            refit_leaf_local<T>(v, base, F, M, x0, x1, leaf_tri, lparent, nparent, qcode, qleaf, nrange, qnodes, scnt,
+                                front, front_cap, mflags, hdr);
+        __syncthreads();
+    }
+}
+
+// pass 2: the climbs handed over by pass 1, from the node they reached (global protocol)
+static __global__ void k_engine_refit_front(Forest F, const int* __restrict__ nparent, const int* __restrict__ qcode,
+                                            QNode* qnodes, unsigned* visits, const int2* __restrict__ front,
+                                            int front_cap, WsHeader* hdr) {
+    const int nf = min(*(volatile int*)&hdr->front, front_cap);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nf; i += gridDim.x * blockDim.x) {
+        const int2 e = front[i];
+        const int m = e.x;
+        const int vo = __ldg(F.voff + m), po = __ldg(F.poff + m);
+        const int n = __ldg(F.voff + m + 1) - vo;
         QNode* qn = qnodes + po;
-        const int lq = __ldg(qleaf + po + p);
-        if (lq < 0 || (lq >> 2) >= n - 1) { atomicOr(status, ST_MALFORMED_TREE); continue; }
-        write_qslot(qn, lq, lo, hi);
-        int code = __ldg(lparent + po + p);
+        int code = e.y;
+        float lo[3], hi[3];
         for (int guard = 0; guard < n; ++guard) {
-            int node = code >> 1;
-            if (code < 0 || node >= n - 1) { atomicOr(status, ST_MALFORMED_TREE); break; }
+            const int node = code >> 1;
+            if (code < 0 || node >= n - 1) { atomicOr(&hdr->status, ST_MALFORMED_TREE); break; }
             __threadfence();
             if ((atomicAdd(visits + po + node, 1u) & 1u) == 0u) break;     // first arrival
             const int qc = __ldg(qcode + po + node);
             if (qc <= QCODE_ODD) {
-                // its box is the union of its two children's adjacent slots in the QNode above
                 const int c0 = QCODE_ODD - qc;
-                if ((c0 >> 2) >= n - 1 || (c0 & 3) > 2) { atomicOr(status, ST_MALFORMED_TREE); break; }
+                if ((c0 >> 2) >= n - 1 || (c0 & 3) > 2) { atomicOr(&hdr->status, ST_MALFORMED_TREE); break; }
                 float l2[3], h2[3];
                 read_qslot(qn, c0, lo, hi);
                 read_qslot(qn, c0 + 1, l2, h2);
@@ -546,7 +638,6 @@ __global__ void k_engine_refit(Forest F, const T* __restrict__ x0, const T* __re
                     hi[c] = fmaxf(hi[c], h2[c]);
                 }
             } else {
-                // the union of its QNode's slots (unused slots are empty boxes)
                 const float4* f = reinterpret_cast<const float4*>(qn + node);
                 lo[0] = hmin4(__ldcg(f + 0));
                 lo[1] = hmin4(__ldcg(f + 1));
@@ -555,7 +646,7 @@ __global__ void k_engine_refit(Forest F, const T* __restrict__ x0, const T* __re
                 hi[1] = hmax4(__ldcg(f + 4));
                 hi[2] = hmax4(__ldcg(f + 5));
                 if (qc == QCODE_ROOT) break;
-                if (qc < 0 || (qc >> 2) >= n - 1) { atomicOr(status, ST_MALFORMED_TREE); break; }
+                if (qc < 0 || (qc >> 2) >= n - 1) { atomicOr(&hdr->status, ST_MALFORMED_TREE); break; }
                 write_qslot(qn, qc, lo, hi);
             }
             code = __ldg(nparent + po + node);

@@ -37,7 +37,8 @@ struct WsHeader {
     int cand_count;
     int subtests;      // continuous sub-tests (pair, type) solved
     int roots;         // roots in [0, 1] filtered
-    int pad[12];
+    int front;         // engine refit: climbs handed from the block pass to the global pass
+    int pad[11];
 };
 
 struct __align__(16) TNode {

@@ -68,3 +68,44 @@ def test_pipeline_steps_equal_single_steps(cuda, graph):
             assert got == expect[i][sid], (k, sid)
     assert np.array_equal(eng.view(spare)["x0"].cpu().numpy(), spare_x0)
     eng.close()
+
+
+def test_pack_rows_capacity_and_meta(cuda):
+    """pack_rows with room for fewer rows than the step produced: the first `capacity` rows
+    are packed, the offsets still count every row, and the status word reports the overflow;
+    with room for all rows each mesh's slice equals its own rows."""
+    from cccollisions_b200 import _native as N
+    from cccollisions_b200 import workloads as W
+    from cccollisions_b200.engine import Engine
+    meshes = [W.jittered_fold(220 + i, 12, 10) for i in range(3)]
+    eng = Engine(tri_capacity=sum(x0.shape[0] for x0, _, _ in meshes) + 16, mesh_capacity=4)
+    sids = [eng.add_mesh(x0.shape[0]) for x0, _, _ in meshes]
+    for sid, (x0, x1, _) in zip(sids, meshes):
+        eng.upload_soup(sid, x0, x1)
+    eng.set_active(sids)
+    eng.build(sids)
+    eng.ccd()
+    st = eng.state(sids)
+    counts = dict(zip(sids, (int(n) for n in st["rows"])))
+    total = sum(counts.values())
+    assert total > 10
+    M = len(sids)
+    meta = torch.empty(2 * M + 2, dtype=torch.int32, device=cuda)
+    rows = torch.full((total, 3), -7, dtype=torch.int64, device=cuda)
+    times = torch.full((total,), -7.0, dtype=torch.float64, device=cuda)
+    eng.pack_rows(rows, times, meta)
+    m = meta.cpu().numpy()
+    assert m[M] == total and m[2 * M + 1] == 0
+    for i, sid in enumerate(m[M + 1:2 * M + 1].tolist()):
+        r, t = eng.collisions(sid, counts[sid])
+        assert m[i + 1] - m[i] == counts[sid]
+        got = _ms(rows[m[i]:m[i + 1]].cpu().numpy(), times[m[i]:m[i + 1]].cpu().numpy())
+        assert got == _ms(r.cpu().numpy(), t.cpu().numpy())
+    small = total // 2
+    rows2 = torch.full((small, 3), -7, dtype=torch.int64, device=cuda)
+    times2 = torch.full((small,), -7.0, dtype=torch.float64, device=cuda)
+    eng.pack_rows(rows2, times2, meta)
+    assert int(meta[M]) == total
+    assert (rows2 >= 0).all()
+    assert eng.state([])["status"] & N.CCC_ST_OUT_OVERFLOW
+    eng.close()
