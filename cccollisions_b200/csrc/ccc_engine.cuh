@@ -656,7 +656,7 @@ static __global__ void k_engine_refit_front(Forest F, const int* __restrict__ np
 }
 
 // Continuous-collision candidates of resident trees: one query leaf per thread walks the
-// QNodes with an explicit stack in shared memory, tests the 4 slot boxes of a node at once
+// QNodes with an explicit per-thread stack (local memory), tests the 4 slot boxes of a node at once
 // (fp32; the query box is the leaf's own outward-rounded slot box), keeps the reference's
 // order rule (a slot is skipped when its rightmost leaf position is not after the query's,
 // so each unordered pair is found once) and emits (min id, max id) in data slots.  Candidates
