@@ -296,3 +296,35 @@ def test_engine_full_size_meshes_match_reference_format_path(cuda):
         got = eng.collisions(sid, int(n))
         assert _ms(got[0].cpu().numpy(), got[1].cpu().numpy()) == _ms(r[:k], times[0, :k, 0].cpu().numpy())
     eng.close()
+
+
+def test_refit_across_block_ranges_matches_oracle(cuda, oracle):
+    """Many small meshes beside larger ones, so that blocks of the block-local refit pass
+    straddle mesh boundaries and hand climbs of every size to the second pass; after a
+    change of positions (refit only, no rebuild) the rows equal the oracle's for the new
+    positions."""
+    from cccollisions_b200 import _native as N
+    from cccollisions_b200 import workloads as W
+    g = np.random.default_rng(9)
+    meshes = []
+    for i in range(40):
+        nx, ny = (int(g.integers(2, 5)), int(g.integers(2, 5))) if i % 5 else (int(g.integers(12, 30)), 14)
+        meshes.append(W.jittered_fold(400 + i, nx, ny))
+    with N.math_library(N.LIB_PORTABLE):
+        eng, sids = _engine(meshes, max_candidates_per_triangle=32)     # about 18 pairs a triangle
+        eng.set_active(sids)
+        eng.build(sids)
+        moved = []
+        for sid, (x0, x1, _) in zip(sids, meshes):
+            x1b = x0 + 1.3 * (x1 - x0)
+            eng.upload_soup(sid, x0, x1b)
+            moved.append((x0, x1b))
+        eng.ccd()
+        st = eng.state(sids)
+        assert st["status"] == 0
+        for sid, (x0, x1), n in zip(sids, moved, st["rows"]):
+            rows, times = eng.collisions(sid, int(n))
+            bb, tr = oracle.bvh(x0, x1)
+            er, et = oracle.ccd(bb, tr, x0, x1)
+            assert _ms(rows.cpu().numpy(), times.cpu().numpy()) == _ms(er, et)
+        eng.close()
