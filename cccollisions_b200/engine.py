@@ -280,6 +280,8 @@ class StepPipeline:
         self._rows = [torch.empty((max(self.capacity, 1), 3), dtype=torch.int64, device=dev) for _ in range(2)]
         self._times = [torch.empty(max(self.capacity, 1), dtype=engine.dtype, device=dev) for _ in range(2)]
         self._meta = [torch.empty(2 * self.M + 2, dtype=torch.int32, device=dev) for _ in range(2)]
+        # page-locked copies the host reads the counts from (step k in slot k % 2)
+        self._meta_h = [torch.empty(2 * self.M + 2, dtype=torch.int32).pin_memory() for _ in range(2)]
         self.compute = torch.cuda.Stream(dev)
         self.copy_in = torch.cuda.Stream(dev)
         self.copy_out = torch.cuda.Stream(dev)
@@ -292,9 +294,9 @@ class StepPipeline:
 
     def run(self, inputs, outputs) -> list[int]:
         """inputs[k]: one (x0, x1) pair of page-locked host tensors per mesh (order of sids)
-        for step k; outputs[k]: (rows, times, meta) page-locked host tensors from
-        host_outputs() that receive step k's rows (the same buffers may serve several steps
-        when the caller does not need the earlier ones).  meta = [row offset of each mesh in
+        for step k; outputs[k]: (rows, times, meta) host tensors from host_outputs() that
+        receive step k's rows (the same triple may serve several steps; each then holds the
+        last of them).  meta = [row offset of each mesh in
         slot order, total, slot ids, status word].  Returns the row count of every step;
         raises if a step's status word reports an error."""
         e, K = self.e, len(inputs)
@@ -317,9 +319,11 @@ class StepPipeline:
         def download(k):
             done[k].synchronize()
             rows_h, times_h, meta_h = outputs[k]
-            n = min(int(meta_h[self.M]), self.capacity)
-            totals[k] = int(meta_h[self.M])
-            status[k] = int(meta_h[2 * self.M + 1])
+            meta = self._meta_h[k % 2]
+            meta_h.copy_(meta)
+            n = min(int(meta[self.M]), self.capacity)
+            totals[k] = int(meta[self.M])
+            status[k] = int(meta[2 * self.M + 1])
             with torch.cuda.stream(self.copy_out):
                 self.copy_out.wait_event(done[k])
                 if n:
@@ -343,7 +347,7 @@ class StepPipeline:
                 if k >= 2:
                     self.compute.wait_event(down[k - 2])
                 e.pack_rows(self._rows[k % 2], self._times[k % 2], self._meta[k % 2])
-                outputs[k][2].copy_(self._meta[k % 2], non_blocking=True)
+                self._meta_h[k % 2].copy_(self._meta[k % 2], non_blocking=True)
                 done[k].record(self.compute)
             if k + 1 < K:
                 upload(k + 1)

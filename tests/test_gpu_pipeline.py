@@ -67,6 +67,14 @@ def test_pipeline_steps_equal_single_steps(cuda, graph):
             got = _ms(rows[off[m]:off[m + 1]], times[off[m]:off[m + 1]])
             assert got == expect[i][sid], (k, sid)
     assert np.array_equal(eng.view(spare)["x0"].cpu().numpy(), spare_x0)
+    # one output triple for every step: it ends up holding the last step
+    one = pipe.host_outputs()
+    totals = pipe.run([host[i] for i in order], [one] * len(order))
+    rows, times, meta = [o.numpy() for o in one]
+    off, ids = meta[:M + 1], meta[M + 1:2 * M + 1]
+    assert off[M] == totals[-1]
+    for m, sid in enumerate(ids.tolist()):
+        assert _ms(rows[off[m]:off[m + 1]], times[off[m]:off[m + 1]]) == expect[order[-1]][sid]
     eng.close()
 
 
