@@ -54,6 +54,11 @@ UNIT = "triangle-steps/s"
 MAXC, MAXCOL = 32, 16            # no candidate overflow on any of the 64 meshes
 FP64_PEAK_NOMINAL_GFLOPS = 37000.0   # B200 FP64 datasheet figure (not measured here)
 FLOPS_PER_SUBTEST = 252          # coefficients 162 + Cardano and filter 90 (transcendentals as 1)
+# DRAM bytes (read + write) of one k_ccd_narrow launch per candidate pair, from ncu's
+# dram__bytes_read.sum + dram__bytes_write.sum on the 16-mesh batched step (74.6 MB + 4.8 MB
+# for 3,091,227 pairs); the 64-mesh launch is too large for a full capture, so its traffic
+# is this figure times its own pair count.
+NARROW_DRAM_BYTES_PER_PAIR = (74.574848e6 + 4.76416e6) / 3091227
 
 
 def parse():
@@ -337,7 +342,11 @@ def run_ours(args, rank, world, dev):
                     "rows_equal_batched": bool(e2e_equal)},
             "roofline": {"kernel": dname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                         "traffic": None, "alg_bytes_per_launch": narrow_bytes, "launch_ms": per_launch,
+                         "traffic": (NARROW_DRAM_BYTES_PER_PAIR * cnt["candidates"]) if dname == "k_ccd_narrow"
+                         else None,
+                         "traffic_source": "ncu DRAM bytes per candidate pair of the 16-mesh capture, times this "
+                                           "launch's pairs",
+                         "alg_bytes_per_launch": narrow_bytes, "launch_ms": per_launch,
                          "note": "the narrow phase is FP64-latency bound; see fp64"},
             "fp64": {"kernel": "k_ccd_narrow", "achieved_gflops": fp64_gflops,
                      "peak_gflops": FP64_PEAK_NOMINAL_GFLOPS, "peak_source": "nominal (B200 datasheet)",
