@@ -57,7 +57,7 @@ def valid(rows):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", default=os.path.join(ROOT, "golden_out"))
     ap.add_argument("--full", action="store_true", help="also compare full-size workloads (report only)")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)

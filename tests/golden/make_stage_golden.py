@@ -49,7 +49,7 @@ def tets_of(x0, x1, items):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", default=os.path.join(ROOT, "golden_out"))
     ap.add_argument("--per-source", type=int, default=4000)
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)

@@ -35,7 +35,7 @@ MC = 32
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", default=os.path.join(ROOT, "golden_out"))
     ap.add_argument("--extra-seeds", type=int, nargs="*", default=[],
                     help="further jittered folds (fp32 and fp64) to record, beside the fixed cases")
     args = ap.parse_args()
