@@ -58,6 +58,13 @@ def test_engine_sizes_are_pure_host(native_lib):
     # argument errors before any device work
     assert native_lib.ccc_engine_create(1, 1000, 0, 4, 16, 16, None, 0, None, None) == 1
     assert native_lib.ccc_engine_ccd(None, None) == 1
+    assert native_lib.ccc_engine_pack_rows(None, None, None, 0, None, None) == 1
+    # triangle-edge queries: bad dtype, too few triangles, missing outputs
+    te = (native_lib.ccc_find_triangle_edge_collisions, native_lib.ccc_find_triangle_edge_candidates2)
+    assert native_lib.ccc_find_triangle_edge_collisions(7, None, None, None, 1, 4, 16, None, None, None, 0, None) == 1
+    assert native_lib.ccc_find_triangle_edge_candidates(1, None, None, None, 1, 1, 16, None, None, 0, None) == 1
+    for f in te:
+        assert f(1, None, None, None, 1, 4, 16, None, None, None, 0, None) == 1
 
 
 def test_api_mirrors_reference_signatures():
