@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--meshes", type=int, default=64)
     ap.add_argument("--served-requests", type=int, default=160)
     ap.add_argument("--served-plain-sample", type=int, default=12)
+    ap.add_argument("--served-budget-gb", type=int, default=40,
+                    help="device-memory budget of the served engine (the workload's is 40 GB)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     return ap.parse_args()
 
@@ -402,7 +404,7 @@ def run_served(args, dev):
     from cccollisions_b200 import workloads as W
     from cccollisions_b200.serve import Request, Server, requests_from_stream
     reqs = requests_from_stream(W.served_stream(num_requests=args.served_requests, rate=2000.0))
-    srv = Server(budget_bytes=40 << 30, device=dev)
+    srv = Server(budget_bytes=args.served_budget_gb << 30, device=dev)
     for r in reqs:
         srv._pin(r)
     st = srv.run(reqs)
@@ -412,7 +414,7 @@ def run_served(args, dev):
     k = max(1, len(reqs) // max(1, args.served_plain_sample))
     sample = reqs[::k][:max(1, args.served_plain_sample)]
     copies = [Request(r.verts0, r.verts1, r.vel, r.faces, r.masses, rid=r.rid) for r in sample]
-    srv = Server(budget_bytes=40 << 30, device=dev)
+    srv = Server(budget_bytes=args.served_budget_gb << 30, device=dev)
     for r in copies:
         srv._pin(r)
     same = srv.run(copies, realtime=False)
@@ -427,7 +429,7 @@ def run_served(args, dev):
     return {"value": st["throughput"], "unit": UNIT, "requests": st["requests"], "rate_per_s": 2000.0,
             "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "makespan_s": st["makespan_s"],
             "request_triangles": st["triangles"], "ticks": st["ticks"], "mean_iterations": st["mean_iterations"],
-            "converged_fraction": st["converged"], "budget_gb": 40,
+            "converged_fraction": st["converged"], "budget_gb": args.served_budget_gb,
             "policy": f"FIFO admission, at most {srv.max_active_triangles} active triangles (a request alone is "
                       "always admitted)",
             "request": "impulse loop (max 50 iterations) on an impulse-workload mesh of log-uniform 2e3..2e5 "
