@@ -608,10 +608,11 @@ template <class T> __device__ __forceinline__ bool ccd_filter(const MTet<T>& tet
         T p = dot(cross(dc, da), cross(da, db)) / norm2(cross(da, db));
         if (s < 0 || s > 1 || p < 0 || p > 1) return false;
         return true;
-    } else if (k < 12) {
-        return is_inside(p0, p1, p2, p3);
     }
-    return is_inside(p1, p2, p3, p0);
+    // face then vertex: (p0, p1, p2 | p3) for k < 12, (p1, p2, p3 | p0) after, picked by
+    // selects so that both kinds run one code path
+    const bool inv = k >= 12;
+    return is_inside(inv ? p1 : p0, inv ? p2 : p1, inv ? p3 : p2, inv ? p0 : p3);
 }
 
 // ------------------------------------------------------------------ impulses

@@ -595,7 +595,8 @@ template <class T> struct CornerSink {
 // every warp of the block runs the same phase's code at the same time:
 //   (1) cubic coefficients and the solver prefix of every sub-test, which classifies it;
 //   (2) the roots, with the sub-tests ordered by solver branch;
-//   (3) the root filter and the output of every root in [0, 1].
+//   (3) the root filter and the output of every root in [0, 1], edge-edge roots first and
+//       vertex-face roots after them, so that a warp runs one of the two filters.
 // Sub-tests take different branches and have 0 to 3 roots: solved in arrival order they
 // leave most lanes idle, and a kernel whose warps are in different phases needs all of its
 // code in the instruction cache at once.  Queued batches are always full, so no phase runs
@@ -631,7 +632,8 @@ template <class T> struct CcdLayout {
 };
 
 // slots of the small int area
-// (class counts and root count come in two sets, used by alternate batches)
+// (class counts and root counts come in two sets, used by alternate batches; each set of
+// root counts holds the edge-edge and the vertex-face count)
 enum CcdInts { CI_WARP = 0, CI_TOTAL = 32, CI_COUNT = 33, CI_ROOTS = 41 };
 
 // a queued sub-test: triangle slots i and j, type k in the top bits of j (slots < 2^28)
@@ -675,7 +677,7 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
     // (the staging barriers order the initial clearing before the first batch)
     int par = 0;
     if (tid < 8) ints[CI_COUNT + tid] = 0;
-    if (tid < 2) ints[CI_ROOTS + tid] = 0;
+    if (tid < 4) ints[CI_ROOTS + tid] = 0;
     for (long long base = (long long)blockIdx.x * CCD_BLOCK;; base += (long long)gridDim.x * CCD_BLOCK) {
         const bool more = base < n;
         if (!more && queued == 0) break;
@@ -762,35 +764,44 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                 }
             }
             __syncthreads();
-            // (2) roots; the ones in [0, 1] go to the root list
+            // (2) roots; the ones in [0, 1] go to the root list, edge-edge roots from its
+            // front and vertex-face roots from its back
             for (int j0 = 0; j0 < nsolve; j0 += CCD_BLOCK) {
                 const int j = j0 + tid;
                 T rr[3] = {(T)-1, (T)-1, (T)-1};
                 int ri = 0;
+                bool ee = false;
                 if (j < nsolve) {
                     int cc = (j >= o1) + (j >= o2) + (j >= o3);
                     ri = clist[j];
+                    ee = ((items[(head + ri) % Q].y >> 28) & 15) < 9;
                     class_roots<T, LIB>(cc + 1, rec[0 * NB + ri], rec[1 * NB + ri], rec[2 * NB + ri], rec[3 * NB + ri],
                                         rec[4 * NB + ri], rec[5 * NB + ri], rr);
                 }
 #pragma unroll
                 for (int s = 0; s < 3; ++s) {
                     bool keep = j < nsolve && (rr[s] >= 0 && rr[s] <= 1);
-                    unsigned m = __ballot_sync(FULL, keep);
-                    int at = 0;
-                    if (lane == 0 && m) at = atomicAdd(&ints[CI_ROOTS + par], __popc(m));
-                    at = __shfl_sync(FULL, at, 0) + __popc(m & lt);
+                    unsigned me = __ballot_sync(FULL, keep && ee);
+                    unsigned mf = __ballot_sync(FULL, keep && !ee);
+                    int ae = 0, af = 0;
+                    if (lane == 0 && me) ae = atomicAdd(&ints[CI_ROOTS + 2 * par], __popc(me));
+                    if (lane == 0 && mf) af = atomicAdd(&ints[CI_ROOTS + 2 * par + 1], __popc(mf));
+                    ae = __shfl_sync(FULL, ae, 0) + __popc(me & lt);
+                    af = __shfl_sync(FULL, af, 0) + __popc(mf & lt);
                     if (keep) {
+                        const int at = ee ? ae : 3 * NB - 1 - af;
                         root_rec[at] = (unsigned short)ri;
                         root_val[at] = rr[s];
                     }
                 }
             }
             __syncthreads();
-            const int nroots = ints[CI_ROOTS + par];
+            const int nee = ints[CI_ROOTS + 2 * par];
+            const int nroots = nee + ints[CI_ROOTS + 2 * par + 1];
             if (tid == 0 && nroots) atomicAdd(&hdr->roots, nroots);
             // (3) filter and output
-            for (int j = tid; j < nroots; j += CCD_BLOCK) {
+            for (int jj = tid; jj < nroots; jj += CCD_BLOCK) {
+                const int j = jj < nee ? jj : 3 * NB - 1 - (jj - nee);
                 int2 it = items[(head + root_rec[j]) % Q];
                 int k = (it.y >> 28) & 15;
                 int2 q = make_int2(it.x, it.y & 0x0fffffff);
@@ -817,7 +828,7 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                 }
             }
             if (tid < 4) ints[CI_COUNT + 4 * (par ^ 1) + tid] = 0;
-            if (tid == 4) ints[CI_ROOTS + (par ^ 1)] = 0;
+            if (tid >= 4 && tid < 6) ints[CI_ROOTS + 2 * (par ^ 1) + tid - 4] = 0;
             par ^= 1;
             head = (head + nb) % Q;
             queued -= nb;
