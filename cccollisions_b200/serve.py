@@ -117,6 +117,8 @@ class Server:
     def run(self, requests: list[Request], realtime: bool = True) -> dict:
         """Serve the requests (arrival times in seconds from now when realtime, else all at
         once); returns throughput and latency statistics.  Results are stored on each request."""
+        if not requests:
+            raise ValueError("no requests to serve")
         for r in requests:
             if not r._pinned:
                 self._pin(r)
