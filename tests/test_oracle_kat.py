@@ -3,8 +3,8 @@
 The reference ships no tests or golden vectors, so the oracle's restatement is pinned by
 hand-derived values: Morton interleaving, the Karras topology over all-equal keys, the
 reference's unbounded-scene-box quirk, each branch of the cubic solver, analytic times of
-impact, the separating-axis test on known configurations, CAMPARY products against exact
-rational arithmetic, and O(F^2) brute force for candidate pairs.
+impact, the separating-axis test and proximity on known configurations, CAMPARY products
+against exact rational arithmetic, and O(F^2) brute force for candidate pairs.
 """
 import math
 from fractions import Fraction
@@ -235,6 +235,35 @@ def test_sat_known_configurations(oracle):
     assert oracle.sat(a, a + [0.1, 0.1, 0])
     assert not oracle.sat(a, a + [2.0, 0, 0])
     assert oracle.sat(a.astype(np.float32), pierce.astype(np.float32))
+
+
+# ----------------------------------------------------------------------------- proximity
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_proximity_parallel_triangles(oracle, dtype):
+    """Triangle 1 lies h above triangle 0, parallel and inside its outline
+    (proximity_static.cu:11-508).  Within the threshold, at distance h:
+    * faces against vertices (k = 9, 10, 11): every vertex of triangle 1 projects inside
+      triangle 0; triangle 0's vertices lie 0.2 outside triangle 1's box, so k = 12..14
+      fail the sub-box test;
+    * no edge pair (k = 3 * e0 + e1, edges 01, 02, 12): triangle 0's edge 12 (x + y = 1)
+      passes over the lines of edges 01 and 02 of triangle 1 beyond their ends (t = 1.5,
+      k = 6, 7); the two edges 12 are parallel (NaN s and t, the point-segment fallback)
+      and sqrt(0.02 + h^2) = 0.15 apart, beyond the threshold (k = 8); the other edge
+      pairs are 0.2 apart in x or y and fail the sub-box test."""
+    h, th = 0.05, 0.1
+    x = np.array([[[0, 0, 0], [1, 0, 0], [0, 1, 0]],
+                  [[0.2, 0.2, h], [0.6, 0.2, h], [0.2, 0.6, h]]], dtype=dtype)
+    bb, tr = oracle.bvh(x)
+    rows, dist = oracle.proximity(bb, tr, x, th)
+    got = sorted(map(tuple, rows.tolist()))
+    assert got == [(0, 1, k) for k in (9, 10, 11)]
+    np.testing.assert_allclose(dist, h, rtol=1e-6)
+    # below the height nothing is close enough; a threshold of 0.2 adds the parallel edges
+    assert len(oracle.proximity(bb, tr, x, 0.04)[0]) == 0
+    wide, wdist = oracle.proximity(bb, tr, x, 0.2)
+    assert (0, 1, 8) in set(map(tuple, wide.tolist()))
+    np.testing.assert_allclose(wdist[wide[:, 2] == 8], np.sqrt(0.02 + h * h), rtol=1e-6)
 
 
 # ----------------------------------------------------------------------------- brute force
