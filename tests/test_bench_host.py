@@ -53,3 +53,13 @@ def test_default_run_length(monkeypatch):
     a = bench.parse()
     assert a.gpus == 1 and a.impl == "ours"
     assert a.warmup >= 3 and a.steps >= 1
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    """Under torchrun only rank 0 runs the reference arm; the other ranks print nothing."""
+    import subprocess
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2"],
+                       env=env, capture_output=True, text=True, timeout=120)
+    assert p.returncode == 0, p.stderr
+    assert p.stdout.strip() == ""
