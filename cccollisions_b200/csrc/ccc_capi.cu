@@ -32,7 +32,7 @@ int num_sms() {
 }
 
 // ---- launch accounting and optional per-kernel event timing ----
-int64_t g_launches = 0;
+std::atomic<int64_t> g_launches{0};
 // elementary functions of the continuous-collision solver (MathLib); CUDA's own by default,
 // which is what the reference calls
 int g_math_lib = LIB_REFERENCE;

@@ -10,6 +10,8 @@
 // rounded outward to fp32 plus child references, so one node visit is four 16-byte loads.
 #pragma once
 
+#include <atomic>
+
 #include <cooperative_groups.h>
 #include <cooperative_groups/reduce.h>
 #include "ccc_geom.cuh"
@@ -839,14 +841,16 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
 
 // Launch of k_ccd_narrow with its dynamic shared memory (the size is raised once per
 // instantiation and device; prepare_ccd_narrow does it ahead of any stream capture).
+// The flags are atomic because host threads may launch on different streams at once; two
+// first calls may both set the attribute, which is harmless.
 template <class T, int MODE, class Sink, int LIB> inline cudaError_t prepare_ccd_narrow() {
-    static bool done[64] = {false};
+    static std::atomic<bool> done[64];
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
+    if (dev >= 0 && dev < 64 && done[dev].load(std::memory_order_acquire)) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(k_ccd_narrow<T, MODE, Sink, LIB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)CcdLayout<T>::bytes);
-    if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
+    if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev].store(true, std::memory_order_release);
     return e;
 }
 

@@ -9,9 +9,12 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 namespace ccc {
 
-extern int64_t g_launches;
+// launches since load (exact when one host thread launches at a time)
+extern std::atomic<int64_t> g_launches;
 // elementary functions of the continuous-collision solver (MathLib)
 extern int g_math_lib;
 

@@ -17,6 +17,11 @@
  *   - Return value: 0 on success or a CCC_ERR_* code for argument / launch errors.
  *     Capacity overflows are reported through the status word (bits below), as the
  *     reference prints a warning and truncates.
+ *   - Threads: the entry points may be called from several host threads at once, each
+ *     with its own workspace (and stream); ccc_find_collisions_continuous_static shares one
+ *     device array between its calls.  The math-library mode and the timing hooks are
+ *     process-wide settings: set them while no other thread is launching.  The launch
+ *     count is exact when one thread launches at a time.
  */
 #ifndef CCC_B200_H
 #define CCC_B200_H
