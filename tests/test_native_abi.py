@@ -24,6 +24,50 @@ def test_header_declares_the_reference_entry_points():
         assert n in names
 
 
+def _declarations():
+    """(name, [parameter text]) of every function the headers declare."""
+    out = []
+    for h in ("ccc_b200.h", "ccc_engine.h"):
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"\b(ccc_[a-z0-9_]+)\s*\(([^)]*)\)\s*;", src):
+            args = m.group(2).strip()
+            out.append((m.group(1), [] if args in ("", "void") else args.split(",")))
+    return out
+
+
+def _c_kind(param):
+    if "*" in param:
+        return "pointer"
+    if "int64_t" in param:
+        return "int64"
+    if "double" in param:
+        return "double"
+    if re.search(r"\b(int|int32_t)\b", param):
+        return "int32"
+    return "unknown: " + param
+
+
+def _ctypes_kind(t):
+    import ctypes
+    if t in (ctypes.c_void_p, ctypes.c_char_p) or isinstance(getattr(t, "_type_", None), type):
+        return "pointer"
+    return {ctypes.c_int64: "int64", ctypes.c_int32: "int32", ctypes.c_double: "double"}.get(t, str(t))
+
+
+def test_ctypes_signatures_match_the_headers():
+    """Every ctypes signature the package binds has the header's parameter count and, per
+    parameter, the same kind (pointer, 64-bit integer, 32-bit integer, double)."""
+    from cccollisions_b200 import _native
+    decls = _declarations()
+    assert len(decls) == len(_declared_functions())
+    for name, params in decls:
+        sig = _native.SIGNATURES[name][1]
+        assert len(sig) == len(params), name
+        for i, (p, t) in enumerate(zip(params, sig)):
+            assert _c_kind(p) == _ctypes_kind(t), (name, i, p, t)
+
+
 def test_library_exports_every_declared_symbol(native_lib):
     from cccollisions_b200 import _native
     for name in _declared_functions():
