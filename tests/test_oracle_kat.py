@@ -222,6 +222,33 @@ def test_ccd_shared_vertex_rejected(oracle):
     assert len(oracle.mincol_cand(bb, tr, x0, x1)) == 0
 
 
+def test_root_filter_known_answers(oracle):
+    """filterCollisions / is_inside (collisions_continuous.cu:615-684) on static tetrahedra
+    (zero displacement, so the points at the root are the points themselves).  Edge-edge:
+    the closest-point parameters s, p of the two lines must lie in [0, 1]; vertex-face: the
+    barycentrics of the vertex's projection on the face's plane must lie in [0, 1].  A NaN
+    parameter fails no comparison and passes."""
+    dv = [[0, 0, 0]] * 4
+    # edge-edge (k < 9): edge (p0, p1) against edge (p2, p3)
+    crossing = [[0, 0, 0], [1, 0, 0], [0.5, -0.5, 0], [0.5, 0.5, 0]]
+    assert oracle.ccd_filter(_tet(crossing, dv), 0, 0.5)
+    beyond = [[0, 0, 0], [1, 0, 0], [1.5, -0.5, 0], [1.5, 0.5, 0]]          # s = 1.5
+    assert not oracle.ccd_filter(_tet(beyond, dv), 0, 0.5)
+    parallel = [[0, 0, 0], [1, 0, 0], [0, 1, 0], [1, 1, 0]]                # |da x db| = 0: NaN
+    assert oracle.ccd_filter(_tet(parallel, dv), 4, 0.5)
+    # vertex-face: face (p0, p1, p2) and vertex p3 for k = 9..11
+    face = [[0, 0, 0], [1, 0, 0], [0, 1, 0]]
+    assert oracle.ccd_filter(_tet(face + [[0.2, 0.2, 0.3]], dv), 9, 0.5)    # projection inside
+    assert not oracle.ccd_filter(_tet(face + [[0.8, 0.8, 0.0]], dv), 10, 0.5)
+    point = [[0.3, 0.3, 0.0]] * 3                                          # degenerate face: NaN
+    assert oracle.ccd_filter(_tet(point + [[5.0, 5.0, 5.0]], dv), 11, 0.5)
+    # k = 12..14: vertex p0 and face (p1, p2, p3)
+    assert oracle.ccd_filter(_tet([[0.2, 0.2, -0.3]] + face, dv), 12, 0.5)
+    assert not oracle.ccd_filter(_tet([[-0.1, 0.5, 0.0]] + face, dv), 13, 0.5)
+    # roots below -1e-16 are rejected before any test
+    assert not oracle.ccd_filter(_tet(crossing, dv), 0, -0.5)
+
+
 # ----------------------------------------------------------------------------- static SAT
 
 def test_sat_known_configurations(oracle):
