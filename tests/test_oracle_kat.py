@@ -249,6 +249,28 @@ def test_root_filter_known_answers(oracle):
     assert not oracle.ccd_filter(_tet(crossing, dv), 0, -0.5)
 
 
+def test_contact_kinematics_known_answers(oracle):
+    """compute_coeficients_and_directions (collisions_impulses.cu:162-543): the normal of
+    the tetrahedron's first two edges at the root, turned from side 0 to side 1 (by the
+    points at the start), the normal velocity, and the mass pair mixed by the contact
+    parameters.  Output: (normal xyz, normal velocity, mass 0, mass 1)."""
+    q = [1.0, 2.0, 3.0, 4.0]
+    face = [[0, 0, 0], [1, 0, 0], [0, 1, 0]]
+    still = [[0, 0, 0]] * 3
+    # vertex above the face falling onto it (k = 9): barycentrics (0.6, 0.2, 0.2) of the
+    # face's points, face mass 3 * 0.2 + 1 * 0.6 + 2 * 0.2
+    o = oracle.contact(_tet(face + [[0.2, 0.2, 0.1]], still + [[0, 0, -0.2]]), 9, 0.5, q)
+    np.testing.assert_allclose(o, [0, 0, 1, -0.2, 1.6, 4.0], atol=1e-12)
+    # vertex below the face rising onto it (k = 12: vertex first); the normal comes out
+    # turned back towards the face's side and the masses swap sides
+    o = oracle.contact(_tet([[0.2, 0.2, -0.1]] + face, [[0, 0, 0.2]] + still), 12, 0.5, q)
+    np.testing.assert_allclose(o, [0, 0, 1, -0.2, 1.0, 4 * 0.2 + 2 * 0.6 + 3 * 0.2], atol=1e-12)
+    # parallel edges (|da x db|^2 < 1e-15): s = t = 0.5, masses (q0 + q1) / 2, (q2 + q3) / 2
+    ee = [[0, 0, 0], [1, 0, 0], [0, 0, 0.1], [1, 0, 0.1]]
+    o = oracle.contact(_tet(ee, [[0, 0, 0], [0, 0, 0], [0, -0.1, 0], [0, -0.1, 0]]), 0, 0.0, q)
+    np.testing.assert_allclose(o, [0, -1, 0, 0.1, 1.5, 3.5], atol=1e-12)
+
+
 # ----------------------------------------------------------------------------- static SAT
 
 def test_sat_known_configurations(oracle):
