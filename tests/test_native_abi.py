@@ -142,3 +142,21 @@ def test_api_rejects_cpu_tensors():
     t = torch.zeros((1, 4, 3, 3))
     with pytest.raises(RuntimeError, match="CUDA"):
         C.bvh(t)
+
+
+def test_served_engine_capacity_fits_the_budget(native_lib):
+    """The server sizes its engine block from a device-memory budget (pure host): the
+    largest triangle capacity whose block fits, so one triangle more does not fit (or
+    exceeds the engine's limits)."""
+    import torch
+    from cccollisions_b200.serve import engine_capacity
+    prev = 0
+    for gb in (1, 2, 40):
+        budget = gb << 30
+        tc, vc = engine_capacity(budget, torch.float64, mesh_capacity=4096, vert_ratio=0.75, maxc=16)
+        assert tc > prev
+        prev = tc
+        assert vc == int(tc * 0.75) + 16
+        assert 0 < native_lib.ccc_engine_bytes(1, tc, vc, 4096, 16, 1) <= budget
+        over = native_lib.ccc_engine_bytes(1, tc + 1, int((tc + 1) * 0.75) + 16, 4096, 16, 1)
+        assert over > budget or over == -1
