@@ -13,6 +13,9 @@ LIB_PATH = os.path.join(_HERE, "libccc_b200.so")
 
 # return codes / status bits (mirrors include/ccc_b200.h)
 CCC_OK = 0
+CCC_ERR_INVALID_ARG = 1
+CCC_ERR_WORKSPACE = 2
+CCC_ERR_CUDA = 3
 CCC_ERR_TOO_LARGE = 4
 LIB_REFERENCE = 0
 LIB_PORTABLE = 1
@@ -52,6 +55,8 @@ SIGNATURES = {
     "ccc_compute_impulses": (_I, [_I, _P, _P, _P, _P, _P, _P, _I64, _I64, _I64, _I64, _P, _P, _P, _P, _I64, _P]),
     "ccc_static_scratch_bytes": (_I64, []),
     "ccc_find_collisions_continuous_static": (_I, [_I, _P, _P, _P, _P, _P, _I64, _I64, _I64, _I64, _P, _P, _P]),
+    "ccc_static_scratch_read_status": (_I, [_I64, _P, _P]),
+    "ccc_static_scratch_read_counters": (_I, [_P, _P]),
     "ccc_compute_impulses_from_collisions": (_I, [_I, _P, _P, _I64, _I64, _P, _P, _P, _I64, _P, _P, _P, _P, _I64,
                                                  _P]),
     # resident engine (include/ccc_engine.h)

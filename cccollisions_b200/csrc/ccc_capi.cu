@@ -102,9 +102,19 @@ inline int narrow_grid() { return num_sms() * NARROW_MIN_BLOCKS; }
 int check_common(int dtype, int64_t B, int64_t F) {
     if (dtype != 0 && dtype != 1) return CCC_ERR_INVALID_ARG;
     if (B < 1 || F < 2) return CCC_ERR_INVALID_ARG;
-    // int32 indexing inside the kernels (and headroom for the Karras range doubling)
-    if (B * F >= (int64_t)1 << 28) return CCC_ERR_INVALID_ARG;
+    // int32 indexing inside the kernels (and headroom for the Karras range doubling); each
+    // factor is bounded first so that the product cannot wrap
+    const int64_t lim = (int64_t)1 << 28;
+    if (B >= lim || F >= lim || B * F >= lim) return CCC_ERR_INVALID_ARG;
     return CCC_OK;
+}
+
+// True when B * F * per * k rows stay below 2^31 (int32 row indices in the kernels).  The
+// test divides instead of multiplying, so a huge per-triangle capacity cannot wrap the
+// product; B * F < 2^28 (check_common) and k <= 15 keep the divisor in range.
+bool rows_fit(int64_t B, int64_t F, int64_t per, int64_t k = 1) {
+    if (per < 1) return false;
+    return per <= ((((int64_t)1 << 31) - 1) / (B * F * k));
 }
 
 struct Prepared {
@@ -249,7 +259,7 @@ int te_entry(int dtype, const void* bboxes, const int64_t* tree, const void* tri
     if (!bboxes || !tree || !triangles || !rows || max_collisions < 1) return CCC_ERR_INVALID_ARG;
     if (OP == TE_COLLISIONS && !coefs) return CCC_ERR_INVALID_ARG;
     if (OP == TE_CANDIDATES2 && !masks) return CCC_ERR_INVALID_ARG;
-    if (B * F * max_collisions >= ((int64_t)1 << 31)) return CCC_ERR_INVALID_ARG;
+    if (!rows_fit(B, F, max_collisions)) return CCC_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     return dtype == 0 ? te_impl<float, OP>(bboxes, tree, triangles, B, F, max_collisions, rows, coefs, masks, ws,
                                            ws_bytes, s)
@@ -422,9 +432,11 @@ const char* ccc_error_string(int code) {
 }
 
 int64_t ccc_workspace_size(int op, int64_t B, int64_t F, int64_t maxc) {
-    if (B < 1 || F < 2) return -1;
+    if (check_common(0, B, F) != CCC_OK) return -1;
     bool nodes = !(op == CCC_OP_BVH);
-    return layout(B, F, nodes ? std::max<int64_t>(maxc, 1) : 0, nodes).end;
+    int64_t per = nodes ? std::max<int64_t>(maxc, 1) : 0;
+    if (nodes && !rows_fit(B, F, per)) return -1;
+    return layout(B, F, per, nodes).end;
 }
 
 int ccc_read_status(const void* ws, int64_t n_mesh, int32_t* out, void* stream) {
@@ -467,7 +479,7 @@ int ccc_find_collisions(int dtype, const void* bboxes, const int64_t* tree, cons
     int rc = check_common(dtype, B, F);
     if (rc) return rc;
     if (!bboxes || !tree || !triangles || !out || max_collisions < 1) return CCC_ERR_INVALID_ARG;
-    if (B * F * max_collisions >= ((int64_t)1 << 31)) return CCC_ERR_INVALID_ARG;
+    if (!rows_fit(B, F, max_collisions)) return CCC_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     return dtype == 0 ? static_impl<float>(bboxes, tree, triangles, B, F, threshold, max_collisions, out, ws, ws_bytes, s)
                       : static_impl<double>(bboxes, tree, triangles, B, F, threshold, max_collisions, out, ws, ws_bytes, s);
@@ -502,7 +514,7 @@ int ccc_find_collisions_continuous(int dtype, const void* bboxes, const int64_t*
     if (rc) return rc;
     if (!bboxes || !tree || !triangles || !triangles_next || !out_rows || !out_times || maxc < 1 || maxcol < 1)
         return CCC_ERR_INVALID_ARG;
-    if (B * F * std::max(maxc, maxcol) >= ((int64_t)1 << 31)) return CCC_ERR_INVALID_ARG;
+    if (!rows_fit(B, F, maxc) || !rows_fit(B, F, maxcol)) return CCC_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     return dtype == 0 ? ccd_impl<float>(bboxes, tree, triangles, triangles_next, mask, B, F, maxc, maxcol, out_rows,
                                         out_times, ws, ws_bytes, s)
@@ -516,7 +528,7 @@ int ccc_find_mincol_cand(int dtype, const void* bboxes, const int64_t* tree, con
     int rc = check_common(dtype, B, F);
     if (rc) return rc;
     if (!bboxes || !tree || !triangles || !triangles_next || !out_rows || max_collisions < 1) return CCC_ERR_INVALID_ARG;
-    if (B * F * max_collisions * 15 >= ((int64_t)1 << 31)) return CCC_ERR_INVALID_ARG;
+    if (!rows_fit(B, F, max_collisions, 15)) return CCC_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     return dtype == 0 ? mincol_impl<float>(bboxes, tree, triangles, triangles_next, B, F, max_collisions, out_rows, ws,
                                            ws_bytes, s)
@@ -530,7 +542,7 @@ int ccc_find_proximity(int dtype, const void* bboxes, const int64_t* tree, const
     int rc = check_common(dtype, B, F);
     if (rc) return rc;
     if (!bboxes || !tree || !triangles || !out_rows || maxc < 1) return CCC_ERR_INVALID_ARG;
-    if (B * F * maxc >= ((int64_t)1 << 31)) return CCC_ERR_INVALID_ARG;
+    if (!rows_fit(B, F, maxc)) return CCC_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     return dtype == 0 ? prox_impl<float>(bboxes, tree, triangles, B, F, threshold, maxc, out_rows, ws, ws_bytes, s)
                       : prox_impl<double>(bboxes, tree, triangles, B, F, threshold, maxc, out_rows, ws, ws_bytes, s);
@@ -545,7 +557,7 @@ int ccc_compute_impulses(int dtype, const void* bboxes, const int64_t* tree, con
     if (rc) return rc;
     if (!bboxes || !tree || !triangles || !triangles_next || !masses || !dv || !dx || !counter || maxc < 1)
         return CCC_ERR_INVALID_ARG;
-    if (B * F * maxc >= ((int64_t)1 << 31)) return CCC_ERR_INVALID_ARG;
+    if (!rows_fit(B, F, maxc)) return CCC_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     return dtype == 0 ? impulses_impl<float>(bboxes, tree, triangles, triangles_next, masses, mask, B, F, maxc, dv, dx,
                                              counter, ws, ws_bytes, s)
@@ -578,16 +590,24 @@ int ccc_compute_impulses_from_collisions(int dtype, const int64_t* collisions, c
 // ccc_find_collisions_continuous lives in a fixed file-scope device array of
 // CCC_STATIC_SCRATCH_BYTES, which every GPU that loads this library holds until the
 // process exits.  The array's name is only a host-side stand-in in host code, so its
-// device address is looked up once per device with cudaGetSymbolAddress (on the first
-// call on that device, which should therefore come before any stream capture).  Every
-// call shares the array: calls whose work overlaps on the GPU (different streams or
-// threads without ordering) race on it.  Each call clears the parts that must start at
-// zero; the rest is fully rewritten before it is read.
+// device address is looked up with cudaGetSymbolAddress, with the calling device current,
+// on every call: after a cudaDeviceReset (or in another context) the module's data is
+// loaded again at a different address, so a cached address could point at someone else's
+// memory.  The first call on a device also loads the module's data there, so it should
+// come before any stream capture.  Every call shares the array: calls whose work overlaps
+// on the GPU (different streams or threads without ordering) race on it.  Each call clears
+// the parts that must start at zero; the rest is fully rewritten before it is read.
 
 #define CCC_STATIC_SCRATCH_BYTES (64ll << 20)
 
 static __device__ __align__(256) unsigned char g_ccc_static_scratch[CCC_STATIC_SCRATCH_BYTES];
-static std::atomic<void*> g_ccc_static_addr[64];
+
+// device address of the array on the current device (nullptr on a CUDA error)
+static void* static_scratch_base() {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_ccc_static_scratch) != cudaSuccess) return nullptr;
+    return p;
+}
 
 int64_t ccc_static_scratch_bytes(void) { return CCC_STATIC_SCRATCH_BYTES; }
 
@@ -597,20 +617,25 @@ int ccc_find_collisions_continuous_static(int dtype, const void* bboxes, const i
                                           void* stream) {
     int rc = check_common(dtype, B, F);
     if (rc) return rc;
-    if (maxc < 1 || maxcol < 1) return CCC_ERR_INVALID_ARG;
+    if (!rows_fit(B, F, maxc) || !rows_fit(B, F, maxcol)) return CCC_ERR_INVALID_ARG;
     int64_t need = layout(B, F, maxc, true).end;
     if (need > CCC_STATIC_SCRATCH_BYTES) return CCC_ERR_TOO_LARGE;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return CCC_ERR_CUDA;
-    void* base = g_ccc_static_addr[dev].load();
-    if (base == nullptr) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_ccc_static_scratch) != cudaSuccess || p == nullptr) return CCC_ERR_CUDA;
-        g_ccc_static_addr[dev].store(p);
-        base = p;
-    }
+    void* base = static_scratch_base();
+    if (base == nullptr) return CCC_ERR_CUDA;
     return ccc_find_collisions_continuous(dtype, bboxes, tree, triangles, triangles_next, mask, B, F, maxc, maxcol,
                                           out_rows, out_times, base, CCC_STATIC_SCRATCH_BYTES, stream);
+}
+
+int ccc_static_scratch_read_status(int64_t n_mesh, int32_t* out, void* stream) {
+    void* base = static_scratch_base();
+    if (base == nullptr) return CCC_ERR_CUDA;
+    return ccc_read_status(base, n_mesh, out, stream);
+}
+
+int ccc_static_scratch_read_counters(int32_t* out, void* stream) {
+    void* base = static_scratch_base();
+    if (base == nullptr) return CCC_ERR_CUDA;
+    return ccc_read_counters(base, out, stream);
 }
 
 }  // extern "C"

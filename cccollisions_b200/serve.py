@@ -51,6 +51,7 @@ class Request:
     iterations: int = -1
     converged: bool = False
     verts1_out: np.ndarray | None = None
+    contacts: list = field(default_factory=list)     # contacts found by each loop iteration
     _sid: int = field(default=-1, repr=False)
     _pinned: tuple = field(default=(), repr=False)
     _result: object = field(default=None, repr=False)    # pinned host buffer for verts1
@@ -71,10 +72,13 @@ class Request:
 def engine_capacity(budget_bytes: int, dtype=torch.float64, mesh_capacity: int = 4096,
                     vert_ratio: float = 0.75, maxc: int = 16) -> tuple[int, int]:
     """Largest (triangle, vertex) capacity whose engine block fits the budget, with
-    vert_ratio vertices per triangle (a grid mesh has about 0.5)."""
+    vert_ratio vertices per triangle (a grid mesh has about 0.5).  The budget also holds the
+    library's fixed module-data array (ccc_static_scratch_bytes, resident on every device
+    where the library is loaded), so the block gets what is left after it."""
     code = 0 if dtype == torch.float32 else 1
     lo, hi = 2, 1 << 27
     L = N.lib()
+    budget_bytes = int(budget_bytes) - int(L.ccc_static_scratch_bytes())
     while lo < hi:
         mid = (lo + hi + 1) // 2
         b = L.ccc_engine_bytes(code, mid, int(mid * vert_ratio) + 16, mesh_capacity, maxc, 1)
@@ -161,6 +165,8 @@ class Server:
                     st = eng.state(sids)
                     if st["status"] & ~N.CCC_ST_NONFINITE:
                         raise RuntimeError(f"engine status {st['status']:#x}")
+                    for sid, c in zip(sids, st["contacts"]):
+                        active[sid].contacts.append(int(c))
                     done = [(sid, int(it), bool(fl & N.CCC_MESH_CONVERGED))
                             for sid, it, fl in zip(sids, st["iterations"], st["flags"]) if fl & N.CCC_MESH_DONE]
                     if done:
@@ -206,7 +212,10 @@ class Server:
                 "throughput": tris / (last - first), "p50_ms": float(np.percentile(lat, 50) * 1e3),
                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3),
                 "ticks": self.ticks, "mean_iterations": float(np.mean([r.iterations for r in requests])),
-                "converged": float(np.mean([r.converged for r in requests]))}
+                "converged": float(np.mean([r.converged for r in requests])),
+                "contacts_first_iteration": int(sum(r.contacts[0] for r in requests if r.contacts)),
+                "contacts_last_iteration": int(sum(r.contacts[-1] for r in requests if r.contacts)),
+                "contacts_all_iterations": int(sum(sum(r.contacts) for r in requests))}
 
 
 def requests_from_stream(stream, dtype=np.float64) -> list[Request]:

@@ -11,7 +11,10 @@
  *   - Outputs are written in place.  Row outputs must be pre-filled with -1 by the caller
  *     (the reference allocates them as -1 * ones); impulse outputs must be zeroed.
  *   - ws / ws_bytes: caller-provided device scratch of at least the size returned by the
- *     matching *_workspace_size call.  The library allocates no device memory.
+ *     matching *_workspace_size call.  The library makes no device allocations at run time;
+ *     it does keep one fixed module-data array of ccc_static_scratch_bytes() (64 MiB) on
+ *     every device where it is loaded (the scratch of ccc_find_collisions_continuous_static),
+ *     which device-memory budgets should leave room for.
  *   - stream: a cudaStream_t (NULL = legacy default stream).  Calls are asynchronous;
  *     ccc_read_status() synchronises the stream and returns the device status word.
  *   - Return value: 0 on success or a CCC_ERR_* code for argument / launch errors.
@@ -201,15 +204,25 @@ int ccc_compute_impulses_from_collisions(int dtype, const int64_t* collisions, c
  * with its scratch in a fixed device array of ccc_static_scratch_bytes() bytes (64 MiB)
  * that every GPU loading this library holds until exit.  Problems whose scratch
  * (ccc_workspace_size(CCC_OP_CONTINUOUS, B, F, max_candidates_per_triangle)) exceeds it
- * return CCC_ERR_TOO_LARGE before any device work.  The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress); make it before any stream capture.
- * All calls share the array: calls that overlap on the GPU race.  Outputs as for
- * ccc_find_collisions_continuous (pre-filled with -1 by the caller). */
+ * return CCC_ERR_TOO_LARGE before any device work.  Every call looks up the array's device
+ * address on the current device (cudaGetSymbolAddress, a host-side lookup, so a
+ * cudaDeviceReset in between is harmless); the first call on a device also loads the
+ * module's data there, so make it before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race.  Outputs as for ccc_find_collisions_continuous
+ * (pre-filled with -1 by the caller). */
 int64_t ccc_static_scratch_bytes(void);
 int ccc_find_collisions_continuous_static(int dtype, const void* bboxes, const int64_t* tree, const void* triangles,
                                           const void* triangles_next, const uint8_t* mask, int64_t B, int64_t F,
                                           int64_t max_candidates_per_triangle, int64_t max_collisions_per_triangle,
                                           int64_t* out_rows, void* out_times, void* stream);
+
+/* ccc_read_status / ccc_read_counters for the last ccc_find_collisions_continuous_static
+ * call on the current device (no counterpart in the reference): the status word (candidate
+ * or output overflow, stack overflow, malformed tree), the candidate count and up to n_mesh
+ * per-mesh row counts; or the four work counters.  They read the shared array, so call them
+ * before the next static call is queued.  Synchronise the stream. */
+int ccc_static_scratch_read_status(int64_t n_mesh, int32_t* out, void* stream);
+int ccc_static_scratch_read_counters(int32_t* out, void* stream);
 
 #ifdef __cplusplus
 }
