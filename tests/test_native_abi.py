@@ -146,10 +146,12 @@ def test_api_rejects_cpu_tensors():
 
 def test_served_engine_capacity_fits_the_budget(native_lib):
     """The server sizes its engine block from a device-memory budget (pure host): the
-    largest triangle capacity whose block fits, so one triangle more does not fit (or
-    exceeds the engine's limits)."""
+    largest triangle capacity whose block fits beside the library's fixed module-data
+    array, so one triangle more does not fit (or exceeds the engine's limits)."""
     import torch
     from cccollisions_b200.serve import engine_capacity
+    fixed = native_lib.ccc_static_scratch_bytes()
+    assert fixed == 64 << 20
     prev = 0
     for gb in (1, 2, 40):
         budget = gb << 30
@@ -157,6 +159,44 @@ def test_served_engine_capacity_fits_the_budget(native_lib):
         assert tc > prev
         prev = tc
         assert vc == int(tc * 0.75) + 16
-        assert 0 < native_lib.ccc_engine_bytes(1, tc, vc, 4096, 16, 1) <= budget
+        assert 0 < native_lib.ccc_engine_bytes(1, tc, vc, 4096, 16, 1) <= budget - fixed
         over = native_lib.ccc_engine_bytes(1, tc + 1, int((tc + 1) * 0.75) + 16, 4096, 16, 1)
-        assert over > budget or over == -1
+        assert over > budget - fixed or over == -1
+
+
+def test_size_checks_cannot_wrap(native_lib):
+    """Capacity checks divide rather than multiply, so per-triangle capacities near 2^63
+    (whose products with B * F would wrap to small numbers) are argument errors, before
+    any pointer is touched; so are batch and triangle counts whose product would wrap."""
+    from cccollisions_b200 import _native as N
+    huge = 1 << 44
+    assert native_lib.ccc_workspace_size(N.OP_CONTINUOUS, 1, 1 << 20, huge) == -1
+    assert native_lib.ccc_workspace_size(N.OP_CONTINUOUS, 1 << 40, 1 << 40, 16) == -1
+    assert native_lib.ccc_workspace_size(N.OP_CONTINUOUS, 1, 1 << 20, 16) > 0
+    args = (None, None, None, None, None, 1, 1 << 20, huge, 16, None, None)
+    assert native_lib.ccc_find_collisions_continuous(1, *args, None, 0, None) == N.CCC_ERR_INVALID_ARG
+    assert native_lib.ccc_find_collisions_continuous_static(1, *args, None) == N.CCC_ERR_INVALID_ARG
+    assert native_lib.ccc_find_collisions_continuous_static(1, None, None, None, None, None, 1 << 40, 1 << 40, 16, 16,
+                                                            None, None, None) == N.CCC_ERR_INVALID_ARG
+    assert native_lib.ccc_compute_impulses(1, None, None, None, None, None, None, 1, 1 << 20, huge, 16, None, None,
+                                           None, None, 0, None) == N.CCC_ERR_INVALID_ARG
+    assert native_lib.ccc_find_mincol_cand(1, None, None, None, None, 1, 1 << 20, huge, None, None, 0,
+                                           None) == N.CCC_ERR_INVALID_ARG
+
+
+def test_reference_module_name_imports_the_drop_in(native_lib):
+    """``import cccollisions`` (the reference's module name) gives this library's functions,
+    with the reference's argument names and defaults."""
+    import inspect
+
+    import cccollisions
+    import cccollisions_b200
+    assert sorted(cccollisions.__all__) == sorted(cccollisions_b200.__all__)
+    for name in cccollisions_b200.__all__:
+        assert getattr(cccollisions, name) is getattr(cccollisions_b200, name)
+    sig = inspect.signature(cccollisions.find_collisions_continuous)
+    assert list(sig.parameters) == ["bboxes", "tree", "triangles", "triangles_next", "max_candidates_per_triangle",
+                                    "max_collisions_per_triangle"]
+    assert sig.parameters["max_candidates_per_triangle"].default == 16
+    sig = inspect.signature(cccollisions.compute_impulses)
+    assert list(sig.parameters)[:5] == ["bboxes", "tree", "triangles", "triangles_next", "triangles_mass"]
