@@ -1,6 +1,7 @@
 """B200-native collision engine, a drop-in for the ``cccollisions`` torch extension.
 
-``import cccollisions_b200 as cccollisions`` gives the reference's module-level functions
+``import cccollisions`` (the alias package beside this one) or ``import cccollisions_b200`` gives
+the reference's module-level functions
 (bvh, bvh_motion, find_collisions, find_collisions_continuous[_partial], find_proximity,
 find_mincol_cand, compute_impulses[_partial], compute_impulses_from_collisions).
 """

@@ -6,6 +6,9 @@ golden fixtures under tests/golden/ on a GPU).  Nothing in the product imports i
 
     python oracle/build_ref.py [--src /path/to/reference]
 
+The source checkout comes from ``--src``, else from the ``CCC_REFERENCE_SRC`` environment
+variable, else from the checkout location of the machine this recipe was written on.
+
 The reference's own build (setup.py + cuda-samples' helper_math.h) is not run.  Instead:
 * ``oracle/ref_shim/helper_math.h`` (project-written) supplies the component-wise float
   vector operators the sources use;
@@ -25,7 +28,14 @@ import sysconfig
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 SHIM = os.path.join(HERE, "ref_shim")
-DEFAULT_SRC = "/root/reference"
+DEFAULT_SRC = os.environ.get("CCC_REFERENCE_SRC", "/root/reference")
+
+
+def reference_src(src=None):
+    """The reference checkout: the argument, else CCC_REFERENCE_SRC, else DEFAULT_SRC; None when
+    that directory holds no ``src/`` (the product build then skips the checker)."""
+    src = src or DEFAULT_SRC
+    return src if os.path.isdir(os.path.join(src, "src")) else None
 
 
 def build(src=DEFAULT_SRC, force=False) -> str:
@@ -83,7 +93,7 @@ def build_probe(src=DEFAULT_SRC, force=False) -> str:
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--src", default="/root/reference")
+    ap.add_argument("--src", default=DEFAULT_SRC)
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()
     print(build(a.src, a.force))

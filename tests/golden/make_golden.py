@@ -32,10 +32,16 @@ sys.path.insert(0, ROOT)
 
 
 def load_reference():
+    """The reference extension built by oracle/build_ref.py, loaded from its file (this
+    repository's own ``cccollisions`` package has the same module name)."""
+    import importlib.util
+
     import torch  # noqa: F401  (loads libtorch for the extension)
-    sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
-    import cccollisions
-    return cccollisions
+    spec = importlib.util.spec_from_file_location("cccollisions", os.path.join(ROOT, "oracle", "_ref",
+                                                                                "cccollisions.so"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
 
 
 def tree_depth(tr):
