@@ -90,6 +90,36 @@ def test_continuous_rows_close_to_reference(oracle, name):
         assert differing <= 0.1 * total, (differing, total)
 
 
+@pytest.mark.parametrize("name", SOUPS)
+def test_partial_variants_match_reference(oracle, name):
+    """find_collisions_continuous_partial / compute_impulses_partial of the reference under
+    the fixture's mask (``ccdp_*``, ``impp_*``).  The reference indexes the mask by sorted
+    leaf position on the query side and by triangle id on the other
+    (src/collisions_continuous.cu:1090, 174-175): every pair of its rows is a candidate of
+    the oracle's masked traversal, which restates that quirk, and the rows agree as closely
+    as the unmasked ones (elementary-function ulps).  Its impulses are those of its own
+    partial rows: counters equal, dv / dx within 1e-12 (fp64) / 1e-6 (fp32) of the largest."""
+    d = _load(name)
+    x0, x1, m = d["x0"], d["x1"], d["masses"]
+    mask = d["mask"].astype(np.uint8)
+    assert 0 < mask.sum() < len(mask)
+    bb, tr = oracle.bvh(x0, x1)
+    cand = set(map(tuple, oracle.candidates(bb, tr, mask=mask).tolist()))
+    full = set(map(tuple, oracle.candidates(bb, tr).tolist()))
+    assert len(cand) < len(full)
+    ref_pairs = {(a, b) for a, b, _ in d["ccdp_rows"].tolist()}
+    assert ref_pairs and ref_pairs <= cand
+    er, _ = oracle.ccd(bb, tr, x0, x1, mask=mask)
+    ref, orc = _ms(d["ccdp_rows"]), _ms(er)
+    differing = sum((ref - orc).values()) + sum((orc - ref).values())
+    assert differing <= 0.1 * max(len(d["ccdp_rows"]), 1), differing
+    dv, dx, cnt = oracle.impulses_from_rows(x0, x1, m, d["ccdp_rows"], d["ccdp_times"])
+    assert (cnt == d["impp_cnt"]).all()
+    tol = 1e-12 if x0.dtype == np.float64 else 1e-6
+    for got, want in ((dv, d["impp_dv"]), (dx, d["impp_dx"])):
+        assert np.abs(got - want).max() <= tol * np.abs(want).max()
+
+
 # ------------------------------------------------------------------ stage by stage
 # tests/golden/stages_*.npz hold, for sampled (i, j, type) sub-tests, the outputs of the
 # reference's own kernels (getCubicCoeffs, solveCubic, filterCollisions,

@@ -131,6 +131,36 @@ def test_impulses_match_reference(cuda, oracle, name):
         assert np.abs(g - r).max() <= tol * np.abs(r).max()
 
 
+@pytest.mark.parametrize("name", SOUPS)
+def test_partial_variants_bit_exact_with_reference(cuda, oracle, name):
+    """find_collisions_continuous_partial and compute_impulses_partial in the default mode
+    against the reference's own outputs under the fixture's mask, including its mask
+    indexing (sorted leaf position on the query side, triangle id on the other,
+    src/collisions_continuous.cu:1090, 174-175): equal row multisets with bit-equal times,
+    equal counters, dv / dx within 1e-6 (fp64) / 1e-4 (fp32) of the largest."""
+    import cccollisions_b200 as C
+    from cccollisions_b200 import _native as N
+    d = _load(name)
+    x0, x1, m, mask = d["x0"], d["x1"], d["masses"], d["mask"]
+    bb, tr = oracle.bvh(x0, x1)
+    args = (_t(bb[None]), _t(tr[None]), _t(x0[None]), _t(x1[None]))
+    with N.math_library(N.LIB_REFERENCE):
+        rows, times = C.find_collisions_continuous_partial(*args, _t(mask[None]), 16, 16)
+        dv, dx, cnt = C.compute_impulses_partial(*args, _t(m[None]), _t(mask[None]), 16, 16)
+    r = rows[0].cpu().numpy()
+    n = int((r[:, 0] >= 0).sum())
+    t = times[0, :n, 0].cpu().numpy().astype(np.float64)
+    got = Counter(zip(map(tuple, r[:n].tolist()), t.tolist()))
+    ref = Counter(zip(map(tuple, d["ccdp_rows"].tolist()), d["ccdp_times"].astype(np.float64).tolist()))
+    assert n > 0 and got == ref, (sum((got - ref).values()), sum((ref - got).values()))
+    assert (cnt[0].cpu().numpy() == d["impp_cnt"]).all()
+    tol = 1e-6 if x0.dtype == np.float64 else 1e-4
+    for g, want in ((dv, d["impp_dv"]), (dx, d["impp_dx"])):
+        g = g[0].cpu().numpy().astype(np.float64)
+        want = want.astype(np.float64)
+        assert np.abs(g - want).max() <= tol * np.abs(want).max()
+
+
 def test_static_and_proximity_match_reference(cuda, oracle):
     import cccollisions_b200 as C
     d = _load("static_fold")
