@@ -376,18 +376,18 @@ int ccc_debug_stage(int op, int lib, const double* in, int in_stride, double* ou
     if (n == 0) return CCC_OK;
     if (!in || !out) return CCC_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
-    CCC_LAUNCH("k_debug_stage", s, k_debug_stage<<<grid_for(n, 128), 128, 0, s>>>(op, lib, in, in_stride, out, out_stride, (int)n));
-    CCC_LAUNCH_CHECK();
-    return CCC_OK;
+    cudaError_t e = cudaSuccess;
+    CCC_LAUNCH("k_debug_stage", s, e = launch_debug_stage(op, lib, in, in_stride, out, out_stride, (int)n, s));
+    return e == cudaSuccess ? CCC_OK : CCC_ERR_CUDA;
 }
 
 int ccc_debug_math(int op, const double* in, double* out, int64_t n, void* stream) {
     if (op < 0 || op > 11 || n < 0 || (n > 0 && (!in || !out)) || n >= ((int64_t)1 << 31)) return CCC_ERR_INVALID_ARG;
     if (n == 0) return CCC_OK;
     cudaStream_t s = (cudaStream_t)stream;
-    CCC_LAUNCH("k_debug_math", s, k_debug_math<<<grid_for(n, 128), 128, 0, s>>>(op, in, out, (int)n));
-    CCC_LAUNCH_CHECK();
-    return CCC_OK;
+    cudaError_t e = cudaSuccess;
+    CCC_LAUNCH("k_debug_math", s, e = launch_debug_math(op, in, out, (int)n, s));
+    return e == cudaSuccess ? CCC_OK : CCC_ERR_CUDA;
 }
 
 int ccc_timing_begin(void) {

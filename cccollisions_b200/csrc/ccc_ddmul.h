@@ -11,7 +11,8 @@
 // needs: an expansion of K in {1,2} terms times one double, rounded to R = 2 terms.
 //
 // Every operation is a single IEEE-754 double add / multiply / fma, so host and device
-// produce identical bits.
+// produce identical bits; every product is a ccc_mul, so the results stay the same in a
+// translation unit compiled with multiply-add contraction.
 #pragma once
 
 #include "ccc_libm.h"
@@ -45,11 +46,11 @@ template <int K> CCC_HD ccc_dd ccc_certmul_k(double x0, double x1, double y) {
     int e0 = ex0 + ey;
     const double step = ccc_pow2i(-BIN);
     s0 = ccc_ldexp(1.5, e0 - BIN + 52);
-    s1 = s0 * step;
-    s2 = s1 * step;
-    s3 = s2 * step;
-    double s4 = s3 * step;
-    double s5 = s4 * step;
+    s1 = ccc_mul(s0, step);
+    s2 = ccc_mul(s1, step);
+    s3 = ccc_mul(s2, step);
+    double s4 = ccc_mul(s3, step);
+    double s5 = ccc_mul(s4, step);
     b0 = s0; b1 = s1; b2 = s2; b3 = s3; b4 = s4; b5 = s5;
     for (int i = 0; i < k; ++i) {
         double xi = i == 0 ? x0 : x1;
@@ -59,7 +60,7 @@ template <int K> CCC_HD ccc_dd ccc_certmul_k(double x0, double x1, double y) {
         int sh = l / BIN;
         l = l - sh * BIN;
         if (sh < 0 || sh >= 3) continue;
-        double p = xi * y;
+        double p = ccc_mul(xi, y);
         double e = ccc_fma(xi, y, -p);
         // the bins touched are sh .. sh+3; work on a window w0..w3 and write it back
         double w0 = sh == 0 ? b0 : (sh == 1 ? b1 : b2);
@@ -159,7 +160,7 @@ CCC_HD bool ccc_pow2_or_special(double x) {
 CCC_HD ccc_dd ccc_certmul1(double x, double y) {
     const int bx = ccc_bexp(x), by = ccc_bexp(y);
     const int e0 = (bx - 1022) + (by - 1022);
-    const double p = x * y;
+    const double p = ccc_mul(x, y);
     const double e = ccc_fma(x, y, -p);
     bool easy = x != 0.0 && y != 0.0 && bx != 0 && bx != 0x7ff && by != 0 && by != 0x7ff && e0 >= -700 &&
                 e0 <= 1000 && !ccc_pow2_or_special(p);
@@ -180,9 +181,9 @@ CCC_HD ccc_dd ccc_certmul1(double x, double y) {
 CCC_HD double ccc_certmul2_hi(double x0, double x1, double y) {
     const int b0 = ccc_bexp(x0), by = ccc_bexp(y);
     const int e0 = (b0 - 1022) + (by - 1022);
-    const double p0 = x0 * y;
+    const double p0 = ccc_mul(x0, y);
     const double er = ccc_fma(x0, y, -p0);
-    const double rest = er + x1 * y;
+    const double rest = er + ccc_mul(x1, y);
     const double c = p0 + rest;
     bool easy = x0 != 0.0 && y != 0.0 && b0 != 0 && b0 != 0x7ff && by != 0 && by != 0x7ff && e0 >= -700 &&
                 e0 <= 1000 && !ccc_pow2_or_special(c) && ccc_bexp(x1) != 0x7ff &&

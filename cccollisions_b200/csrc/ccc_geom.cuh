@@ -42,6 +42,18 @@ template <class T> __device__ __forceinline__ V3<T> lin3(V3<T> a, T u, V3<T> b, 
 }
 // a*b - c*d  ->  fma(a, b, -(c*d))
 template <class T> __device__ __forceinline__ T fms2(T a, T b, T c, T d) { return fmaT(a, b, -(c * d)); }
+// A rounded product, sum or difference that the compiler never fuses with a neighbouring
+// operation.  The continuous narrow phase is compiled with multiply-add contraction on (as
+// the reference is: it must call CUDA's pow as the reference's build compiles it), so every
+// product of this library's own that feeds a sum is written with these (or inside an
+// explicit fmaT, whose operands are never fused either): the code rounds as written under
+// either setting.
+__device__ __forceinline__ float mulrn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mulrn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float addrn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double addrn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float subrn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double subrn(double a, double b) { return __dsub_rn(a, b); }
 
 // Elementary functions of the cubic solver and of normalize(): CUDA's own (the reference's
 // calls: cbrt, cbrtf, acos, cos, sin, pow(x, 2), rsqrt) or this library's portable ones,
@@ -248,17 +260,14 @@ template <class T> __device__ __forceinline__ uint32_t ccd_subbox_mask(const MTr
 // straight from the soups one axis at a time: both are conjunctions over the axes (equal
 // coordinates; intervals that overlap), so the per-axis results are ANDed.  Same boxes and
 // comparisons as share_vertex + ccd_subbox_mask (v and v + dv with dv = x1 - x0, min / max
-// merges, inclusive bounds), with a third of the live values.  Returns 0 when the
-// triangles share a vertex, else the mask of sub-tests whose swept boxes overlap
-// (REJECT_RIGID: 0 as well for a pair whose sub-tests can have no root, see the end).
-template <class T, bool REJECT_RIGID = true>
-__device__ __forceinline__ uint32_t ccd_pair_mask(const T* __restrict__ x0, const T* __restrict__ x1, long long i,
-                                                  long long j) {
+// merges, inclusive bounds), with a third of the live values.
+
+// shareVertex of the start positions (figures.cu:527-544): any vertex of i equal to one of
+// j on every axis
+template <class T>
+__device__ __forceinline__ bool ccd_pair_shares_vertex(const T* __restrict__ x0, long long i, long long j) {
     const T* a0 = x0 + i * 9;
-    const T* a1 = x1 + i * 9;
     const T* b0 = x0 + j * 9;
-    const T* b1 = x1 + j * 9;
-    // shared vertices first (start positions only): most rejected pairs are mesh neighbours
     uint32_t eq = 0x1ffu;       // vertex pairs (ia, jb) equal on every axis so far: bit 3 ia + jb
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
@@ -274,7 +283,18 @@ __device__ __forceinline__ uint32_t ccd_pair_mask(const T* __restrict__ x0, cons
             for (int jb = 0; jb < 3; ++jb)
                 if (!(av[ia] == bv[jb])) eq &= ~(1u << (3 * ia + jb));
     }
-    if (eq) return 0u;
+    return eq != 0u;
+}
+
+// The mask of sub-tests whose swept boxes overlap, for a pair that shares no vertex
+// (REJECT_RIGID: 0 as well for a pair whose sub-tests can have no root, see the end).
+template <class T, bool REJECT_RIGID = true>
+__device__ __forceinline__ uint32_t ccd_pair_subbox_mask(const T* __restrict__ x0, const T* __restrict__ x1,
+                                                         long long i, long long j) {
+    const T* a0 = x0 + i * 9;
+    const T* a1 = x1 + i * 9;
+    const T* b0 = x0 + j * 9;
+    const T* b1 = x1 + j * 9;
     uint32_t m = 0x7fffu;
     bool rigid = true;          // every vertex moves by the same displacement (on all axes so far)
 #pragma unroll
@@ -329,6 +349,14 @@ __device__ __forceinline__ uint32_t ccd_pair_mask(const T* __restrict__ x0, cons
     // root of that linear case (collisions_continuous.cu:531-535), so no sub-test of the pair
     // can give a row or a contact.
     return REJECT_RIGID && rigid ? 0u : m;
+}
+
+// 0 when the triangles share a vertex, else ccd_pair_subbox_mask
+template <class T, bool REJECT_RIGID = true>
+__device__ __forceinline__ uint32_t ccd_pair_mask(const T* __restrict__ x0, const T* __restrict__ x1, long long i,
+                                                  long long j) {
+    if (ccd_pair_shares_vertex<T>(x0, i, j)) return 0u;
+    return ccd_pair_subbox_mask<T, REJECT_RIGID>(x0, x1, i, j);
 }
 
 // The same table packed into constants, so a runtime type k selects points without
@@ -492,8 +520,12 @@ __device__ __forceinline__ int cubic_prefix(double a, double b, double c, double
     double f3 = ccc_cube_hi(f);
     // the reference's pow(g, 2) resolves (through std::pow's promotion) to CUDA's general
     // pow(double, double), which is not always the rounded square
-    double g2 = lib == LIB_REFERENCE ? pow(g, 2.0) : g * g;
-    h = g2 / 4.0 + f3 / 27.0;
+    // the reference's pow(g, 2) resolves (through std::pow's promotion) to CUDA's general
+    // pow(double, double), which is not always the rounded square; CUDA's pow itself depends
+    // on the contraction setting it is compiled with, and the narrow phase is compiled with
+    // the reference's (ccc_narrow.cu).  g2 / 4 is exact.
+    double g2 = lib == LIB_REFERENCE ? pow(g, 2.0) : mulrn(g, g);
+    h = addrn(mulrn(g2, 0.25), f3 / 27.0);
     if (f == 0 && g == 0 && h == 0) return CUBIC_TRIPLE;
     return h <= 0 ? CUBIC_THREE : CUBIC_ONE;
 }
@@ -520,7 +552,7 @@ template <class T, int lib> __device__ __forceinline__ void triple_roots(double 
 
 template <class T, int lib>
 __device__ __forceinline__ void three_roots(double a, double b, double g, double h, T r[3], int& nr) {
-    double i = ccc_sqrt(((g * g) / 4.0) - h);
+    double i = ccc_sqrt(subrn(mulrn(mulrn(g, g), 0.25), h));
     double j, k, M, sn;
     if (lib == LIB_REFERENCE) {
         j = cbrt(i);
@@ -538,7 +570,7 @@ __device__ __forceinline__ void three_roots(double a, double b, double g, double
     const double r3 = ccc_sqrt(3.0);
     double L = j * -1;
     double P = (b / (3.0 * a)) * -1;
-    double x1 = (2 * j) * M - (b / (3.0 * a));
+    double x1 = subrn(mulrn(2 * j, M), b / (3.0 * a));
     double x2 = fmaT(L, fmaT(r3, sn, M), P);
     double x3 = fmaT(L, fmaT(-r3, sn, M), P);
     add_root<T>(r, (T)x1, nr);
@@ -548,12 +580,13 @@ __device__ __forceinline__ void three_roots(double a, double b, double g, double
 
 template <class T, int lib>
 __device__ __forceinline__ void one_root(double a, double b, double g, double h, T r[3], int& nr) {
-    double R = -(g / 2.0) + ccc_sqrt(h);
+    const double hg = mulrn(g, 0.5);      // g / 2, exact
+    double R = addrn(-hg, ccc_sqrt(h));
     double S, U;
     double Ra = R >= 0 ? R : -R;
     S = lib == LIB_REFERENCE ? cbrt(Ra) : ccc_cbrt(Ra);
     if (R < 0) S = -S;
-    double V = -(g / 2.0) - ccc_sqrt(h);
+    double V = subrn(-hg, ccc_sqrt(h));
     double Va = V >= 0 ? V : -V;
     U = lib == LIB_REFERENCE ? cbrt(Va) : ccc_cbrt(Va);
     if (V < 0) U = -U;
@@ -799,7 +832,7 @@ template <class T>
 __device__ __forceinline__ void impulse_point(const MTet<T>& tet, int k, int pt, const Contact<T>& ct,
                                               const ImpulseScale<T>& sc, V3<T>& imp, V3<T>& idx) {
     T mag = (k < 9) ? (pt < 2 ? sc.mag0 : sc.mag1) : (k < 12 ? (pt < 3 ? sc.mag0 : sc.mag1) : (pt < 1 ? sc.mag0 : sc.mag1));
-    imp = ct.n * mag;
+    imp = mk<T>(mulrn(ct.n.x, mag), mulrn(ct.n.y, mag), mulrn(ct.n.z, mag));
     // the point's displacement by value selects: a run-time index into tet would move the
     // whole tetrahedron to local memory
     const V3<T> d = pt == 0 ? tet.dv[0] : (pt == 1 ? tet.dv[1] : (pt == 2 ? tet.dv[2] : tet.dv[3]));

@@ -629,14 +629,17 @@ template <class T> struct CcdLayout {
     static constexpr size_t root_rec = clist + CCD_BATCH * 2;                          // u16 [3 BATCH]
     static constexpr size_t rec_cls = root_rec + 3 * CCD_BATCH * 2;                    // u8 [BATCH]
     static constexpr size_t rec_pos = align16(rec_cls + CCD_BATCH);                    // u16 [BATCH]
-    static constexpr size_t ints = align16(rec_pos + CCD_BATCH * 2);                   // int [64]
+    static constexpr size_t spairs = align16(rec_pos + CCD_BATCH * 2);                 // int2 [BLOCK]
+    static constexpr size_t pbuf = spairs + CCD_BLOCK * sizeof(int2);                   // u16 [BLOCK / 32][64]
+    static constexpr size_t ints = align16(pbuf + (CCD_BLOCK / 32) * 64 * 2);          // int [64]
     static constexpr size_t bytes = ints + 64 * sizeof(int);
 };
 
 // slots of the small int area
 // (class counts and root counts come in two sets, used by alternate batches; each set of
 // root counts holds the edge-edge and the vertex-face count)
-enum CcdInts { CI_WARP = 0, CI_TOTAL = 32, CI_COUNT = 33, CI_ROOTS = 41 };
+// (the live-pair counter of a chunk also comes in two, used by alternate chunks)
+enum CcdInts { CI_WARP = 0, CI_TOTAL = 32, CI_COUNT = 33, CI_ROOTS = 41, CI_LIVE = 45 };
 
 // a queued sub-test: triangle slots i and j, type k in the top bits of j (slots < 2^28)
 __device__ __forceinline__ int2 pack_subtest(int i, int j, int k) { return make_int2(i, j | (k << 28)); }
@@ -650,6 +653,19 @@ __device__ __forceinline__ int warp_inclusive_scan(int v, int lane) {
     return v;
 }
 
+// The continuous narrow phase is compiled in one translation unit only, ccc_narrow.cu, with
+// nvcc's default multiply-add contraction as the reference is compiled (CUDA's pow, which the
+// solver calls, computes slightly different results on rare arguments under -fmad=false);
+// every operation of this library's own in it is contraction-proof (mulrn / addrn / subrn,
+// fmaT).  The other units see only the launcher's declaration; ccc_narrow.cu instantiates
+// the (type, mode, sink, math library) combinations the library launches.
+template <class T, int MODE, class Sink, int LIB>
+cudaError_t launch_ccd_narrow(int grid, cudaStream_t s, const int2* cand, int cand_cap, WsHeader* hdr, const T* x0,
+                              const T* x1, Forest F, long long* rows, T* times, int max_per_tri, int* mesh_counters,
+                              Sink sink);
+template <class T, int MODE, class Sink, int LIB> cudaError_t prepare_ccd_narrow();
+
+#ifdef CCC_NARROW_TU
 template <class T, int MODE, class Sink, int LIB>
 __global__ void __launch_bounds__(CCD_BLOCK, CCD_MIN_BLOCKS)
 k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ x0,
@@ -664,6 +680,8 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
     unsigned short* root_rec = reinterpret_cast<unsigned short*>(smem + L::root_rec);
     unsigned char* rec_cls = smem + L::rec_cls;
     unsigned short* rec_pos = reinterpret_cast<unsigned short*>(smem + L::rec_pos);
+    int2* spairs = reinterpret_cast<int2*>(smem + L::spairs);
+    unsigned short* pbuf = reinterpret_cast<unsigned short*>(smem + L::pbuf);
     int* ints = reinterpret_cast<int*>(smem + L::ints);
     constexpr int NW = CCD_BLOCK / 32;
     constexpr int NB = CCD_BATCH;
@@ -677,19 +695,40 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
     // class counts and root count of a batch, two sets used by alternate batches: a batch
     // clears the other set at its end, when every read of that set is two barriers back
     // (the staging barriers order the initial clearing before the first batch)
-    int par = 0;
+    int par = 0, cpar = 0;
     if (tid < 8) ints[CI_COUNT + tid] = 0;
     if (tid < 4) ints[CI_ROOTS + tid] = 0;
+    if (tid < 2) ints[CI_LIVE + tid] = 0;
+    __syncthreads();
     for (long long base = (long long)blockIdx.x * CCD_BLOCK;; base += (long long)gridDim.x * CCD_BLOCK) {
         const bool more = base < n;
         if (!more && queued == 0) break;
         if (more) {
+            // about half of the candidate pairs are mesh neighbours that share a vertex: the
+            // chunk's other pairs are gathered first (block-wide), so that the 15 swept
+            // sub-box tests run on full warps
             long long c = base + tid;
-            uint32_t bits = 0;
             int2 pr = make_int2(0, 0);
+            bool live = false;
             if (c < n) {
                 pr = cand[c];
-                bits = ccd_pair_mask<T, MODE != CCD_MINCOL>(x0, x1, pr.x, pr.y);
+                live = !ccd_pair_shares_vertex<T>(x0, pr.x, pr.y);
+            }
+            const unsigned lb = __ballot_sync(FULL, live);
+            int lbase = 0;
+            if (lane == 0 && lb) lbase = atomicAdd(&ints[CI_LIVE + cpar], __popc(lb));
+            lbase = __shfl_sync(FULL, lbase, 0);
+            if (live) spairs[lbase + __popc(lb & lt)] = pr;
+            __syncthreads();
+            const int nlive = ints[CI_LIVE + cpar];
+            // the other chunk parity's counter was last read before the barrier above
+            if (tid == 0) ints[CI_LIVE + (cpar ^ 1)] = 0;
+            cpar ^= 1;
+            uint32_t bits = 0;
+            pr = make_int2(0, 0);
+            if (tid < nlive) {
+                pr = spairs[tid];
+                bits = ccd_pair_subbox_mask<T, MODE != CCD_MINCOL>(x0, x1, pr.x, pr.y);
             }
             if (MODE == CCD_MINCOL) {
                 while (bits) {
@@ -704,6 +743,8 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                         rows[o * 3 + 2] = k;
                     }
                 }
+                // the next chunk reuses spairs and the other live counter
+                __syncthreads();
                 continue;
             }
             // append the chunk's sub-tests (block-wide exclusive scan of the counts)
@@ -740,12 +781,12 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                 MTet<T> tet = load_tet(x0, x1, it.x, it.y & 0x0fffffff, k);
                 T cf[4];
                 cubic_coeffs(tet, cf);
-                double g, h;
-                int cls = cubic_prefix<LIB>((double)cf[0], (double)cf[1], (double)cf[2], (double)cf[3], g, h);
                 rec[0 * NB + ri] = (double)cf[0];
                 rec[1 * NB + ri] = (double)cf[1];
                 rec[2 * NB + ri] = (double)cf[2];
                 rec[3 * NB + ri] = (double)cf[3];
+                double g, h;
+                int cls = cubic_prefix<LIB>((double)cf[0], (double)cf[1], (double)cf[2], (double)cf[3], g, h);
                 rec[4 * NB + ri] = g;
                 rec[5 * NB + ri] = h;
                 rec_cls[ri] = (unsigned char)cls;
@@ -774,11 +815,11 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                 int ri = 0;
                 bool ee = false;
                 if (j < nsolve) {
-                    int cc = (j >= o1) + (j >= o2) + (j >= o3);
                     ri = clist[j];
                     ee = ((items[(head + ri) % Q].y >> 28) & 15) < 9;
-                    class_roots<T, LIB>(cc + 1, rec[0 * NB + ri], rec[1 * NB + ri], rec[2 * NB + ri], rec[3 * NB + ri],
-                                        rec[4 * NB + ri], rec[5 * NB + ri], rr);
+                    int cc = (j >= o1) + (j >= o2) + (j >= o3);
+                    class_roots<T, LIB>(cc + 1, rec[0 * NB + ri], rec[1 * NB + ri], rec[2 * NB + ri],
+                                        rec[3 * NB + ri], rec[4 * NB + ri], rec[5 * NB + ri], rr);
                 }
 #pragma unroll
                 for (int s = 0; s < 3; ++s) {
@@ -802,25 +843,59 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
             const int nroots = nee + ints[CI_ROOTS + 2 * par + 1];
             if (tid == 0 && nroots) atomicAdd(&hdr->roots, nroots);
             // (3) filter and output
-            for (int jj = tid; jj < nroots; jj += CCD_BLOCK) {
-                const int j = jj < nee ? jj : 3 * NB - 1 - (jj - nee);
-                int2 it = items[(head + root_rec[j]) % Q];
-                int k = (it.y >> 28) & 15;
-                int2 q = make_int2(it.x, it.y & 0x0fffffff);
-                T root = root_val[j];
-                MTet<T> tet = load_tet(x0, x1, q.x, q.y, k);
-                if (!ccd_filter(tet, k, root)) continue;
-                if (MODE == CCD_ROWS) {
-                    OutRegion R = out_region(F, M, q.x, max_per_tri);
+            if (MODE == CCD_ROWS) {
+                // about one root in twelve passes the filter: those are buffered per warp and
+                // their rows written 32 at a time, so that the mesh lookup and the row append
+                // run on full warps rather than on the few lanes that passed
+                unsigned short* pb = pbuf + warp * 64;
+                int np = 0;                        // buffered roots of this warp (warp-uniform)
+                auto emit = [&](int j) {
+                    const int2 it = items[(head + root_rec[j]) % Q];
+                    const int qx = it.x, qy = it.y & 0x0fffffff, k = (it.y >> 28) & 15;
+                    OutRegion R = out_region(F, M, qx, max_per_tri);
                     long long r = append_row(mesh_counters, F, R.m, R.cap, &hdr->status);
                     if (r >= 0) {
                         long long o = (long long)R.po * max_per_tri + r;
-                        rows[o * 3 + 0] = q.x - R.po;
-                        rows[o * 3 + 1] = q.y - R.po;
+                        rows[o * 3 + 0] = qx - R.po;
+                        rows[o * 3 + 1] = qy - R.po;
                         rows[o * 3 + 2] = k;
-                        times[o] = root;
+                        times[o] = root_val[j];
                     }
-                } else {
+                };
+                for (int b0 = warp * 32; b0 < nroots; b0 += CCD_BLOCK) {
+                    const int jj = b0 + lane;
+                    int j = 0;
+                    bool pass = false;
+                    if (jj < nroots) {
+                        j = jj < nee ? jj : 3 * NB - 1 - (jj - nee);
+                        const int2 it = items[(head + root_rec[j]) % Q];
+                        const int k = (it.y >> 28) & 15;
+                        MTet<T> tet = load_tet(x0, x1, it.x, it.y & 0x0fffffff, k);
+                        pass = ccd_filter(tet, k, root_val[j]);
+                    }
+                    const unsigned pm = __ballot_sync(FULL, pass);
+                    if (pass) pb[np + __popc(pm & lt)] = (unsigned short)j;
+                    np += __popc(pm);
+                    if (np >= 32) {
+                        __syncwarp();
+                        emit(pb[lane]);
+                        __syncwarp();
+                        if (lane < np - 32) pb[lane] = pb[32 + lane];
+                        __syncwarp();
+                        np -= 32;
+                    }
+                }
+                __syncwarp();
+                if (lane < np) emit(pb[lane]);
+            } else {
+                for (int jj = tid; jj < nroots; jj += CCD_BLOCK) {
+                    const int j = jj < nee ? jj : 3 * NB - 1 - (jj - nee);
+                    int2 it = items[(head + root_rec[j]) % Q];
+                    int k = (it.y >> 28) & 15;
+                    int2 q = make_int2(it.x, it.y & 0x0fffffff);
+                    T root = root_val[j];
+                    MTet<T> tet = load_tet(x0, x1, q.x, q.y, k);
+                    if (!ccd_filter(tet, k, root)) continue;
                     T mq[4];
 #pragma unroll
                     for (int pt = 0; pt < 4; ++pt)
@@ -843,7 +918,7 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
 // instantiation and device; prepare_ccd_narrow does it ahead of any stream capture).
 // The flags are atomic because host threads may launch on different streams at once; two
 // first calls may both set the attribute, which is harmless.
-template <class T, int MODE, class Sink, int LIB> inline cudaError_t prepare_ccd_narrow() {
+template <class T, int MODE, class Sink, int LIB> cudaError_t prepare_ccd_narrow() {
     static std::atomic<bool> done[64];
     int dev = 0;
     cudaGetDevice(&dev);
@@ -855,15 +930,17 @@ template <class T, int MODE, class Sink, int LIB> inline cudaError_t prepare_ccd
 }
 
 template <class T, int MODE, class Sink, int LIB>
-inline cudaError_t launch_ccd_narrow(int grid, cudaStream_t s, const int2* cand, int cand_cap, WsHeader* hdr,
-                                     const T* x0, const T* x1, Forest F, long long* rows, T* times, int max_per_tri,
-                                     int* mesh_counters, Sink sink) {
+cudaError_t launch_ccd_narrow(int grid, cudaStream_t s, const int2* cand, int cand_cap, WsHeader* hdr, const T* x0,
+                              const T* x1, Forest F, long long* rows, T* times, int max_per_tri, int* mesh_counters,
+                              Sink sink) {
     cudaError_t e = prepare_ccd_narrow<T, MODE, Sink, LIB>();
     if (e != cudaSuccess) return e;
     k_ccd_narrow<T, MODE, Sink, LIB><<<grid, CCD_BLOCK, CcdLayout<T>::bytes, s>>>(
         cand, cand_cap, hdr, x0, x1, F, rows, times, max_per_tri, mesh_counters, sink);
     return cudaSuccess;
 }
+
+#endif  // CCC_NARROW_TU
 
 // proximity (proximity_static.cu:11-508)
 template <class T>
@@ -917,100 +994,10 @@ k_impulses_from_rows(const long long* __restrict__ rows, const T* __restrict__ r
     }
 }
 
-// Element-wise evaluation of the solver's arithmetic building blocks, for tests that compare
-// them bit for bit with the CPU oracle and against CUDA's own elementary functions.
-// op 0 cbrt, 1 acos, 2 cos, 3 sin, 4 certified product (in: x0, x1, k, y; out: r0, r1),
-// 5 solve_cubic (in: a, b, c, d; out: three roots), 6 CUDA cbrt, 7 CUDA acos, 8 CUDA cos,
-// 9 CUDA sin.  in has 4 doubles per element, out 3.
-static __global__ void k_debug_math(int op, const double* __restrict__ in, double* __restrict__ out, int n) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double* a = in + 4 * i;
-    double* o = out + 3 * i;
-    o[0] = o[1] = o[2] = 0.0;
-    switch (op) {
-        case 0: o[0] = ccc_cbrt(a[0]); break;
-        case 1: o[0] = ccc_acos(a[0]); break;
-        case 2: o[0] = ccc_cos(a[0]); break;
-        case 3: o[0] = ccc_sin(a[0]); break;
-        case 4: {
-            ccc_dd d = ccc_certmul(a[0], a[1], (int)a[2], a[3]);
-            o[0] = d.hi;
-            o[1] = d.lo;
-            break;
-        }
-        case 5: solve_cubic<double, LIB_PORTABLE>(a[0], a[1], a[2], a[3], o); break;
-        case 6: o[0] = cbrt(a[0]); break;
-        case 7: o[0] = acos(a[0]); break;
-        case 8: o[0] = cos(a[0]); break;
-        case 9: o[0] = sin(a[0]); break;
-        case 10: case 11: {
-            double A = a[0], Bc = a[1], Cc = a[2], Dc = a[3];
-            double f = ((3.0 * Cc / A) - ((Bc * Bc) / (A * A))) / 3.0;
-            double b3 = 2 * ccc_cube_hi(Bc);
-            ccc_dd a2dd = ccc_sq_dd(A);
-            double a3 = ccc_certmul(a2dd.hi, a2dd.lo, 2, A).hi;
-            double g = (b3 / a3 - (Bc * Cc * 9) / a2dd.hi + 27.0 * Dc / A) / 27.0;
-            double h = g * g / 4.0 + ccc_cube_hi(f) / 27.0;
-            if (op == 10) { o[0] = f; o[1] = g; o[2] = h; }
-            else { o[0] = b3; o[1] = a2dd.hi; o[2] = a3; }
-            break;
-        }
-        default: break;
-    }
-}
-
-// Stages of the continuous narrow phase on caller tetrahedra (v0..v3, dv0..dv3 = 24
-// doubles per element), for tests against the reference's own kernels and the oracle.
-// op 0: cubic coefficients -> 4 doubles; op 1: cubic solve (in: 4 coefficients) -> 3
-// roots; op 2: root filter (in: tet, type, root) -> 1.0 / 0.0; op 3: contact kinematics
-// (in: tet, type, root, 4 masses) -> normal (3), normal velocity, mass pair (2).
-// lib selects the elementary functions (MathLib).
-static __global__ void k_debug_stage(int op, int lib, const double* __restrict__ in, int in_stride,
-                              double* __restrict__ out, int out_stride, int n) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double* a = in + (long long)i * in_stride;
-    double* o = out + (long long)i * out_stride;
-    MTet<double> t;
-    if (op != 1) {
-        for (int p = 0; p < 4; ++p) {
-            t.v[p] = mk<double>(a[3 * p], a[3 * p + 1], a[3 * p + 2]);
-            t.dv[p] = mk<double>(a[12 + 3 * p], a[12 + 3 * p + 1], a[12 + 3 * p + 2]);
-        }
-    }
-    if (op == 0) {
-        cubic_coeffs(t, o);
-    } else if (op == 1) {
-        if (lib == LIB_REFERENCE) solve_cubic<double, LIB_REFERENCE>(a[0], a[1], a[2], a[3], o);
-        else solve_cubic<double, LIB_PORTABLE>(a[0], a[1], a[2], a[3], o);
-    } else if (op == 2) {
-        o[0] = ccd_filter(t, (int)a[24], a[25]) ? 1.0 : 0.0;
-    } else if (op == 4) {
-        // (f, g, h) of the solver prefix for coefficients (c3, c2, c1, c0)
-        double A = a[0], B = a[1], Cc = a[2], D = a[3];
-        double f = ((3.0 * Cc / A) - ((B * B) / (A * A))) / 3.0;
-        double b3 = 2 * ccc_cube_hi(B);
-        ccc_dd a2dd = ccc_sq_dd(A);
-        double a3 = ccc_certmul(a2dd.hi, a2dd.lo, 2, A).hi;
-        double g = (b3 / a3 - (B * Cc * 9) / a2dd.hi + 27.0 * D / A) / 27.0;
-        double g2 = lib == LIB_REFERENCE ? pow(g, 2.0) : g * g;
-        o[0] = f;
-        o[1] = g;
-        o[2] = g2 / 4.0 + ccc_cube_hi(f) / 27.0;
-    } else if (op == 5) {
-        // squares of a[0]: pow(x, 2), pow(x, 2.0), x * x
-        double x = a[0];
-        volatile int two = 2;
-        o[0] = pow(x, two);
-        o[1] = pow(x, (double)two);
-        o[2] = x * x;
-    } else if (op == 3) {
-        double q[4] = {a[26], a[27], a[28], a[29]};
-        Contact<double> ct = lib == LIB_REFERENCE ? contact<double, LIB_REFERENCE>(t, (int)a[24], a[25], q)
-                                                  : contact<double, LIB_PORTABLE>(t, (int)a[24], a[25], q);
-        o[0] = ct.n.x; o[1] = ct.n.y; o[2] = ct.n.z; o[3] = ct.vn; o[4] = ct.m0; o[5] = ct.m1;
-    }
-}
+// Test hooks of the solver's arithmetic (k_debug_math, k_debug_stage), compiled in
+// ccc_narrow.cu with the continuous narrow phase, so that they compute what it computes.
+cudaError_t launch_debug_math(int op, const double* in, double* out, int n, cudaStream_t s);
+cudaError_t launch_debug_stage(int op, int lib, const double* in, int in_stride, double* out, int out_stride, int n,
+                               cudaStream_t s);
 
 }  // namespace ccc

@@ -48,6 +48,32 @@ CCC_HD double ccc_fma(double a, double b, double c) {
 #endif
 }
 
+// Rounded product, sum and difference that a compiler never fuses with a neighbouring
+// operation, even in a translation unit built with multiply-add contraction on (the
+// continuous narrow phase is; the host side is built with -ffp-contract=off).  Every
+// product in this header that feeds a sum is one of these or an operand of ccc_fma.
+CCC_HD double ccc_mul(double a, double b) {
+#if defined(__CUDA_ARCH__)
+    return __dmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+CCC_HD double ccc_add(double a, double b) {
+#if defined(__CUDA_ARCH__)
+    return __dadd_rn(a, b);
+#else
+    return a + b;
+#endif
+}
+CCC_HD double ccc_sub(double a, double b) {
+#if defined(__CUDA_ARCH__)
+    return __dsub_rn(a, b);
+#else
+    return a - b;
+#endif
+}
+
 CCC_HD uint64_t ccc_dbits(double x) {
 #if defined(__CUDA_ARCH__)
     return (uint64_t)__double_as_longlong(x);
@@ -86,19 +112,19 @@ CCC_HD double ccc_ldexp(double x, int n) {
     // split into at most three in-range power-of-two factors; each intermediate stays
     // normal except possibly the last multiply, so only one rounding can occur
     while (n > 1023) {
-        x = x * ccc_pow2i(1023);
+        x = ccc_mul(x, ccc_pow2i(1023));
         n -= 1023;
     }
     if (n < -1022) {
         // keep an intermediate in range before the final (possibly rounding) multiply
         if (n < -1022 - 1022) {
-            x = x * ccc_pow2i(-1022);
+            x = ccc_mul(x, ccc_pow2i(-1022));
             n += 1022;
         }
-        x = x * ccc_pow2i(n + 60);
-        return x * ccc_pow2i(-60);
+        x = ccc_mul(x, ccc_pow2i(n + 60));
+        return ccc_mul(x, ccc_pow2i(-60));
     }
-    return x * ccc_pow2i(n);
+    return ccc_mul(x, ccc_pow2i(n));
 }
 
 // Exponent e of frexp: x = m * 2^e with |m| in [0.5, 1); 0 for x == 0 (and for inf/NaN).
@@ -109,7 +135,7 @@ CCC_HD int ccc_frexp_exp(double x) {
     if (be == 0) {
         if ((u << 1) == 0) return 0;
         // subnormal: scale up by 2^64 (exact) and re-read
-        double y = x * ccc_pow2i(64);
+        double y = ccc_mul(x, ccc_pow2i(64));
         uint64_t v = ccc_dbits(y);
         return (int)((v >> 52) & 0x7ff) - 1022 - 64;
     }
@@ -204,7 +230,7 @@ CCC_HD_CALL double ccc_sin(double x) {
     double s = ccc_sin_series(h), c = ccc_cos_series(h);
     for (int i = 0; i < k; ++i) {
         double s2 = 2.0 * s * c;
-        double c2 = 1.0 - 2.0 * s * s;
+        double c2 = ccc_sub(1.0, ccc_mul(2.0 * s, s));
         s = s2;
         c = c2;
     }
@@ -221,7 +247,7 @@ CCC_HD_CALL double ccc_cos(double x) {
     double s = ccc_sin_series(h), c = ccc_cos_series(h);
     for (int i = 0; i < k; ++i) {
         double s2 = 2.0 * s * c;
-        double c2 = 1.0 - 2.0 * s * s;
+        double c2 = ccc_sub(1.0, ccc_mul(2.0 * s, s));
         s = s2;
         c = c2;
     }
@@ -272,6 +298,6 @@ CCC_HD_CALL double ccc_acos(double x) {
     if (x != x) return x + x;
     if (x > 1.0 || x < -1.0) return (x - x) / (x - x);   // NaN outside the domain
     if (x >= 0.5) return 2.0 * ccc_asin_small(ccc_sqrt((1.0 - x) * 0.5));
-    if (x <= -0.5) return PI - 2.0 * ccc_asin_small(ccc_sqrt((1.0 + x) * 0.5));
+    if (x <= -0.5) return ccc_sub(PI, 2.0 * ccc_asin_small(ccc_sqrt((1.0 + x) * 0.5)));
     return PI_2 - ccc_asin_small(x);
 }
