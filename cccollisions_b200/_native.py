@@ -75,6 +75,9 @@ SIGNATURES = {
     "ccc_engine_capture": (_I, [_P, _I, ctypes.c_int32, _P]),
     "ccc_engine_replay": (_I, [_P, _I, _P]),
     "ccc_engine_autotune": (_I, [_P, _P, _P]),
+    "ccc_engine_schedule_count": (_I, []),
+    "ccc_engine_schedule_info": (_I, [ctypes.c_int32, _P]),
+    "ccc_engine_set_schedule": (_I, [_P, ctypes.c_int32]),
     "ccc_engine_read_state": (_I, [_P, _P, _I64, _P, _P, _P, _P, _P, _P]),
     "ccc_engine_pack_rows": (_I, [_P, _P, _P, _I64, _P, _P]),
     "ccc_engine_counters": (_I, [_P, _P, _P]),

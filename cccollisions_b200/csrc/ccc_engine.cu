@@ -156,11 +156,13 @@ struct Ranges {
 };
 
 // launch shapes: traversal blocks per SM, narrow-phase blocks per SM (one is resident at
-// a time; more blocks split the work finer)
+// a time; more blocks split the work finer), and the traversal's schedule (0: one query
+// per thread, k_traverse_q; 1: 32 queries per warp walking together, k_traverse_w)
 struct Shape {
-    int trav, narrow;
+    int trav, narrow, warp;
 };
-constexpr Shape SHAPES[] = {{4, 1}, {8, 1}, {16, 1}, {4, 2}, {8, 2}, {16, 2}, {8, 4}, {16, 4}, {32, 8}};
+constexpr Shape SHAPES[] = {{4, 1, 0}, {8, 1, 0}, {16, 1, 0}, {4, 2, 0}, {8, 2, 0}, {16, 2, 0}, {8, 4, 0},
+                            {16, 4, 0}, {32, 8, 0}, {4, 2, 1},  {8, 2, 1}, {16, 2, 1}, {32, 2, 1}};
 constexpr int NSHAPES = sizeof(SHAPES) / sizeof(SHAPES[0]);
 constexpr int DEFAULT_SHAPE = 4;
 
@@ -259,9 +261,14 @@ template <class T> int refit(ccc_engine* e, const Tables& t, const int* flags, c
 
 template <class T> int traverse(ccc_engine* e, const Tables& t, const int* flags, cudaStream_t s) {
     int g = num_sms() * SHAPES[e->shape].trav;
-    CCC_LAUNCH("k_traverse", s, k_traverse_q<<<g, TRAV_THREADS, 0, s>>>(
-        e->at<QNode>(e->L.qnodes), e->at<int>(e->L.qleaf), e->at<int>(e->L.leaf_tri), t.f, e->at<int2>(e->L.cand),
-        (int)e->L.cand_cap, e->hdr(), flags));
+    if (SHAPES[e->shape].warp)
+        CCC_LAUNCH("k_traverse", s, k_traverse_w<<<g, TRAV_THREADS, 0, s>>>(
+            e->at<QNode>(e->L.qnodes), e->at<int>(e->L.qleaf), e->at<int>(e->L.leaf_tri), t.f, e->at<int2>(e->L.cand),
+            (int)e->L.cand_cap, e->hdr(), flags));
+    else
+        CCC_LAUNCH("k_traverse", s, k_traverse_q<<<g, TRAV_THREADS, 0, s>>>(
+            e->at<QNode>(e->L.qnodes), e->at<int>(e->L.qleaf), e->at<int>(e->L.leaf_tri), t.f, e->at<int2>(e->L.cand),
+            (int)e->L.cand_cap, e->hdr(), flags));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -690,6 +697,22 @@ int ccc_engine_autotune(ccc_engine* e, void* stream, int32_t* choice) {
         g_tune_cache[key] = best;
     }
     if (choice) *choice = best;
+    return CCC_OK;
+}
+
+int ccc_engine_schedule_count(void) { return NSHAPES; }
+
+int ccc_engine_schedule_info(int32_t choice, int32_t* out) {
+    if (choice < 0 || choice >= NSHAPES || !out) return CCC_ERR_INVALID_ARG;
+    out[0] = SHAPES[choice].trav;
+    out[1] = SHAPES[choice].narrow;
+    out[2] = SHAPES[choice].warp;
+    return CCC_OK;
+}
+
+int ccc_engine_set_schedule(ccc_engine* e, int32_t choice) {
+    if (!e || choice < 0 || choice >= NSHAPES) return CCC_ERR_INVALID_ARG;
+    e->shape = choice;
     return CCC_OK;
 }
 

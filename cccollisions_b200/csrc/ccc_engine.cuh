@@ -756,6 +756,136 @@ k_traverse_q(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, co
     if (nbuf > 0) flush_rest(cbuf, tid, nbuf, cand, cand_cap, hdr);
 }
 
+// Warp-cooperative form of k_traverse_q (collisions_static.cu:10-103): the 32 lanes of a warp
+// take 32 consecutive query leaves and walk the QNode tree together with one stack, held
+// across the lanes' registers (entry e in lane e % 32, word e / 32).  Each visited QNode is
+// fetched once per warp with same-address loads (one L1 request per load, broadcast to the
+// lanes) instead of once per lane, every lane tests its own query against the node's four
+// slots, and an internal slot is descended into when any lane's query reaches it.  A lane
+// emits exactly the pairs of the per-thread walk: it emits leaf L when its box overlaps L's
+// and its position is before L's (the order rule), and then it also overlaps every slot box
+// above L (a slot box contains the boxes below it) and is before their rightmost leaves, so
+// the warp, which descends wherever some lane's walk would, reaches L.  Lanes of a warp whose
+// leaves lie in two meshes walk mesh by mesh.
+static __global__ void __launch_bounds__(TRAV_THREADS)
+k_traverse_w(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, const int* __restrict__ leaf_tri,
+             Forest F, int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const int* __restrict__ mflags) {
+    __shared__ int2 cbuf[TRAV_BUF][TRAV_THREADS];     // candidate buffer (see flush_candidates)
+    const unsigned FULL = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31;
+    int nbuf = 0;
+    const int M = forest_size(F);
+    const int total = __ldg(F.voff + M);
+    const int wpb = TRAV_THREADS / 32;
+    const long long wstride = (long long)gridDim.x * wpb * 32;
+    for (long long base = ((long long)blockIdx.x * wpb + (tid >> 5)) * 32; base < total; base += wstride) {
+        const int v = (int)base + lane;
+        const bool valid = v < total;
+        const int m = valid ? find_mesh(F.voff, M, v, 0) : -1;
+        unsigned pending = __ballot_sync(FULL, valid);
+        while (pending) {
+            const int mm = __shfl_sync(FULL, m, __ffs(pending) - 1);
+            const bool mine = valid && m == mm;
+            pending &= ~__ballot_sync(FULL, mine);
+            const int vo = __ldg(F.voff + mm), po = __ldg(F.poff + mm);
+            const int n = __ldg(F.voff + mm + 1) - vo;
+            if (n < 2) continue;
+            if (mflags && (__ldg(mflags + __ldg(F.sid + mm)) & MF_DONE)) continue;
+            const QNode* qn = qnodes + po;
+            const int p = v - vo;
+            bool act = mine;
+            int qid = 0;
+            float qlo[3] = {0.f, 0.f, 0.f}, qhi[3] = {0.f, 0.f, 0.f};
+            if (act) {
+                qid = __ldg(leaf_tri + po + p);
+                const int lq = __ldg(qleaf + po + p);
+                if (qid < 0 || qid >= n || lq < 0 || (lq >> 2) >= n - 1) {
+                    atomicOr(&hdr->status, ST_MALFORMED_TREE);
+                    act = false;
+                } else {
+                    const float* f = reinterpret_cast<const float*>(qn + (lq >> 2));
+                    const int sl = lq & 3;
+                    qlo[0] = __ldg(f + 0 + sl);
+                    qlo[1] = __ldg(f + 4 + sl);
+                    qlo[2] = __ldg(f + 8 + sl);
+                    qhi[0] = __ldg(f + 12 + sl);
+                    qhi[1] = __ldg(f + 16 + sl);
+                    qhi[2] = __ldg(f + 20 + sl);
+                }
+            }
+            if (!__any_sync(FULL, act)) continue;
+            int s0 = 0, s1 = 0;          // the warp's stack, entry e in lane e % 32, word e / 32
+            int sp = 0, node = 0;
+            const int limit = 2 * n + 64;
+            for (int it = 0;; ++it) {
+                if (it > limit) {
+                    if (lane == 0) atomicOr(&hdr->status, ST_MALFORMED_TREE);
+                    break;
+                }
+                const float4* f = reinterpret_cast<const float4*>(qn + node);
+                const float4 LX = __ldg(f + 0), LY = __ldg(f + 1), LZ = __ldg(f + 2);
+                const float4 HX = __ldg(f + 3), HY = __ldg(f + 4), HZ = __ldg(f + 5);
+                const int4 R = __ldg(reinterpret_cast<const int4*>(f + 6));
+                const int4 A = __ldg(reinterpret_cast<const int4*>(f + 7));
+                const float lx[4] = {LX.x, LX.y, LX.z, LX.w}, ly[4] = {LY.x, LY.y, LY.z, LY.w};
+                const float lz[4] = {LZ.x, LZ.y, LZ.z, LZ.w}, hx[4] = {HX.x, HX.y, HX.z, HX.w};
+                const float hy[4] = {HY.x, HY.y, HY.z, HY.w}, hz[4] = {HZ.x, HZ.y, HZ.z, HZ.w};
+                const int rr[4] = {R.x, R.y, R.z, R.w}, aa[4] = {A.x, A.y, A.z, A.w};
+                int next = -1;
+                bool bad = false, deep = false;
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    const int ref = rr[s];
+                    if (ref == Q_EMPTY) continue;
+                    if (ref >= n - 1 || (ref < 0 && ~ref >= n)) { bad = true; continue; }
+                    const int rightmost = ref < 0 ? ~ref : aa[s];
+                    const bool hit = act && p < rightmost && (qlo[0] <= hx[s]) && (qhi[0] >= lx[s]) &&
+                                     (qlo[1] <= hy[s]) && (qhi[1] >= ly[s]) && (qlo[2] <= hz[s]) && (qhi[2] >= lz[s]);
+                    if (ref < 0) {
+                        if (hit) {
+                            const int cid = aa[s];
+                            cbuf[nbuf++][tid] = make_int2(po + min(qid, cid), po + max(qid, cid));
+                            if (nbuf == TRAV_BUF) {
+                                cg::coalesced_group grp = cg::coalesced_threads();
+                                int b0 = 0;
+                                if (grp.thread_rank() == 0) b0 = atomicAdd(&hdr->cand_count, TRAV_BUF * (int)grp.size());
+                                b0 = grp.shfl(b0, 0) + TRAV_BUF * (int)grp.thread_rank();
+                                flush_candidates(cbuf, tid, TRAV_BUF, b0, cand, cand_cap, hdr);
+                                nbuf = 0;
+                            }
+                        }
+                    } else if (__any_sync(FULL, hit)) {
+                        if (next < 0) {
+                            next = ref;
+                        } else if (sp < STACK_DEPTH) {
+                            if (lane == (sp & 31)) {
+                                if (sp < 32) s0 = ref;
+                                else s1 = ref;
+                            }
+                            ++sp;
+                        } else {
+                            deep = true;
+                        }
+                    }
+                }
+                if (bad || deep) {
+                    if (lane == 0) atomicOr(&hdr->status, bad ? ST_MALFORMED_TREE : ST_STACK_OVERFLOW);
+                    break;
+                }
+                if (next >= 0) {
+                    node = next;
+                } else {
+                    if (sp == 0) break;
+                    --sp;
+                    const int w0 = __shfl_sync(FULL, s0, sp & 31), w1 = __shfl_sync(FULL, s1, sp & 31);
+                    node = sp < 32 ? w0 : w1;
+                }
+            }
+        }
+    }
+    if (nbuf > 0) flush_rest(cbuf, tid, nbuf, cand, cand_cap, hdr);
+}
+
 // ---------------------------------------------------------------------------------------
 // Impulse loop
 

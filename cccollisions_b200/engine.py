@@ -184,6 +184,21 @@ class Engine:
         N.check(N.lib().ccc_engine_autotune(self.handle, _stream(self.device), ctypes.byref(c)), "ccc_engine_autotune")
         return int(c.value)
 
+    @staticmethod
+    def schedules() -> list[dict]:
+        """The autotuner's candidate schedules: traversal blocks per SM, narrow-phase blocks
+        per SM (in units of the resident count) and the traversal form (0 one query per
+        thread, 1 32 queries per warp)."""
+        out = []
+        for i in range(N.lib().ccc_engine_schedule_count()):
+            a = (ctypes.c_int32 * 3)()
+            N.check(N.lib().ccc_engine_schedule_info(i, a), "ccc_engine_schedule_info")
+            out.append({"traversal_blocks_per_sm": a[0], "narrow_blocks": a[1], "warp_traversal": a[2]})
+        return out
+
+    def set_schedule(self, choice: int):
+        N.check(N.lib().ccc_engine_set_schedule(self.handle, int(choice)), "ccc_engine_set_schedule")
+
     def state(self, sids: Sequence[int]) -> dict:
         """Synchronises; status word and per-mesh rows, contacts, iterations, flags."""
         a, p, n = _ids(sids)

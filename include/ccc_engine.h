@@ -110,6 +110,14 @@ int ccc_engine_replay(ccc_engine* e, int op, void* stream);
  * only recomputes collision rows.  Choices are cached per (dtype, size class). */
 int ccc_engine_autotune(ccc_engine* e, void* stream, int32_t* choice);
 
+/* The autotuner's candidate schedules (no counterpart in the reference): their number;
+ * the parameters of one (out[0] traversal blocks per SM, out[1] narrow-phase blocks per SM
+ * in units of the resident count, out[2] traversal form: 0 one query per thread, 1 32
+ * queries per warp walking the tree together); and fixing the engine to one of them. */
+int ccc_engine_schedule_count(void);
+int ccc_engine_schedule_info(int32_t choice, int32_t* out);
+int ccc_engine_set_schedule(ccc_engine* e, int32_t choice);
+
 /* Synchronise the stream and read the status word and, for each given mesh, its row
  * count, contacts of the last loop iteration, iterations and flags (NULL to skip). */
 int ccc_engine_read_state(ccc_engine* e, const int32_t* slot_ids, int64_t n, int32_t* status, int32_t* rows,

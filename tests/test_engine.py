@@ -108,6 +108,35 @@ def test_graph_replay_follows_the_active_set(cuda):
     eng.close()
 
 
+@pytest.mark.parametrize("warp", [0, 1])
+def test_every_schedule_gives_the_oracle_rows(cuda, oracle, warp):
+    """Each candidate schedule of the autotuner, with the traversal run one query per thread
+    (k_traverse_q) or 32 queries per warp (k_traverse_w), gives the oracle's rows bit for
+    bit; the meshes are uneven, so warps straddle mesh boundaries."""
+    from cccollisions_b200 import _native as N
+    from cccollisions_b200.engine import Engine
+    meshes = _meshes(11, seed=21)
+    scheds = [i for i, s in enumerate(Engine.schedules()) if s["warp_traversal"] == warp]
+    assert scheds
+    with N.math_library(N.LIB_PORTABLE):
+        eng, sids = _engine(meshes)
+        eng.set_active(sids)
+        eng.build(sids)
+        expect = {}
+        for sid, (x0, x1, _) in zip(sids, meshes):
+            bb, tr = oracle.bvh(x0, x1)
+            expect[sid] = _ms(*oracle.ccd(bb, tr, x0, x1))
+        for i in scheds:
+            eng.set_schedule(i)
+            eng.ccd()
+            st = eng.state(sids)
+            assert st["status"] == 0
+            for sid, n in zip(sids, st["rows"]):
+                r, t = eng.collisions(sid, int(n))
+                assert _ms(r.cpu().numpy(), t.cpu().numpy()) == expect[sid], (i, sid)
+        eng.close()
+
+
 def test_autotune_and_cached_choice(cuda):
     meshes = _meshes(6, seed=9)
     eng, sids = _engine(meshes)
