@@ -14,6 +14,11 @@ plain per-mesh path, with exact pair sets and p50 / p99 latency.
 * ``plain`` — the same 64 meshes through the reference-format API one mesh at a time
   (bvh_motion + find_collisions_continuous, as the reference's caller does); its rows and
   times are compared with the batched form's as multisets (``pair_sets_equal``).
+* ``query`` / ``reference_gpu`` — find_collisions_continuous alone per mesh on the same
+  prebuilt reference-order trees: this library's, and the reference extension's own CUDA
+  path (compiled unmodified from its sources into oracle/_ref; a baseline leg, like
+  ``cpu_baseline``), whose rows are compared with the batched form's.  The reference's
+  bvh_motion is not run: its split search can loop without end on a GPU.
 * ``served`` — a Poisson stream of impulse-loop requests (rate 2,000/s, meshes of
   log-uniform 2e3..2e5 triangles as in the impulse workload) under a 40 GB engine budget:
   throughput (request triangles over the makespan) and p50 / p99 latency (arrival to result
@@ -30,7 +35,8 @@ plain per-mesh path, with exact pair sets and p50 / p99 latency.
 
 Multi-GPU: meshes are independent and the step has no exchange, so N ranks run N replicas
 ("replicas only"); value is the total over ranks divided by the slowest rank.
-``--impl reference`` times the CPU implementation of the path (the oracle) on rank 0 only.
+``--impl reference`` times the CPU implementation of the path (the oracle) on rank 0 only,
+whole steps over every mesh of the same workload.
 """
 from __future__ import annotations
 
@@ -142,6 +148,31 @@ class ClockSampler:
 def batched_meshes(n):
     from cccollisions_b200 import workloads as W
     return W.batched(n)
+
+
+def workload_config(meshes, world):
+    """The workload, identical on both arms (no results in it)."""
+    return {"workload": f"batched CCD: {len(meshes)} cloth+icosphere meshes (1e3..1e5 cloth tris + 20,480 sphere "
+                        f"tris each)",
+            "triangles": int(sum(x0.shape[0] for x0, _ in meshes)), "meshes": len(meshes),
+            "max_candidates_per_triangle": MAXC, "max_collisions_per_triangle": MAXCOL, "positions": "fp64",
+            "step": "refit + traversal + continuous narrow phase of every mesh",
+            "l2": "flushed between steps (256 MiB write); inputs 377 MB > L2",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+
+def load_reference_extension():
+    """The reference's own CUDA extension, compiled from its sources (unmodified) by
+    oracle/build_ref.py into oracle/_ref/cccollisions.so, or None where it was not built.
+    Used only by the reference-GPU baseline leg."""
+    import importlib.util
+    so = os.path.join(ROOT, "oracle", "_ref", "cccollisions.so")
+    if not os.path.exists(so):
+        return None
+    spec = importlib.util.spec_from_file_location("cccollisions", so)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
 
 
 def cpu_sample(meshes, seconds):
@@ -271,6 +302,7 @@ def run_ours(args, rank, world, dev):
     # ---------------- plain per-mesh path through the reference-format API
     X = [(torch.from_numpy(x0).to(dev), torch.from_numpy(x1).to(dev)) for x0, x1 in meshes]
     api.CHECK_STATUS = True
+    api.STRICT = True              # a candidate or row overflow would raise: no truncated sets
     plain_out = None
 
     def plain():
@@ -280,26 +312,62 @@ def run_ours(args, rank, world, dev):
             out.append(C.find_collisions_continuous(bb, tr, X0[None], X1[None], MAXC, MAXCOL))
         return out
 
+    def timed(fn, n):
+        ms, res = [], None
+        for i in range(n):
+            flush.fill_(i & 0xFF)
+            torch.cuda.synchronize(dev)
+            a, b = ev(), ev()
+            a.record()
+            res = fn()
+            b.record()
+            torch.cuda.synchronize(dev)
+            ms.append(a.elapsed_time(b))
+        return statistics.mean(ms), res
+
     torch.cuda.synchronize(dev)
     for _ in range(warm):
         plain_out = plain()
-    torch.cuda.synchronize(dev)
-    pms = []
-    for i in range(args.steps):
-        flush.fill_(i & 0xFF)
-        torch.cuda.synchronize(dev)
-        a, b = ev(), ev()
-        a.record()
-        plain_out = plain()
-        b.record()
-        torch.cuda.synchronize(dev)
-        pms.append(a.elapsed_time(b))
-    plain_ms = statistics.mean(pms)
-    equal = True
-    for sid, (rows, times) in zip(sids, plain_out):
-        r = rows[0].cpu().numpy()
-        k = int((r[:, 0] >= 0).sum())
-        equal &= _ms(r[:k], times[0, :k, 0].cpu().numpy()) == batched_rows[sid]
+    plain_ms, plain_out = timed(plain, args.steps)
+
+    def rows_of(out):
+        res = []
+        for rows, times in out:
+            r = rows[0].cpu().numpy()
+            k = int((r[:, 0] >= 0).sum())
+            res.append(_ms(r[:k], times[0, :k, 0].cpu().numpy()))
+        return res
+
+    equal = all(a == batched_rows[sid] for sid, a in zip(sids, rows_of(plain_out)))
+
+    # ---------------- query-only legs on the same reference-order trees: this library's
+    # find_collisions_continuous and the reference extension's own (its bvh_motion is not
+    # run: its split search can loop without end on a GPU)
+    trees = [C.bvh_motion(X0[None], X1[None]) for X0, X1 in X]
+
+    def query():
+        return [C.find_collisions_continuous(bb, tr, X0[None], X1[None], MAXC, MAXCOL) for (bb, tr), (X0, X1) in
+                zip(trees, X)]
+
+    query()
+    query_ms, _ = timed(query, args.steps)
+    api.STRICT = False
+    ref_gpu = None
+    R = load_reference_extension()
+    if R is None:
+        ref_gpu = {"unavailable": "the reference extension (oracle/_ref/cccollisions.so) is not built"}
+    else:
+        def ref_query():
+            return [R.find_collisions_continuous(bb, tr, X0[None], X1[None], MAXC, MAXCOL) for (bb, tr), (X0, X1)
+                    in zip(trees, X)]
+
+        ref_steps = max(1, min(args.steps, 5))
+        ref_query()
+        ref_ms, ref_out = timed(ref_query, ref_steps)
+        ref_equal = all(a == batched_rows[sid] for sid, a in zip(sids, rows_of(ref_out)))
+        ref_gpu = {"value": world * total / (ref_ms / 1e3), "ms_per_step": ref_ms, "steps": ref_steps,
+                   "rows_equal_batched": bool(ref_equal),
+                   "path": "reference extension: find_collisions_continuous per mesh on prebuilt trees"}
 
     # ---------------- rooflines
     peak, peak_kind = load_peaks()
@@ -319,50 +387,40 @@ def run_ours(args, rank, world, dev):
     result = None
     if rank == 0:
         clocks = clk.summary()
+        r3 = lambda x: float(f"{x:.4g}")
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": warm,
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded cloth grids + icospheres)",
-            "config": {"workload": f"batched: {len(meshes)} cloth+icosphere meshes, log-uniform 1e3..1e5 cloth "
-                                   f"triangles + 20,480 sphere triangles each, one CUDA-graph replay per step",
-                       "triangles": total, "meshes": len(meshes), "max_candidates_per_triangle": MAXC,
-                       "max_collisions_per_triangle": MAXCOL, "positions": "fp64", "tree_boxes": "fp32",
-                       "l2": "flushed between steps (256 MiB write); inputs (377 MB) larger than L2",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "autotuned_shape": shape, "candidates": cnt["candidates"], "subtests": cnt["subtests"],
-                       "roots_in_unit_interval": cnt["roots"], "collision_rows": int(sum(nrow)),
-                       "status": cnt["status"]},
-            "plain": {"value": world * total / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
-                      "path": "per mesh: bvh_motion + find_collisions_continuous (reference-format API)"},
-            "batched_over_plain": plain_ms / ms_per_step,
-            "pair_sets_equal": bool(equal),
-            "e2e": {"value": world * total / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
-                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "path": "engine.StepPipeline: per step, H2D of both soups of every mesh from page-locked "
-                            "memory, graph replay, device packing of the rows, D2H of rows + times; copies of "
-                            "step k overlap the kernels of steps k-1 / k+1",
-                    "rows_equal_batched": bool(e2e_equal)},
+            "gpu_launches": int(launches),
+            "config": workload_config(meshes, world),
             "roofline": {"kernel": dname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
                          "traffic": (NARROW_DRAM_BYTES_PER_PAIR * cnt["candidates"]) if dname == "k_ccd_narrow"
                          else None,
-                         "traffic_source": "ncu DRAM bytes per candidate pair of the 16-mesh capture, times this "
-                                           "launch's pairs",
-                         "alg_bytes_per_launch": narrow_bytes, "launch_ms": per_launch,
-                         "note": "the narrow phase is FP64-latency bound; see fp64"},
-            "fp64": {"kernel": "k_ccd_narrow", "achieved_gflops": fp64_gflops,
-                     "peak_gflops": FP64_PEAK_NOMINAL_GFLOPS, "peak_source": "nominal (B200 datasheet)",
-                     "frac": fp64_gflops / FP64_PEAK_NOMINAL_GFLOPS, "flops_per_subtest": FLOPS_PER_SUBTEST},
-            "refit_roofline": {"kernel": "k_engine_refit + k_engine_refit_front", "bound": "hbm", "alg_bytes": rb, "launch_ms": refit_ms,
-                               "achieved": rb / (refit_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                               "frac": rb / (refit_ms / 1e3) / 1e9 / peak},
-            "build_roofline": {"kernels": "bounds, Morton, radix sort, Karras, refit", "bound": "hbm",
-                               "alg_bytes": bb_, "ms": build_ms, "achieved": bb_ / (build_ms / 1e3) / 1e9,
-                               "peak": peak, "unit": "GB/s", "frac": bb_ / (build_ms / 1e3) / 1e9 / peak},
-            "kernel_ms_per_step": {k: v[0] / v[1] for k, v in kern.items()},
-            "kernel_share": {k: round(v[0] / sum(x[0] for x in kern.values()), 4) for k, v in kern.items()},
-            "gpu_launches": int(launches),
+                         "alg_bytes_per_launch": narrow_bytes, "launch_ms": per_launch},
             "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+            "e2e": {"value": world * total / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "path": "engine.StepPipeline from pinned host memory, rows + times back",
+                    "rows_equal_batched": bool(e2e_equal)},
+            "work": {"autotuned_shape": shape, "candidates": cnt["candidates"], "subtests": cnt["subtests"],
+                     "roots_in_unit_interval": cnt["roots"], "collision_rows": int(sum(nrow)), "status": cnt["status"],
+                     "tree_boxes": "fp32"},
+            "kernel_ms_per_step": {k: r3(v[0] / v[1]) for k, v in kern.items()},
+            "fp64": {"kernel": "k_ccd_narrow", "achieved_gflops": r3(fp64_gflops),
+                     "peak_gflops": FP64_PEAK_NOMINAL_GFLOPS, "peak_source": "nominal (B200 datasheet)",
+                     "frac": r3(fp64_gflops / FP64_PEAK_NOMINAL_GFLOPS)},
+            "refit_roofline": {"alg_bytes": rb, "ms": r3(refit_ms), "achieved": r3(rb / (refit_ms / 1e3) / 1e9),
+                               "peak": peak, "unit": "GB/s", "frac": r3(rb / (refit_ms / 1e3) / 1e9 / peak)},
+            "build_roofline": {"alg_bytes": bb_, "ms": r3(build_ms), "achieved": r3(bb_ / (build_ms / 1e3) / 1e9),
+                               "peak": peak, "unit": "GB/s", "frac": r3(bb_ / (build_ms / 1e3) / 1e9 / peak)},
+            "plain": {"value": world * total / (plain_ms / 1e3), "ms_per_step": plain_ms,
+                      "path": "per mesh: bvh_motion + find_collisions_continuous"},
+            "query": {"value": world * total / (query_ms / 1e3), "ms_per_step": query_ms,
+                      "path": "per mesh: find_collisions_continuous on prebuilt trees"},
+            "reference_gpu": ref_gpu,
+            "pair_sets_equal": bool(equal),
         }
     return result, meshes
 
@@ -426,41 +484,49 @@ def run_served(args, dev):
     torch.cuda.synchronize(dev)
     dt = time.perf_counter() - t0
     ptris = sum(r.F for r in sample)
-    return {"value": st["throughput"], "unit": UNIT, "requests": st["requests"], "rate_per_s": 2000.0,
-            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "makespan_s": st["makespan_s"],
-            "request_triangles": st["triangles"], "ticks": st["ticks"], "mean_iterations": st["mean_iterations"],
-            "converged_fraction": st["converged"], "budget_gb": args.served_budget_gb,
-            "policy": f"FIFO admission, at most {srv.max_active_triangles} active triangles (a request alone is "
-                      "always admitted)",
-            "request": "impulse loop (max 50 iterations) on an impulse-workload mesh of log-uniform 2e3..2e5 "
-                       "triangles, fp64",
+    r3 = lambda x: float(f"{x:.4g}")
+    return {"value": r3(st["throughput"]), "unit": UNIT, "requests": st["requests"], "rate_per_s": 2000.0,
+            "p50_ms": r3(st["p50_ms"]), "p99_ms": r3(st["p99_ms"]), "mean_ms": r3(st["mean_ms"]),
+            "makespan_s": r3(st["makespan_s"]), "request_triangles": st["triangles"], "ticks": st["ticks"],
+            "mean_iterations": st["mean_iterations"], "converged_fraction": st["converged"],
+            "contacts_first_iteration": st["contacts_first_iteration"],
+            "contacts_last_iteration": st["contacts_last_iteration"],
+            "contacts_all_iterations": st["contacts_all_iterations"], "budget_gb": args.served_budget_gb,
+            "max_active_triangles": srv.max_active_triangles,
             "same_set": {"requests": len(sample), "triangles": ptris,
-                         "engine": {"value": same["throughput"], "seconds": same["makespan_s"],
-                                    "mean_iterations": same["mean_iterations"]},
-                         "plain": {"value": ptris / dt, "seconds": dt, "mean_iterations": float(np.mean(its)),
-                                   "path": "per request, one after another: bvh_motion + compute_impulses per "
-                                           "iteration, per-vertex averaging with torch"}}}
+                         "engine": {"value": r3(same["throughput"]), "seconds": r3(same["makespan_s"])},
+                         "plain": {"value": r3(ptris / dt), "seconds": r3(dt), "mean_iterations": float(np.mean(its))}}}
 
 
 def run_reference(args):
+    """The CPU implementation of the path (the oracle: C++ restatement of the reference's
+    bvh_motion + find_collisions_continuous, all host threads), whole steps over every mesh
+    of the same workload: W untimed steps, then K timed ones (wall clock)."""
+    from oracle import oracle as O
+    O.build()
     meshes = batched_meshes(args.meshes)
-    per = max(1.0, args.cpu_seconds / max(args.steps + args.warmup, 1))
-    vals = []
-    desc, threads = "", 0
-    for i in range(args.warmup + args.steps):
-        v, threads, desc = cpu_sample(meshes, per)
-        if i >= args.warmup:
-            vals.append(v)
-    v = statistics.median(vals)
+    nthreads = O.num_threads()
+    total = sum(x0.shape[0] for x0, _ in meshes)
+
+    def step():
+        for x0, x1 in meshes:
+            bb, tr = O.bvh(x0, x1)
+            O.ccd(bb, tr, x0, x1, nthreads=nthreads)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    v = total / (ms / 1e3)
     return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": sum(x0.shape[0] for x0, _ in meshes) / v * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded cloth grids + icospheres)",
-            "config": {"workload": f"batched: {len(meshes)} cloth+icosphere meshes (CPU sample per step)",
-                       "triangles": sum(x0.shape[0] for x0, _ in meshes)},
-            "impl": "reference",
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"per step: {desc}"},
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cloth grids + icospheres)",
+            "config": workload_config(meshes, args.gpus), "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
+                             "sample": f"every step: all {len(meshes)} meshes ({total} triangles), bvh_motion + "
+                                       f"continuous collisions per mesh"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -484,13 +550,19 @@ def main():
         if world > 1:
             torch.distributed.barrier()
         if rank == 0:
+            if world == 1:
+                v, threads, desc = cpu_sample(meshes, args.cpu_seconds)
+                res["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
             if world == 1 and args.served_requests > 0:
                 res["served"] = run_served(args, dev)
                 ss = res["served"]["same_set"]
                 res["served_over_plain"] = ss["engine"]["value"] / ss["plain"]["value"]
-            if world == 1:
-                v, threads, desc = cpu_sample(meshes, args.cpu_seconds)
-                res["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
+            # the headline ratios last, so that any tail of the line holds them
+            res["batched_over_plain"] = res["plain"]["ms_per_step"] / res["ms_per_step"]
+            rg = res["reference_gpu"]
+            if rg and "ms_per_step" in rg:
+                res["batched_over_reference_gpu"] = rg["ms_per_step"] / res["ms_per_step"]
+                res["query_over_reference_gpu"] = rg["ms_per_step"] / res["query"]["ms_per_step"]
             print(json.dumps(res))
     finally:
         if world > 1:

@@ -53,10 +53,14 @@ def test_admission_waits_for_memory(cuda):
     from cccollisions_b200.serve import Server, engine_capacity
     reqs = _requests(6, seed=5, lo=20, hi=22, spacing=0.0)
     biggest = max(r.F for r in reqs)
-    # a block with room for about two requests at a time
-    budget = 1 << 20
-    while engine_capacity(budget, mesh_capacity=8, vert_ratio=1.0)[0] < 2 * biggest + 16:
-        budget *= 2
+    # a block with room for about two requests at a time, beside the library's fixed
+    # module-data array
+    from cccollisions_b200 import _native as N
+    fixed = N.lib().ccc_static_scratch_bytes()
+    extra = 1 << 16
+    while engine_capacity(fixed + extra, mesh_capacity=8, vert_ratio=1.0)[0] < 2 * biggest + 16:
+        extra *= 2
+    budget = fixed + extra
     srv = Server(budget_bytes=budget, mesh_capacity=8, vert_ratio=1.0)
     tc = engine_capacity(budget, mesh_capacity=8, vert_ratio=1.0)[0]
     assert tc < sum(r.F for r in reqs)               # not everything fits at once
