@@ -759,9 +759,10 @@ k_traverse_q(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, co
 // Warp-cooperative form of k_traverse_q (collisions_static.cu:10-103): the 32 lanes of a warp
 // take 32 consecutive query leaves and walk the QNode tree together with one stack, held
 // across the lanes' registers (entry e in lane e % 32, word e / 32).  Each visited QNode is
-// fetched once per warp with same-address loads (one L1 request per load, broadcast to the
-// lanes) instead of once per lane, every lane tests its own query against the node's four
-// slots, and an internal slot is descended into when any lane's query reaches it.  A lane
+// staged once per warp in shared memory (one coalesced 128-byte load, a word per lane) and
+// read from there by every lane, instead of being fetched once per lane; every lane tests
+// its own query against the node's four slots, and an internal slot is descended into when
+// any lane's query reaches it.  A lane
 // emits exactly the pairs of the per-thread walk: it emits leaf L when its box overlaps L's
 // and its position is before L's (the order rule), and then it also overlaps every slot box
 // above L (a slot box contains the boxes below it) and is before their rightmost leaves, so
@@ -771,12 +772,15 @@ static __global__ void __launch_bounds__(TRAV_THREADS)
 k_traverse_w(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, const int* __restrict__ leaf_tri,
              Forest F, int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const int* __restrict__ mflags) {
     __shared__ int2 cbuf[TRAV_BUF][TRAV_THREADS];     // candidate buffer (see flush_candidates)
+    __shared__ __align__(16) int nbuf_s[TRAV_THREADS / 32][32];    // each warp's staged QNode
     const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31;
     int nbuf = 0;
     const int M = forest_size(F);
     const int total = __ldg(F.voff + M);
     const int wpb = TRAV_THREADS / 32;
+    int* stage = nbuf_s[tid >> 5];
+    const float4* sf = reinterpret_cast<const float4*>(stage);
     const long long wstride = (long long)gridDim.x * wpb * 32;
     for (long long base = ((long long)blockIdx.x * wpb + (tid >> 5)) * 32; base < total; base += wstride) {
         const int v = (int)base + lane;
@@ -822,11 +826,13 @@ k_traverse_w(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, co
                     if (lane == 0) atomicOr(&hdr->status, ST_MALFORMED_TREE);
                     break;
                 }
-                const float4* f = reinterpret_cast<const float4*>(qn + node);
-                const float4 LX = __ldg(f + 0), LY = __ldg(f + 1), LZ = __ldg(f + 2);
-                const float4 HX = __ldg(f + 3), HY = __ldg(f + 4), HZ = __ldg(f + 5);
-                const int4 R = __ldg(reinterpret_cast<const int4*>(f + 6));
-                const int4 A = __ldg(reinterpret_cast<const int4*>(f + 7));
+                // stage the node: word `lane` of its 128 bytes from each lane
+                __syncwarp();
+                stage[lane] = __ldg(reinterpret_cast<const int*>(qn + node) + lane);
+                __syncwarp();
+                const float4 LX = sf[0], LY = sf[1], LZ = sf[2], HX = sf[3], HY = sf[4], HZ = sf[5];
+                const int4 R = reinterpret_cast<const int4*>(sf)[6];
+                const int4 A = reinterpret_cast<const int4*>(sf)[7];
                 const float lx[4] = {LX.x, LX.y, LX.z, LX.w}, ly[4] = {LY.x, LY.y, LY.z, LY.w};
                 const float lz[4] = {LZ.x, LZ.y, LZ.z, LZ.w}, hx[4] = {HX.x, HX.y, HX.z, HX.w};
                 const float hy[4] = {HY.x, HY.y, HY.z, HY.w}, hz[4] = {HZ.x, HZ.y, HZ.z, HZ.w};
