@@ -279,7 +279,7 @@ int ccd_impl(const void* bboxes, const int64_t* tree, const void* x0, const void
     cudaError_t le = cudaSuccess;
     CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV>(
         num_sms() * CCD_MIN_BLOCKS, s, P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, (long long*)rows,
-        (T*)times, (int)maxcol, P.mesh_cnt, CornerSink<T>{})));
+        (T*)times, (int)maxcol, P.mesh_cnt, Weld{}, CornerSink<T>{})));
     if (le != cudaSuccess) return CCC_ERR_CUDA;
     CCC_LAUNCH_CHECK();
     return CCC_OK;
@@ -296,7 +296,7 @@ int mincol_impl(const void* bboxes, const int64_t* tree, const void* x0, const v
     cudaError_t le = cudaSuccess;
     CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_MINCOL, CornerSink<T>, LIB_PORTABLE>(
         num_sms() * CCD_MIN_BLOCKS, s, P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, (long long*)rows,
-        nullptr, (int)(maxc * 15), P.mesh_cnt, CornerSink<T>{}));
+        nullptr, (int)(maxc * 15), P.mesh_cnt, Weld{}, CornerSink<T>{}));
     if (le != cudaSuccess) return CCC_ERR_CUDA;
     CCC_LAUNCH_CHECK();
     return CCC_OK;
@@ -329,7 +329,7 @@ int impulses_impl(const void* bboxes, const int64_t* tree, const void* x0, const
     cudaError_t le = cudaSuccess;
     CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_IMPULSES, CornerSink<T>, LIBV>(
         num_sms() * CCD_MIN_BLOCKS, s, P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, nullptr, nullptr, 0,
-        P.mesh_cnt, CornerSink<T>{(const T*)masses, (T*)dv, (T*)dx, (int*)cnt})));
+        P.mesh_cnt, Weld{}, CornerSink<T>{(const T*)masses, (T*)dv, (T*)dx, (int*)cnt})));
     if (le != cudaSuccess) return CCC_ERR_CUDA;
     CCC_LAUNCH_CHECK();
     return CCC_OK;

@@ -53,7 +53,8 @@ struct EngineLayout {
     int64_t leaf_tri, lparent, nparent, visits, nodes, qnodes, qcode, qleaf, nrange, front;
     int64_t rows, times, cand;
     int64_t keys0, keys1, vals0, vals1, hist;
-    int64_t verts0, verts1, vel, acc, end;
+    int64_t verts0, verts1, vel, acc;
+    int64_t wtab, vidc, wcnt, fan_end, fan, vid4, twin4, third4, stage, live, end;
     int64_t zero_bytes, hist_len, cand_cap;
 };
 
@@ -103,6 +104,18 @@ EngineLayout engine_layout(int64_t tsz, int64_t tc, int64_t vc, int64_t mc, int6
     L.verts1 = take(vc * 3 * tsz);
     L.vel = take(vc * 3 * tsz);
     L.acc = take(vc * 8 * 8);
+    // corner classes (Weld): table (then the classes' first member entries), per-corner-id
+    // arrays (4 ids per slot), member list
+    L.wtab = take(tc * 6 * 4);
+    L.vidc = take(tc * 4 * 4);
+    L.wcnt = take(tc * 4 * 4);
+    L.fan_end = take(tc * 4 * 4);
+    L.fan = take(tc * 3 * 16);
+    L.vid4 = take(tc * 16);
+    L.twin4 = take(tc * 16);
+    L.third4 = take(tc * 16);
+    L.stage = take(L.cand_cap * 4);
+    L.live = take(L.cand_cap * 16);
     L.end = o;
     return L;
 }
@@ -273,18 +286,75 @@ template <class T> int traverse(ccc_engine* e, const Tables& t, const int* flags
     return CCC_OK;
 }
 
+// corner classes of the active meshes' current positions (k_weld_*)
+template <class T> int weld(ccc_engine* e, const Tables& t, cudaStream_t s) {
+    const EngineLayout& L = e->L;
+    if (cudaMemsetAsync(e->base + L.wtab, 0xff, e->tri_cap * 6 * 4, s) != cudaSuccess ||
+        cudaMemsetAsync(e->base + L.wcnt, 0, e->tri_cap * 4 * 4, s) != cudaSuccess)
+        return CCC_ERR_CUDA;
+    const T* x0 = e->at<T>(L.x0);
+    const T* x1 = e->at<T>(L.x1);
+    int* vidc = e->at<int>(L.vidc);
+    int* cnt = e->at<int>(L.wcnt);
+    int* fan_end = e->at<int>(L.fan_end);
+    CCC_LAUNCH("k_weld_insert", s, k_weld_insert<T><<<item_grid(), ITEM_THREADS, 0, s>>>(
+        t.f, x0, e->at<int>(L.wtab), vidc, e->hdr()));
+    CCC_LAUNCH_CHECK();
+    CCC_LAUNCH("k_weld_count", s, k_weld_count<T><<<item_grid(), ITEM_THREADS, 0, s>>>(t.f, x0, x1, vidc, cnt));
+    CCC_LAUNCH_CHECK();
+    // (the table is not read after k_weld_insert: its space holds the classes' first entries)
+    int* fan_start = e->at<int>(L.wtab);
+    CCC_LAUNCH("k_weld_alloc", s, k_weld_alloc<<<item_grid(), WELD_THREADS, 0, s>>>(
+        t.f, vidc, cnt, fan_start, fan_end, e->hdr()));
+    CCC_LAUNCH_CHECK();
+    CCC_LAUNCH("k_weld_fill", s, k_weld_fill<<<item_grid(), ITEM_THREADS, 0, s>>>(
+        t.f, vidc, fan_start, fan_end, e->at<int4>(L.fan)));
+    CCC_LAUNCH_CHECK();
+    CCC_LAUNCH("k_weld_sort", s, k_weld_sort<<<item_grid(), ITEM_THREADS, 0, s>>>(t.f, vidc, cnt, fan_end, e->at<int4>(L.fan)));
+    CCC_LAUNCH_CHECK();
+    CCC_LAUNCH("k_weld_tri", s, k_weld_tri<<<item_grid(), ITEM_THREADS, 0, s>>>(
+        t.f, vidc, cnt, fan_start, e->at<int4>(L.fan), e->at<int4>(L.vid4), e->at<int4>(L.twin4),
+        e->at<int4>(L.third4)));
+    CCC_LAUNCH_CHECK();
+    return CCC_OK;
+}
+
+Weld engine_weld(ccc_engine* e) {
+    const EngineLayout& L = e->L;
+    return Weld{e->at<int4>(L.vid4), e->at<int4>(L.fan), e->at<int4>(L.twin4), e->at<int4>(L.third4),
+                e->at<int4>(L.live)};
+}
+
+// the sub-tests of every candidate pair, for the narrow phase (k_ccd_stage_*)
+template <class T> int stage(ccc_engine* e, cudaStream_t s) {
+    CCC_LAUNCH("k_ccd_stage_mask", s, k_ccd_stage_mask<T><<<num_sms() * 2, STAGE_THREADS, 0, s>>>(
+        e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), engine_weld(e),
+        e->at<unsigned>(e->L.stage)));
+    CCC_LAUNCH_CHECK();
+    CCC_LAUNCH("k_ccd_stage_solvers", s, k_ccd_stage_solvers<<<num_sms() * 8, STAGE_THREADS, 0, s>>>(
+        e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), engine_weld(e), e->at<unsigned>(e->L.stage),
+        e->at<int4>(e->L.live)));
+    CCC_LAUNCH_CHECK();
+    return CCC_OK;
+}
+
 template <class T> int ccd_step(ccc_engine* e, cudaStream_t s) {
     if (cudaMemsetAsync(e->base, 0, e->L.zero_bytes, s) != cudaSuccess) return CCC_ERR_CUDA;
     Tables t = e->active();
-    int rc = refit<T>(e, t, nullptr, s);
+    int rc = weld<T>(e, t, s);
+    if (rc) return rc;
+    rc = refit<T>(e, t, nullptr, s);
     if (rc) return rc;
     rc = traverse<T>(e, t, nullptr, s);
+    if (rc) return rc;
+    rc = stage<T>(e, s);
     if (rc) return rc;
     int g = num_sms() * CCD_MIN_BLOCKS * SHAPES[e->shape].narrow;
     cudaError_t le = cudaSuccess;
     CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV>(
         g, s, e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f,
-        e->at<long long>(e->L.rows), e->at<T>(e->L.times), (int)e->maxcol, e->at<int>(e->L.mesh_cnt), CornerSink<T>{})));
+        e->at<long long>(e->L.rows), e->at<T>(e->L.times), (int)e->maxcol, e->at<int>(e->L.mesh_cnt), engine_weld(e),
+        CornerSink<T>{})));
     if (le != cudaSuccess) return CCC_ERR_CUDA;
     CCC_LAUNCH_CHECK();
     return CCC_OK;
@@ -295,16 +365,20 @@ template <class T> int loop_step(ccc_engine* e, int max_iter, cudaStream_t s) {
     Tables t = e->active();
     int* flags = e->at<int>(e->L.flags);
     int* contacts = e->at<int>(e->L.contacts);
-    int rc = refit<T>(e, t, flags, s);
+    int rc = weld<T>(e, t, s);
+    if (rc) return rc;
+    rc = refit<T>(e, t, flags, s);
     if (rc) return rc;
     rc = traverse<T>(e, t, flags, s);
+    if (rc) return rc;
+    rc = stage<T>(e, s);
     if (rc) return rc;
     int g = num_sms() * CCD_MIN_BLOCKS * SHAPES[e->shape].narrow;
     LoopSink<T> sink{e->at<T>(e->L.masses), e->at<int>(e->L.faces), t.vt, e->at<long long>(e->L.acc), contacts};
     cudaError_t le = cudaSuccess;
     CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIBV>(
         g, s, e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f, nullptr,
-        nullptr, 0, e->at<int>(e->L.mesh_cnt), sink)));
+        nullptr, 0, e->at<int>(e->L.mesh_cnt), engine_weld(e), sink)));
     if (le != cudaSuccess) return CCC_ERR_CUDA;
     CCC_LAUNCH_CHECK();
     CCC_LAUNCH("k_loop_update", s, k_loop_update<<<grid_for(e->mesh_cap, ITEM_THREADS), ITEM_THREADS, 0, s>>>(
@@ -742,7 +816,17 @@ int ccc_engine_pack_rows(ccc_engine* e, int64_t* out_rows, void* out_times, int6
 
 int ccc_engine_counters(ccc_engine* e, int32_t* out, void* stream) {
     if (!e || !out) return CCC_ERR_INVALID_ARG;
-    return ccc_read_counters(e->base + e->L.hdr, out, stream);
+    cudaStream_t s = (cudaStream_t)stream;
+    WsHeader h;
+    if (cudaMemcpyAsync(&h, e->base + e->L.hdr, sizeof(WsHeader), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return CCC_ERR_CUDA;
+    out[0] = h.status;
+    out[1] = h.cand_count;
+    out[2] = h.subtests;
+    out[3] = h.roots;
+    out[4] = h.solved;
+    return CCC_OK;
 }
 
 int ccc_engine_read_state(ccc_engine* e, const int32_t* ids, int64_t n, int32_t* status, int32_t* rows,

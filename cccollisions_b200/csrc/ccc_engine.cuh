@@ -456,6 +456,261 @@ static __global__ void k_qtree_slots(Forest F, const TNode* __restrict__ nodes, 
 }
 
 // ---------------------------------------------------------------------------------------
+// Corner classes of the active meshes (Weld, for the narrow phase's repeated sub-tests),
+// rebuilt in every step because the caller may rewrite the positions between steps.  Mesh
+// m owns the part [6 poff[m], 6 (poff[m] + F_m)) of an open-addressing table of corner ids
+// (4 * slot + corner), twice its corner count, cleared to -1 before k_weld_insert:
+//  * k_weld_insert: every corner looks for an entry with its start position (compared with
+//    ==, so -0 meets +0 and NaN meets nothing) and claims an empty one otherwise; the
+//    claiming corner is the class's representative;
+//  * k_weld_count: class sizes (cnt, zeroed before), and CLS_NODEDUP on a class with a
+//    corner that differs from the representative in a bit of either position or whose
+//    coordinates do not come back from their displacement (x0 + (x1 - x0) != x1);
+//  * k_weld_alloc: each class's range of the member list (a block-wide scan and one atomic
+//    per block), k_weld_fill: the members with their triangles' classes, k_weld_sort: each
+//    class's members in ascending corner id;
+//  * k_weld_tri: each triangle's classes, named by their first entry in the member list,
+//    with CLS_NODEDUP also for classes of more than WELD_FANCAP corners and the three class
+//    sizes, and the twin of each edge with the class of the twin's third corner.
+// The classes are a function of the positions; which corner represents a class depends on
+// the order of arrival, which no result depends on.
+
+__device__ __forceinline__ unsigned long long weld_mix(unsigned long long z) {     // SplitMix64 finaliser
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+template <class T> __device__ __forceinline__ unsigned long long weld_key(T v) {
+    const T z = v + (T)0;    // -0 + 0 = +0
+    return sizeof(T) == 4 ? (unsigned long long)__float_as_uint((float)z)
+                          : (unsigned long long)__double_as_longlong((double)z);
+}
+template <class T> __device__ __forceinline__ unsigned long long weld_bits(T v) {
+    return sizeof(T) == 4 ? (unsigned long long)__float_as_uint((float)v)
+                          : (unsigned long long)__double_as_longlong((double)v);
+}
+
+// the mesh and data slot of work item v (triangle position) of the active table
+struct WeldItem {
+    int m, n, po;
+    long long slot;
+};
+__device__ __forceinline__ WeldItem weld_item(const Forest& F, int M, int v) {
+    WeldItem w;
+    w.m = find_mesh(F.voff, M, v, 0);
+    const int vo = __ldg(F.voff + w.m);
+    w.po = __ldg(F.poff + w.m);
+    w.n = __ldg(F.voff + w.m + 1) - vo;
+    w.slot = (long long)w.po + (v - vo);
+    return w;
+}
+
+template <class T>
+__global__ void k_weld_insert(Forest F, const T* __restrict__ x0, int* tab, int* __restrict__ vidc, WsHeader* hdr) {
+    const int M = forest_size(F);
+    const int total = __ldg(F.voff + M);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
+        const WeldItem w = weld_item(F, M, v);
+        int* part = tab + 6LL * w.po;
+        const unsigned long long size = 6ull * (unsigned long long)w.n;
+        for (int c = 0; c < 3; ++c) {
+            const T* p = x0 + w.slot * 9 + 3 * c;
+            const T px = __ldg(p), py = __ldg(p + 1), pz = __ldg(p + 2);
+            const unsigned long long h = weld_mix(weld_key(px) ^ weld_mix(weld_key(py) ^ weld_mix(weld_key(pz))));
+            unsigned long long at = __umul64hi(h, size);
+            const int id = (int)(4 * w.slot + c);
+            int rep = -1;
+            for (unsigned long long probe = 0; probe < size; ++probe) {
+                int cur = __ldcg(part + at);
+                if (cur == -1) {
+                    cur = atomicCAS(part + at, -1, id);
+                    if (cur == -1) {
+                        rep = id;
+                        break;
+                    }
+                }
+                const T* q = x0 + (long long)(cur >> 2) * 9 + 3 * (cur & 3);
+                if (__ldg(q) == px && __ldg(q + 1) == py && __ldg(q + 2) == pz) {
+                    rep = cur;
+                    break;
+                }
+                if (++at == size) at = 0;
+            }
+            // (the table has twice the mesh's corners, so every corner finds its entry)
+            if (rep < 0) {
+                atomicOr(&hdr->status, ST_MALFORMED_TREE);
+                rep = id;
+            }
+            vidc[id] = rep;
+        }
+    }
+}
+
+template <class T>
+__global__ void k_weld_count(Forest F, const T* __restrict__ x0, const T* __restrict__ x1,
+                             const int* __restrict__ vidc, int* cnt) {
+    const int M = forest_size(F);
+    const int total = __ldg(F.voff + M);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
+        const WeldItem w = weld_item(F, M, v);
+        for (int c = 0; c < 3; ++c) {
+            const int id = (int)(4 * w.slot + c);
+            const int rep = __ldg(vidc + id);
+            const T* p0 = x0 + w.slot * 9 + 3 * c;
+            const T* p1 = x1 + w.slot * 9 + 3 * c;
+            const T* r0 = x0 + (long long)(rep >> 2) * 9 + 3 * (rep & 3);
+            const T* r1 = x1 + (long long)(rep >> 2) * 9 + 3 * (rep & 3);
+            bool ok = true;
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax) {
+                const T a0 = __ldg(p0 + ax), a1 = __ldg(p1 + ax);
+                const T d = a1 - a0;
+                ok = ok && (a0 + d) == a1;     // MovingTriangle::ComputeBBoxVertex's v + dv
+                ok = ok && weld_bits(a0) == weld_bits(__ldg(r0 + ax)) && weld_bits(a1) == weld_bits(__ldg(r1 + ax));
+            }
+            atomicAdd(cnt + rep, 1);
+            if (!ok) atomicOr(cnt + rep, CLS_NODEDUP);
+        }
+    }
+}
+
+static constexpr int WELD_THREADS = 256;
+
+static __global__ void __launch_bounds__(WELD_THREADS)
+k_weld_alloc(Forest F, const int* __restrict__ vidc, const int* __restrict__ cnt, int* __restrict__ fan_start,
+             int* __restrict__ fan_end, WsHeader* hdr) {
+    __shared__ int wsum[WELD_THREADS / 32];
+    __shared__ int base_s;
+    const int M = forest_size(F);
+    const int total = __ldg(F.voff + M);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int b0 = blockIdx.x * WELD_THREADS; b0 < total; b0 += gridDim.x * WELD_THREADS) {
+        const int v = b0 + threadIdx.x;
+        int sz[3] = {0, 0, 0};
+        long long slot = 0;
+        if (v < total) {
+            slot = weld_item(F, M, v).slot;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const int id = (int)(4 * slot + c);
+                if (__ldg(vidc + id) == id) sz[c] = __ldg(cnt + id) & CLS_MASK;
+            }
+        }
+        const int mine = sz[0] + sz[1] + sz[2];
+        const int incl = warp_inclusive_scan(mine, lane);
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            const int x = lane < WELD_THREADS / 32 ? wsum[lane] : 0;
+            const int sc = warp_inclusive_scan(x, lane);
+            if (lane < WELD_THREADS / 32) wsum[lane] = sc - x;
+            if (lane == 31) base_s = sc ? atomicAdd(&hdr->fan_cursor, sc) : 0;
+        }
+        __syncthreads();
+        int at = base_s + wsum[warp] + incl - mine;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            if (sz[c]) {
+                fan_start[4 * slot + c] = at;
+                fan_end[4 * slot + c] = at;       // k_weld_fill moves it to the end
+                at += sz[c];
+            }
+        __syncthreads();
+    }
+}
+
+static __global__ void k_weld_fill(Forest F, const int* __restrict__ vidc, const int* __restrict__ fan_start,
+                                   int* fan_end, int4* __restrict__ fan) {
+    const int M = forest_size(F);
+    const int total = __ldg(F.voff + M);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
+        const long long slot = weld_item(F, M, v).slot;
+        const int r0 = __ldg(vidc + 4 * slot), r1 = __ldg(vidc + 4 * slot + 1), r2 = __ldg(vidc + 4 * slot + 2);
+        const int4 en = make_int4(0, __ldg(fan_start + r0), __ldg(fan_start + r1), __ldg(fan_start + r2));
+        for (int c = 0; c < 3; ++c) {
+            const int pos = atomicAdd(fan_end + (c == 0 ? r0 : (c == 1 ? r1 : r2)), 1);
+            fan[pos] = make_int4((int)(4 * slot + c), en.y, en.z, en.w);
+        }
+    }
+}
+
+// each class's members in ascending corner id (classes of at most WELD_FANCAP corners; the
+// larger ones are not shared)
+static __global__ void k_weld_sort(Forest F, const int* __restrict__ vidc, const int* __restrict__ cnt,
+                                   const int* __restrict__ fan_end, int4* fan) {
+    const int M = forest_size(F);
+    const int total = __ldg(F.voff + M);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
+        const long long slot = weld_item(F, M, v).slot;
+        for (int c = 0; c < 3; ++c) {
+            const int id = (int)(4 * slot + c);
+            if (__ldg(vidc + id) != id) continue;
+            const int n = __ldg(cnt + id) & CLS_MASK;
+            if (n < 2 || n > WELD_FANCAP) continue;
+            int4* f = fan + (__ldg(fan_end + id) - n);
+            for (int i = 1; i < n; ++i) {
+                const int4 x = f[i];
+                int j = i - 1;
+                while (j >= 0 && f[j].x > x.x) {
+                    f[j + 1] = f[j];
+                    --j;
+                }
+                f[j + 1] = x;
+            }
+        }
+    }
+}
+
+static __global__ void k_weld_tri(Forest F, const int* __restrict__ vidc, const int* __restrict__ cnt,
+                                  const int* __restrict__ fan_start, const int4* __restrict__ fan,
+                                  int4* __restrict__ vid, int4* __restrict__ twin, int4* __restrict__ third) {
+    const int M = forest_size(F);
+    const int total = __ldg(F.voff + M);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
+        const long long slot = weld_item(F, M, v).slot;
+        int st[3], n[3], fl[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int r = __ldg(vidc + 4 * slot + c);
+            const int cv = __ldg(cnt + r);
+            st[c] = __ldg(fan_start + r);
+            n[c] = cv & CLS_MASK;
+            fl[c] = ((cv & CLS_NODEDUP) || n[c] > WELD_FANCAP) ? CLS_NODEDUP : 0;
+        }
+        int tw[3], th[3];
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+            const int a0 = e > 1, a1 = e > 0 ? 2 : 1;
+            tw[e] = TWIN_NONE;
+            th[e] = 0;
+            if (fl[a0] | fl[a1]) continue;      // no sub-test over this edge is shared
+            const int u1 = st[a1];
+            int found = 0;
+            for (int i = st[a0]; i < st[a0] + n[a0]; ++i) {
+                const int4 en = __ldg(fan + i);
+                const int t = en.x >> 2, ca = en.x & 3;
+                for (int cb = ca + 1; cb < 3; ++cb) {
+                    if ((long long)t == slot && ca == a0 && cb == a1) continue;    // the edge itself
+                    if ((cb == 1 ? en.z : en.w) == u1) {
+                        ++found;
+                        tw[e] = 4 * t + (ca + cb - 1);
+                        const int oc = 3 - ca - cb;            // the twin's third corner
+                        th[e] = oc == 0 ? en.y : (oc == 1 ? en.z : en.w);
+                    }
+                }
+            }
+            if (found > 1) tw[e] = TWIN_MANY;
+        }
+        int w = min(n[0], 31) | (min(n[1], 31) << 5) | (min(n[2], 31) << 10);
+#pragma unroll
+        for (int e = 0; e < 3; ++e) w |= (tw[e] == TWIN_NONE ? 0 : (tw[e] == TWIN_MANY ? 2 : 1)) << (15 + 2 * e);
+        vid[slot] = make_int4(st[0] | fl[0], st[1] | fl[1], st[2] | fl[2], w);
+        twin[slot] = make_int4(tw[0], tw[1], tw[2], 0);
+        third[slot] = make_int4(th[0], th[1], th[2], 0);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // Refit: swept leaf boxes rounded outward to fp32 into their slots, then bottom-up the box of
 // every even-depth node into its own slot.
 

@@ -37,10 +37,13 @@ enum MeshFlags {
 struct WsHeader {
     int status;
     int cand_count;
-    int subtests;      // continuous sub-tests (pair, type) solved
+    int subtests;      // continuous sub-tests (pair, type) whose swept sub-boxes overlap
     int roots;         // roots in [0, 1] filtered
     int front;         // engine refit: climbs handed from the block pass to the global pass
-    int pad[11];
+    int solved;        // sub-tests solved (fewer than subtests when repeated ones are shared)
+    int fan_cursor;    // engine corner classes: member list slots handed out
+    int live_count;    // engine staging: pairs with sub-tests to solve (Weld.live)
+    int pad[8];
 };
 
 struct __align__(16) TNode {
@@ -641,8 +644,179 @@ template <class T> struct CcdLayout {
 // (the live-pair counter of a chunk also comes in two, used by alternate chunks)
 enum CcdInts { CI_WARP = 0, CI_TOTAL = 32, CI_COUNT = 33, CI_ROOTS = 41, CI_LIVE = 45 };
 
-// a queued sub-test: triangle slots i and j, type k in the top bits of j (slots < 2^28)
-__device__ __forceinline__ int2 pack_subtest(int i, int j, int k) { return make_int2(i, j | (k << 28)); }
+// a queued sub-test: triangle slots i and j, type k in the top bits of j (slots < 2^28),
+// bit 28 of i set when the sub-test stands for all its repeats (see Weld)
+constexpr int SLOT_MASK = 0x0fffffff;
+__device__ __forceinline__ int2 pack_subtest(int i, int j, int k, int shared = 0) {
+    return make_int2(i | (shared << 28), j | (k << 28));
+}
+
+// Repeated sub-tests (resident engine only).  On a mesh a vertex-face sub-test (v, face B)
+// is the sub-test of every pair (A', B) whose triangle A' has a corner at v, and an
+// edge-edge sub-test belongs to every pair of triangles carrying the two edges with their
+// corners in the same order: the tetrahedra are bit for bit the same, and so are their
+// roots, filter decisions and contacts.  The pairs that produce one of them are known from
+// the corner classes alone:
+//  * the corners of a mesh whose start positions are equal (==, the reference's
+//    shared-vertex relation, figures.cu:527-544) form a class; a pair shares a vertex
+//    exactly when its triangles have a class in common;
+//  * every such pair is live (shares no vertex), is a candidate pair of the reference (a
+//    vertex's swept sub-box lies in its triangle's leaf box, the merge of the triangle's
+//    boxes at both ends of the step, when x0 + (x1 - x0) == x1 for its coordinates), and
+//    has the sub-test's sub-box bit (the boxes of the same points);
+//  * for vertex-face types 12..14 (vertex of the first triangle) they are the pairs
+//    (A', B) with A' < B over the class's corners, for 9..11 the pairs (A, B') with
+//    B' > A; for edge-edge types the pairs over each edge and its twin, the other
+//    triangle edge whose corners are the same classes in the same order.
+// The smallest of those (slot, slot, type) triples solves the sub-test and emits the rows
+// or contacts of all of them; the others drop it.  A class is excluded (CLS_NODEDUP) when
+// its corners are not bit-identical at both ends of the step, when x0 + (x1 - x0) != x1 for
+// one of its coordinates, or when it has more than WELD_FANCAP corners; an edge with more
+// than one twin is excluded too.  A sub-test touching an excluded class or edge is solved
+// by each of its pairs, as without the classes.  Every pair finds the same members, so
+// each repeat is solved exactly once.  Pairs with a rigid motion have no sub-test with a
+// root (ccd_pair_subbox_mask), so it does not matter which of them is the smallest.
+constexpr int CLS_MASK = (1 << 30) - 1;
+constexpr int CLS_NODEDUP = 1 << 30;
+constexpr int TWIN_NONE = -1, TWIN_MANY = -2;
+constexpr int WELD_FANCAP = 16;
+struct Weld {
+    const int4* vid;       // per triangle slot: the class of each corner (its first entry in
+                           // fan) | CLS_NODEDUP; in w the three class sizes (bits 5c..5c+4,
+                           // sizes above 31 as 31) and whether each edge e has no twin, one
+                           // or more (bits 15+2e..16+2e: 0, 1, 2); null: no classes
+    const int4* fan;       // the classes' members, class by class in ascending corner id:
+                           // (corner id 4 * slot + corner, the classes of its triangle)
+    const int4* twin;      // per triangle slot and edge {01, 02, 12}: 4 * slot + edge of its
+                           // twin, TWIN_NONE or TWIN_MANY
+    const int4* third;     // per triangle slot and edge: the class of the twin's third corner
+    const int4* live;      // the pairs with sub-tests to solve (hdr->live_count of them, from
+                           // k_ccd_stage_*): slots i, j and the sub-tests it solves (bits
+                           // 0..14) with those that stand for their repeats (bits 15..29)
+};
+
+__device__ __forceinline__ int int4_at(int4 v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); }
+__device__ __forceinline__ bool classes_meet(int4 a, int4 b) {
+    const int a0 = a.x & CLS_MASK, a1 = a.y & CLS_MASK, a2 = a.z & CLS_MASK;
+    const int b0 = b.x & CLS_MASK, b1 = b.y & CLS_MASK, b2 = b.z & CLS_MASK;
+    return a0 == b0 || a0 == b1 || a0 == b2 || a1 == b0 || a1 == b1 || a1 == b2 || a2 == b0 || a2 == b1 ||
+           a2 == b2;
+}
+__device__ __forceinline__ int class_size(int4 v, int c) { return (v.w >> (5 * c)) & 31; }
+__device__ __forceinline__ int twin_kind(int4 v, int e) { return (v.w >> (15 + 2 * e)) & 3; }
+
+// Calls fn(a, b, type) for every pair that has sub-test k of pair (A, B) (A < B, live), the
+// pair itself included, and returns true; returns false without a call when the sub-test
+// is solved by each of its pairs.  VA, VB: W.vid[A], W.vid[B].
+template <class Fn>
+__device__ __forceinline__ bool weld_members(const Weld& W, int A, int B, int k, int4 VA, int4 VB, Fn&& fn) {
+    if (k >= 9) {
+        const bool vf = k >= 12;                 // vertex of A, face of B (else face of A)
+        const int4 Vface = vf ? VB : VA;
+        const int4 Vvert = vf ? VA : VB;
+        const int c = vf ? k - 12 : k - 9;
+        const int v = int4_at(Vvert, c);
+        // (a class of one corner: the pair is the sub-test's only one)
+        if (((v | Vface.x | Vface.y | Vface.z) & CLS_NODEDUP) || class_size(Vvert, c) < 2) return false;
+        const int end = v + class_size(Vvert, c);
+        for (int i = v; i < end; ++i) {
+            const int4 en = __ldg(W.fan + i);
+            const int t = en.x >> 2, cc = en.x & 3;
+            if (vf ? t >= B : t <= A) continue;
+            if (classes_meet(make_int4(en.y, en.z, en.w, 0), Vface)) continue;
+            if (vf) fn(t, B, 12 + cc);
+            else fn(A, t, 9 + cc);
+        }
+        return true;
+    }
+    const int e = k / 3, f = k - 3 * e;
+    // (edges without a twin: the pair is the sub-test's only one)
+    const int ka = twin_kind(VA, e), kb = twin_kind(VB, f);
+    if (ka == 2 || kb == 2 || (ka | kb) == 0) return false;
+    // edge {01, 02, 12}[e]: corners e > 1 ? 1 : 0 and e > 0 ? 2 : 1
+    const int ua = int4_at(VA, e > 1), ub = int4_at(VA, e > 0 ? 2 : 1);
+    const int wa = int4_at(VB, f > 1), wb = int4_at(VB, f > 0 ? 2 : 1);
+    if ((ua | ub | wa | wb) & CLS_NODEDUP) return false;
+    const int ta = ka ? int4_at(__ldg(W.twin + A), e) : TWIN_NONE;
+    const int tb = kb ? int4_at(__ldg(W.twin + B), f) : TWIN_NONE;
+    // the twins' classes: the edge's two and their third corner's
+    const int4 TA = make_int4(ua, ub, ta >= 0 ? int4_at(__ldg(W.third + A), e) : 0, 0);
+    const int4 TB = make_int4(wa, wb, tb >= 0 ? int4_at(__ldg(W.third + B), f) : 0, 0);
+    for (int i = 0; i < 2; ++i) {
+        if (i == 1 && ta < 0) break;
+        const int a = i ? ta >> 2 : A, sa = i ? ta & 3 : e;
+        for (int j = 0; j < 2; ++j) {
+            if (j == 1 && tb < 0) break;
+            const int b = j ? tb >> 2 : B, sb = j ? tb & 3 : f;
+            if (a >= b) continue;
+            if ((i | j) && classes_meet(i ? TA : VA, j ? TB : VB)) continue;
+            fn(a, b, 3 * sa + sb);
+        }
+    }
+    return true;
+}
+
+// Whether pair (A, B) solves its sub-test k: true when the sub-test is not shared or when
+// (A, B, k) is the smallest of its pairs; *shared tells which.  The members of a class are
+// in ascending corner id, so a vertex-face scan stops at the first pair that has the
+// sub-test.
+__device__ __forceinline__ bool weld_solves(const Weld& W, int A, int B, int k, int4 VA, int4 VB, bool* shared) {
+    *shared = false;
+    if (k >= 9) {
+        const bool vf = k >= 12;
+        const int4 Vface = vf ? VB : VA;
+        const int4 Vvert = vf ? VA : VB;
+        const int c = vf ? k - 12 : k - 9;
+        const int v = int4_at(Vvert, c);
+        if (((v | Vface.x | Vface.y | Vface.z) & CLS_NODEDUP) || class_size(Vvert, c) < 2) return true;
+        *shared = true;
+        const int end = v + class_size(Vvert, c);
+        for (int i = v; i < end; ++i) {
+            const int4 en = __ldg(W.fan + i);
+            const int t = en.x >> 2, cc = en.x & 3;
+            if (vf ? t >= B : t <= A) {
+                if (vf) break;             // the remaining corners are on later triangles
+                continue;
+            }
+            if (classes_meet(make_int4(en.y, en.z, en.w, 0), Vface)) continue;
+            return vf ? (t == A && cc == c) : (t == B && cc == c);
+        }
+        return true;    // (not reached: the pair itself has the sub-test)
+    }
+    int ma = A, mb = B, mk = k;
+    const bool sh = weld_members(W, A, B, k, VA, VB, [&](int a, int b, int kk) {
+        if (a < ma || (a == ma && (b < mb || (b == mb && kk < mk)))) {
+            ma = a;
+            mb = b;
+            mk = kk;
+        }
+    });
+    *shared = sh;
+    return !sh || (ma == A && mb == B && mk == k);
+}
+
+// The pairs of sub-test k of pair (A, B) in (ma, mb, mk), at most WELD_FANCAP of them (a
+// shared vertex-face sub-test has one per corner of its class, an edge-edge one at most
+// four); the pair alone when the sub-test is not shared.  Returns their number.
+__device__ __forceinline__ int weld_list(const Weld& W, int A, int B, int k, bool shared, int* ma, int* mb, int* mk) {
+    int n = 0;
+    if (shared)
+        weld_members(W, A, B, k, __ldg(W.vid + A), __ldg(W.vid + B), [&](int a, int b, int kk) {
+            if (n < WELD_FANCAP) {
+                ma[n] = a;
+                mb[n] = b;
+                mk[n] = kk;
+                ++n;
+            }
+        });
+    if (n == 0) {
+        ma[0] = A;
+        mb[0] = B;
+        mk[0] = k;
+        n = 1;
+    }
+    return n;
+}
 
 __device__ __forceinline__ int warp_inclusive_scan(int v, int lane) {
 #pragma unroll
@@ -651,6 +825,95 @@ __device__ __forceinline__ int warp_inclusive_scan(int v, int lane) {
         if (lane >= o) v += y;
     }
     return v;
+}
+
+// Staging of the resident engine's candidate pairs for k_ccd_narrow (Weld.live), in two
+// kernels so that each runs at the occupancy its work needs:
+//  * k_ccd_stage_mask: per pair, 0 when the triangles share a vertex (a corner class in
+//    common, the same relation as the reference's coordinate test), else the sub-box mask
+//    with the exact leaf-box test (the engine's candidates come from fp32 boxes rounded
+//    outward); hdr->subtests counts the sub-tests of the masks;
+//  * k_ccd_stage_solvers: the mask cut to the sub-tests the pair solves (weld_solves), with
+//    the shared ones marked in bits 15..29, appended to the list of pairs with work; each
+//    warp spreads its 32 pairs' sub-tests over its lanes, and few registers keep enough
+//    warps resident for the latency-bound scans of the corner classes.
+static constexpr int STAGE_THREADS = 256;
+template <class T>
+__global__ void __launch_bounds__(STAGE_THREADS, 2)
+k_ccd_stage_mask(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ x0,
+                 const T* __restrict__ x1, Weld W, unsigned* __restrict__ stage) {
+    const int n = min(*(volatile int*)&hdr->cand_count, cand_cap);
+    int masked = 0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const int2 pr = cand[c];
+        unsigned bits = 0;
+        if (!classes_meet(__ldg(W.vid + pr.x), __ldg(W.vid + pr.y))) {
+            bits = ccd_pair_subbox_mask<T, true>(x0, x1, pr.x, pr.y, true);
+            masked += __popc(bits);
+        }
+        stage[c] = bits;
+    }
+    masked = __reduce_add_sync(0xffffffffu, masked);
+    if ((threadIdx.x & 31) == 0 && masked) atomicAdd(&hdr->subtests, masked);
+}
+
+static __global__ void __launch_bounds__(STAGE_THREADS)
+k_ccd_stage_solvers(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, Weld W,
+                    const unsigned* __restrict__ stage, int4* __restrict__ live) {
+    // per warp: 32 pairs, their slots, classes, masks, the prefix of their sub-test counts
+    // and the sub-tests they solve; the warp's lanes take the pairs' sub-tests 32 at a time
+    __shared__ int2 s_pr[STAGE_THREADS];
+    __shared__ int4 s_va[STAGE_THREADS], s_vb[STAGE_THREADS];
+    __shared__ unsigned s_bits[STAGE_THREADS], s_word[STAGE_THREADS];
+    __shared__ int s_pre[STAGE_THREADS];
+    const int n = min(*(volatile int*)&hdr->cand_count, cand_cap);
+    const int tid = threadIdx.x, lane = tid & 31, w0 = tid & ~31;
+    const unsigned FULL = 0xffffffffu;
+    const int warps = gridDim.x * (STAGE_THREADS / 32);
+    for (int base = (blockIdx.x * (STAGE_THREADS / 32) + (tid >> 5)) * 32; base < n; base += warps * 32) {
+        const int c = base + lane;
+        const unsigned bits = c < n ? stage[c] : 0u;
+        int2 pr = make_int2(0, 0);
+        if (bits) {
+            pr = cand[c];
+            s_va[tid] = __ldg(W.vid + pr.x);
+            s_vb[tid] = __ldg(W.vid + pr.y);
+        }
+        s_pr[tid] = pr;
+        s_word[tid] = 0u;
+        // edge-edge sub-tests first, vertex-face ones after, so that a round of 32 runs one
+        // of the two scans
+#pragma unroll 1
+        for (int kind = 0; kind < 2; ++kind) {
+            const unsigned kb = bits & (kind ? 0x7e00u : 0x01ffu);
+            s_bits[tid] = kb;
+            const int incl = warp_inclusive_scan(__popc(kb), lane);
+            s_pre[tid] = incl;
+            const int total = __shfl_sync(FULL, incl, 31);
+            __syncwarp();
+            for (int r = lane; r < total; r += 32) {
+                int lo = 0, hi = 31;                       // the pair: first prefix above r
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (s_pre[w0 + mid] > r) hi = mid;
+                    else lo = mid + 1;
+                }
+                const int p = w0 + lo;
+                const int k = __fns(s_bits[p], 0, r - (lo ? s_pre[p - 1] : 0) + 1);
+                bool sh = false;
+                if (weld_solves(W, s_pr[p].x, s_pr[p].y, k, s_va[p], s_vb[p], &sh))
+                    atomicOr(&s_word[p], (1u << k) | (sh ? 1u << (15 + k) : 0u));
+            }
+            __syncwarp();
+        }
+        const unsigned word = s_word[tid];
+        const unsigned has = __ballot_sync(FULL, word != 0u);
+        int at = 0;
+        if (lane == 0 && has) at = atomicAdd(&hdr->live_count, __popc(has));
+        at = __shfl_sync(FULL, at, 0) + __popc(has & ((1u << lane) - 1u));
+        if (word) live[at] = make_int4(pr.x, pr.y, (int)word, 0);     // (at most one per candidate)
+        __syncwarp();
+    }
 }
 
 // The continuous narrow phase is compiled in one translation unit only, ccc_narrow.cu, with
@@ -662,7 +925,7 @@ __device__ __forceinline__ int warp_inclusive_scan(int v, int lane) {
 template <class T, int MODE, class Sink, int LIB>
 cudaError_t launch_ccd_narrow(int grid, cudaStream_t s, const int2* cand, int cand_cap, WsHeader* hdr, const T* x0,
                               const T* x1, Forest F, long long* rows, T* times, int max_per_tri, int* mesh_counters,
-                              Sink sink);
+                              Weld W, Sink sink);
 template <class T, int MODE, class Sink, int LIB> cudaError_t prepare_ccd_narrow();
 
 #ifdef CCC_NARROW_TU
@@ -670,7 +933,7 @@ template <class T, int MODE, class Sink, int LIB>
 __global__ void __launch_bounds__(CCD_BLOCK, CCD_MIN_BLOCKS)
 k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ x0,
              const T* __restrict__ x1, Forest F, long long* __restrict__ rows, T* __restrict__ times, int max_per_tri,
-             int* __restrict__ mesh_counters, Sink sink) {
+             int* __restrict__ mesh_counters, Weld W, Sink sink) {
     extern __shared__ __align__(16) unsigned char smem[];
     using L = CcdLayout<T>;
     double* rec = reinterpret_cast<double*>(smem + L::rec);
@@ -690,8 +953,9 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned FULL = 0xffffffffu;
     const unsigned lt = (1u << lane) - 1u;
-    const int n = min(*(volatile int*)&hdr->cand_count, cand_cap);
+    const int n = min(*(volatile int*)(W.live ? &hdr->live_count : &hdr->cand_count), cand_cap);
     int head = 0, queued = 0;           // ring queue of sub-tests (block-uniform)
+    int masked = 0;                     // this thread's sub-tests before repeats are shared
     // class counts and root count of a batch, two sets used by alternate batches: a batch
     // clears the other set at its end, when every read of that set is two barriers back
     // (the staging barriers order the initial clearing before the first batch)
@@ -704,48 +968,62 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
         const bool more = base < n;
         if (!more && queued == 0) break;
         if (more) {
-            // about half of the candidate pairs are mesh neighbours that share a vertex: the
-            // chunk's other pairs are gathered first (block-wide), so that the 15 swept
-            // sub-box tests run on full warps
-            long long c = base + tid;
             int2 pr = make_int2(0, 0);
-            bool live = false;
-            if (c < n) {
-                pr = cand[c];
-                live = !ccd_pair_shares_vertex<T>(x0, pr.x, pr.y);
-            }
-            const unsigned lb = __ballot_sync(FULL, live);
-            int lbase = 0;
-            if (lane == 0 && lb) lbase = atomicAdd(&ints[CI_LIVE + cpar], __popc(lb));
-            lbase = __shfl_sync(FULL, lbase, 0);
-            if (live) spairs[lbase + __popc(lb & lt)] = pr;
-            __syncthreads();
-            const int nlive = ints[CI_LIVE + cpar];
-            // the other chunk parity's counter was last read before the barrier above
-            if (tid == 0) ints[CI_LIVE + (cpar ^ 1)] = 0;
-            cpar ^= 1;
             uint32_t bits = 0;
-            pr = make_int2(0, 0);
-            if (tid < nlive) {
-                pr = spairs[tid];
-                bits = ccd_pair_subbox_mask<T, MODE != CCD_MINCOL>(x0, x1, pr.x, pr.y);
-            }
-            if (MODE == CCD_MINCOL) {
-                while (bits) {
-                    int k = __ffs(bits) - 1;
-                    bits &= bits - 1;
-                    OutRegion R = out_region(F, M, pr.x, max_per_tri);
-                    long long r = append_row(mesh_counters, F, R.m, R.cap, &hdr->status);
-                    if (r >= 0) {
-                        long long o = (long long)R.po * max_per_tri + r;
-                        rows[o * 3 + 0] = pr.x - R.po;
-                        rows[o * 3 + 1] = pr.y - R.po;
-                        rows[o * 3 + 2] = k;
-                    }
+            unsigned shared_bits = 0;
+            if (W.live) {
+                // the resident engine's pairs come staged by k_ccd_stage_*: the pairs with
+                // sub-tests to solve, which ones, and which of them stand for their repeats
+                const long long c = base + tid;
+                if (c < n) {
+                    const int4 rec = W.live[c];
+                    pr = make_int2(rec.x, rec.y);
+                    bits = (unsigned)rec.z & 0x7fffu;
+                    shared_bits = ((unsigned)rec.z >> 15) & 0x7fffu;
                 }
-                // the next chunk reuses spairs and the other live counter
+            } else {
+                // about half of the candidate pairs are mesh neighbours that share a vertex:
+                // the chunk's other pairs are gathered first (block-wide), so that the 15
+                // swept sub-box tests run on full warps
+                long long c = base + tid;
+                bool live = false;
+                if (c < n) {
+                    pr = cand[c];
+                    live = !ccd_pair_shares_vertex<T>(x0, pr.x, pr.y);
+                }
+                const unsigned lb = __ballot_sync(FULL, live);
+                int lbase = 0;
+                if (lane == 0 && lb) lbase = atomicAdd(&ints[CI_LIVE + cpar], __popc(lb));
+                lbase = __shfl_sync(FULL, lbase, 0);
+                if (live) spairs[lbase + __popc(lb & lt)] = pr;
                 __syncthreads();
-                continue;
+                const int nlive = ints[CI_LIVE + cpar];
+                // the other chunk parity's counter was last read before the barrier above
+                if (tid == 0) ints[CI_LIVE + (cpar ^ 1)] = 0;
+                cpar ^= 1;
+                pr = make_int2(0, 0);
+                if (tid < nlive) {
+                    pr = spairs[tid];
+                    bits = ccd_pair_subbox_mask<T, MODE != CCD_MINCOL>(x0, x1, pr.x, pr.y);
+                }
+                if (MODE != CCD_MINCOL) masked += __popc(bits);
+                if (MODE == CCD_MINCOL) {
+                    while (bits) {
+                        int k = __ffs(bits) - 1;
+                        bits &= bits - 1;
+                        OutRegion R = out_region(F, M, pr.x, max_per_tri);
+                        long long r = append_row(mesh_counters, F, R.m, R.cap, &hdr->status);
+                        if (r >= 0) {
+                            long long o = (long long)R.po * max_per_tri + r;
+                            rows[o * 3 + 0] = pr.x - R.po;
+                            rows[o * 3 + 1] = pr.y - R.po;
+                            rows[o * 3 + 2] = k;
+                        }
+                    }
+                    // the next chunk reuses spairs and the other live counter
+                    __syncthreads();
+                    continue;
+                }
             }
             // append the chunk's sub-tests (block-wide exclusive scan of the counts)
             const int cnt = __popc(bits);
@@ -764,10 +1042,10 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
             while (bits) {
                 int k = __ffs(bits) - 1;
                 bits &= bits - 1;
-                items[pos % Q] = pack_subtest(pr.x, pr.y, k);
+                items[pos % Q] = pack_subtest(pr.x, pr.y, k, (shared_bits >> k) & 1u);
                 ++pos;
             }
-            if (tid == 0 && total) atomicAdd(&hdr->subtests, total);
+            if (tid == 0 && total) atomicAdd(&hdr->solved, total);
             queued += total;
             __syncthreads();
         }
@@ -778,7 +1056,7 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
             for (int ri = tid; ri < nb; ri += CCD_BLOCK) {
                 int2 it = items[(head + ri) % Q];
                 int k = (it.y >> 28) & 15;
-                MTet<T> tet = load_tet(x0, x1, it.x, it.y & 0x0fffffff, k);
+                MTet<T> tet = load_tet(x0, x1, it.x & SLOT_MASK, it.y & SLOT_MASK, k);
                 T cf[4];
                 cubic_coeffs(tet, cf);
                 rec[0 * NB + ri] = (double)cf[0];
@@ -851,15 +1129,21 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                 int np = 0;                        // buffered roots of this warp (warp-uniform)
                 auto emit = [&](int j) {
                     const int2 it = items[(head + root_rec[j]) % Q];
-                    const int qx = it.x, qy = it.y & 0x0fffffff, k = (it.y >> 28) & 15;
-                    OutRegion R = out_region(F, M, qx, max_per_tri);
-                    long long r = append_row(mesh_counters, F, R.m, R.cap, &hdr->status);
-                    if (r >= 0) {
-                        long long o = (long long)R.po * max_per_tri + r;
-                        rows[o * 3 + 0] = qx - R.po;
-                        rows[o * 3 + 1] = qy - R.po;
-                        rows[o * 3 + 2] = k;
-                        times[o] = root_val[j];
+                    const int qx = it.x & SLOT_MASK, qy = it.y & SLOT_MASK, k = (it.y >> 28) & 15;
+                    const T tv = root_val[j];
+                    // every pair of a shared sub-test is in the mesh of (qx, qy)
+                    const OutRegion R = out_region(F, M, qx, max_per_tri);
+                    int ma[WELD_FANCAP], mb[WELD_FANCAP], mk[WELD_FANCAP];
+                    const int nm = weld_list(W, qx, qy, k, (it.x >> 28) & 1, ma, mb, mk);
+                    for (int i = 0; i < nm; ++i) {
+                        long long r = append_row(mesh_counters, F, R.m, R.cap, &hdr->status);
+                        if (r >= 0) {
+                            long long o = (long long)R.po * max_per_tri + r;
+                            rows[o * 3 + 0] = ma[i] - R.po;
+                            rows[o * 3 + 1] = mb[i] - R.po;
+                            rows[o * 3 + 2] = mk[i];
+                            times[o] = tv;
+                        }
                     }
                 };
                 for (int b0 = warp * 32; b0 < nroots; b0 += CCD_BLOCK) {
@@ -870,7 +1154,7 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                         j = jj < nee ? jj : 3 * NB - 1 - (jj - nee);
                         const int2 it = items[(head + root_rec[j]) % Q];
                         const int k = (it.y >> 28) & 15;
-                        MTet<T> tet = load_tet(x0, x1, it.x, it.y & 0x0fffffff, k);
+                        MTet<T> tet = load_tet(x0, x1, it.x & SLOT_MASK, it.y & SLOT_MASK, k);
                         pass = ccd_filter(tet, k, root_val[j]);
                     }
                     const unsigned pm = __ballot_sync(FULL, pass);
@@ -892,16 +1176,22 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                     const int j = jj < nee ? jj : 3 * NB - 1 - (jj - nee);
                     int2 it = items[(head + root_rec[j]) % Q];
                     int k = (it.y >> 28) & 15;
-                    int2 q = make_int2(it.x, it.y & 0x0fffffff);
+                    int2 q = make_int2(it.x & SLOT_MASK, it.y & SLOT_MASK);
                     T root = root_val[j];
                     MTet<T> tet = load_tet(x0, x1, q.x, q.y, k);
                     if (!ccd_filter(tet, k, root)) continue;
-                    T mq[4];
+                    // the contact of every pair with this sub-test (its own corner masses)
+                    int ma[WELD_FANCAP], mb[WELD_FANCAP], mk[WELD_FANCAP];
+                    const int nm = weld_list(W, q.x, q.y, k, (it.x >> 28) & 1, ma, mb, mk);
+                    for (int i = 0; i < nm; ++i) {
+                        const int a = ma[i], b = mb[i], kk = mk[i];
+                        T mq[4];
 #pragma unroll
-                    for (int pt = 0; pt < 4; ++pt)
-                        mq[pt] = sink.masses[(long long)(tet_side(k, pt) ? q.y : q.x) * 3 + tet_corner(k, pt)];
-                    Contact<T> ct = contact<T, LIB>(tet, k, root, mq);
-                    sink.add(tet, q.x, q.y, k, root, ct, F, M, &hdr->status);
+                        for (int pt = 0; pt < 4; ++pt)
+                            mq[pt] = sink.masses[(long long)(tet_side(kk, pt) ? b : a) * 3 + tet_corner(kk, pt)];
+                        Contact<T> ct = contact<T, LIB>(tet, kk, root, mq);
+                        sink.add(tet, a, b, kk, root, ct, F, M, &hdr->status);
+                    }
                 }
             }
             if (tid < 4) ints[CI_COUNT + 4 * (par ^ 1) + tid] = 0;
@@ -911,6 +1201,11 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
             queued -= nb;
             __syncthreads();
         }
+    }
+    // (the loop ends for the whole block at once)
+    if (MODE != CCD_MINCOL) {
+        const int ws = __reduce_add_sync(FULL, masked);
+        if (lane == 0 && ws) atomicAdd(&hdr->subtests, ws);
     }
 }
 
@@ -932,11 +1227,11 @@ template <class T, int MODE, class Sink, int LIB> cudaError_t prepare_ccd_narrow
 template <class T, int MODE, class Sink, int LIB>
 cudaError_t launch_ccd_narrow(int grid, cudaStream_t s, const int2* cand, int cand_cap, WsHeader* hdr, const T* x0,
                               const T* x1, Forest F, long long* rows, T* times, int max_per_tri, int* mesh_counters,
-                              Sink sink) {
+                              Weld W, Sink sink) {
     cudaError_t e = prepare_ccd_narrow<T, MODE, Sink, LIB>();
     if (e != cudaSuccess) return e;
     k_ccd_narrow<T, MODE, Sink, LIB><<<grid, CCD_BLOCK, CcdLayout<T>::bytes, s>>>(
-        cand, cand_cap, hdr, x0, x1, F, rows, times, max_per_tri, mesh_counters, sink);
+        cand, cand_cap, hdr, x0, x1, F, rows, times, max_per_tri, mesh_counters, W, sink);
     return cudaSuccess;
 }
 

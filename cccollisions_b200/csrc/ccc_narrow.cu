@@ -22,7 +22,7 @@ namespace ccc {
 #define CCC_NARROW_INSTANCE(T, MODE, SINK, LIB)                                                                     \
     template cudaError_t launch_ccd_narrow<T, MODE, SINK, LIB>(int, cudaStream_t, const int2*, int, WsHeader*,     \
                                                                const T*, const T*, Forest, long long*, T*, int,     \
-                                                               int*, SINK);                                         \
+                                                               int*, Weld, SINK);                                   \
     template cudaError_t prepare_ccd_narrow<T, MODE, SINK, LIB>();
 #define CCC_NARROW_TYPES(MODE, SINK, LIB)                                                                          \
     CCC_NARROW_INSTANCE(float, MODE, SINK<float>, LIB)                                                              \

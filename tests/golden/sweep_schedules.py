@@ -4,8 +4,9 @@ each schedule's rows against the reference's digests in ``full_batched.npz``.
     python tests/golden/sweep_schedules.py [--meshes 64] [--only 4,10] [--steps 5]
 
 One JSON line per schedule: the schedule's fields (traversal and narrow blocks an SM, warp
-traversal), the meshes whose rows differ from the reference's (``bad``, empty when equal)
-and the mean device time of each kernel over ``--steps`` steps.  Needs a CUDA device.
+traversal), the meshes whose rows differ from the reference's (``bad``, empty when equal),
+the work counters of the last step and the mean device time of each kernel over
+``--steps`` steps.  Needs a CUDA device.
 """
 import argparse
 import json
@@ -66,7 +67,7 @@ def main():
                 eng.ccd()
             kern = N.timing_end()
             stream.synchronize()
-            print(json.dumps({"schedule": i, **sched, "bad": bad,
+            print(json.dumps({"schedule": i, **sched, "bad": bad, "counters": eng.counters(),
                               "ms": {k: round(v[0] / v[1], 4) for k, v in kern.items()}}), flush=True)
     eng.close()
     sys.exit(1 if failed else 0)
