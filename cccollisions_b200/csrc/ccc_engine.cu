@@ -54,7 +54,7 @@ struct EngineLayout {
     int64_t rows, times, cand;
     int64_t keys0, keys1, vals0, vals1, hist;
     int64_t verts0, verts1, vel, acc;
-    int64_t wtab, vidc, wcnt, fan_end, fan, vid4, twin4, third4, stage, live, end;
+    int64_t wtab, vidc, wcnt, fan_end, fan, vid4, twin4, third4, pending, live, end;
     int64_t zero_bytes, hist_len, cand_cap;
 };
 
@@ -114,7 +114,7 @@ EngineLayout engine_layout(int64_t tsz, int64_t tc, int64_t vc, int64_t mc, int6
     L.vid4 = take(tc * 16);
     L.twin4 = take(tc * 16);
     L.third4 = take(tc * 16);
-    L.stage = take(L.cand_cap * 4);
+    L.pending = take(L.cand_cap * 16);
     L.live = take(L.cand_cap * 16);
     L.end = o;
     return L;
@@ -298,9 +298,7 @@ template <class T> int weld(ccc_engine* e, const Tables& t, cudaStream_t s) {
     int* cnt = e->at<int>(L.wcnt);
     int* fan_end = e->at<int>(L.fan_end);
     CCC_LAUNCH("k_weld_insert", s, k_weld_insert<T><<<item_grid(), ITEM_THREADS, 0, s>>>(
-        t.f, x0, e->at<int>(L.wtab), vidc, e->hdr()));
-    CCC_LAUNCH_CHECK();
-    CCC_LAUNCH("k_weld_count", s, k_weld_count<T><<<item_grid(), ITEM_THREADS, 0, s>>>(t.f, x0, x1, vidc, cnt));
+        t.f, x0, x1, e->at<int>(L.wtab), vidc, cnt, e->hdr()));
     CCC_LAUNCH_CHECK();
     // (the table is not read after k_weld_insert: its space holds the classes' first entries)
     int* fan_start = e->at<int>(L.wtab);
@@ -329,11 +327,10 @@ Weld engine_weld(ccc_engine* e) {
 template <class T> int stage(ccc_engine* e, cudaStream_t s) {
     CCC_LAUNCH("k_ccd_stage_mask", s, k_ccd_stage_mask<T><<<num_sms() * 2, STAGE_THREADS, 0, s>>>(
         e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), engine_weld(e),
-        e->at<unsigned>(e->L.stage)));
+        e->at<int4>(e->L.live), e->at<int4>(e->L.pending)));
     CCC_LAUNCH_CHECK();
-    CCC_LAUNCH("k_ccd_stage_solvers", s, k_ccd_stage_solvers<<<num_sms() * 8, STAGE_THREADS, 0, s>>>(
-        e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), engine_weld(e), e->at<unsigned>(e->L.stage),
-        e->at<int4>(e->L.live)));
+    CCC_LAUNCH("k_ccd_stage_pending", s, k_ccd_stage_pending<<<num_sms() * 8, STAGE_THREADS, 0, s>>>(
+        (int)e->L.cand_cap, e->hdr(), engine_weld(e), e->at<int4>(e->L.pending), e->at<int4>(e->L.live)));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }

@@ -462,10 +462,10 @@ static __global__ void k_qtree_slots(Forest F, const TNode* __restrict__ nodes, 
 // (4 * slot + corner), twice its corner count, cleared to -1 before k_weld_insert:
 //  * k_weld_insert: every corner looks for an entry with its start position (compared with
 //    ==, so -0 meets +0 and NaN meets nothing) and claims an empty one otherwise; the
-//    claiming corner is the class's representative;
-//  * k_weld_count: class sizes (cnt, zeroed before), and CLS_NODEDUP on a class with a
-//    corner that differs from the representative in a bit of either position or whose
-//    coordinates do not come back from their displacement (x0 + (x1 - x0) != x1);
+//    claiming corner is the class's representative; the class sizes (cnt, zeroed before),
+//    and CLS_NODEDUP on a class with a corner that differs from the representative in a bit
+//    of either position or whose coordinates do not come back from their displacement
+//    (x0 + (x1 - x0) != x1);
 //  * k_weld_alloc: each class's range of the member list (a block-wide scan and one atomic
 //    per block), k_weld_fill: the members with their triangles' classes, k_weld_sort: each
 //    class's members in ascending corner id;
@@ -506,7 +506,8 @@ __device__ __forceinline__ WeldItem weld_item(const Forest& F, int M, int v) {
 }
 
 template <class T>
-__global__ void k_weld_insert(Forest F, const T* __restrict__ x0, int* tab, int* __restrict__ vidc, WsHeader* hdr) {
+__global__ void k_weld_insert(Forest F, const T* __restrict__ x0, const T* __restrict__ x1, int* tab,
+                              int* __restrict__ vidc, int* cnt, WsHeader* hdr) {
     const int M = forest_size(F);
     const int total = __ldg(F.voff + M);
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
@@ -542,28 +543,15 @@ __global__ void k_weld_insert(Forest F, const T* __restrict__ x0, int* tab, int*
                 rep = id;
             }
             vidc[id] = rep;
-        }
-    }
-}
-
-template <class T>
-__global__ void k_weld_count(Forest F, const T* __restrict__ x0, const T* __restrict__ x1,
-                             const int* __restrict__ vidc, int* cnt) {
-    const int M = forest_size(F);
-    const int total = __ldg(F.voff + M);
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
-        const WeldItem w = weld_item(F, M, v);
-        for (int c = 0; c < 3; ++c) {
-            const int id = (int)(4 * w.slot + c);
-            const int rep = __ldg(vidc + id);
-            const T* p0 = x0 + w.slot * 9 + 3 * c;
+            // the class's size, and whether this corner keeps it from being shared
             const T* p1 = x1 + w.slot * 9 + 3 * c;
             const T* r0 = x0 + (long long)(rep >> 2) * 9 + 3 * (rep & 3);
             const T* r1 = x1 + (long long)(rep >> 2) * 9 + 3 * (rep & 3);
+            const T pc[3] = {px, py, pz};
             bool ok = true;
 #pragma unroll
             for (int ax = 0; ax < 3; ++ax) {
-                const T a0 = __ldg(p0 + ax), a1 = __ldg(p1 + ax);
+                const T a0 = pc[ax], a1 = __ldg(p1 + ax);
                 const T d = a1 - a0;
                 ok = ok && (a0 + d) == a1;     // MovingTriangle::ComputeBBoxVertex's v + dv
                 ok = ok && weld_bits(a0) == weld_bits(__ldg(r0 + ax)) && weld_bits(a1) == weld_bits(__ldg(r1 + ax));

@@ -43,7 +43,8 @@ struct WsHeader {
     int solved;        // sub-tests solved (fewer than subtests when repeated ones are shared)
     int fan_cursor;    // engine corner classes: member list slots handed out
     int live_count;    // engine staging: pairs with sub-tests to solve (Weld.live)
-    int pad[8];
+    int pending_count; // engine staging: pairs left with vertex-face sub-tests to place
+    int pad[7];
 };
 
 struct __align__(16) TNode {
@@ -705,6 +706,28 @@ __device__ __forceinline__ bool classes_meet(int4 a, int4 b) {
 __device__ __forceinline__ int class_size(int4 v, int c) { return (v.w >> (5 * c)) & 31; }
 __device__ __forceinline__ int twin_kind(int4 v, int e) { return (v.w >> (15 + 2 * e)) & 3; }
 
+// The edge-edge pairs of sub-test 3e + f of pair (A, B): over the edges' twins ta, tb
+// (4 * slot + edge, or TWIN_NONE) whose third corners have classes ha, hb, the pairs
+// (a < b) that share no vertex, the pair itself first.
+template <class Fn>
+__device__ __forceinline__ void weld_ee_members(int A, int B, int e, int f, int4 VA, int4 VB, int ta, int tb, int ha,
+                                                int hb, Fn&& fn) {
+    // edge {01, 02, 12}[e]: corners e > 1 ? 1 : 0 and e > 0 ? 2 : 1
+    const int4 TA = make_int4(int4_at(VA, e > 1), int4_at(VA, e > 0 ? 2 : 1), ha, 0);
+    const int4 TB = make_int4(int4_at(VB, f > 1), int4_at(VB, f > 0 ? 2 : 1), hb, 0);
+    for (int i = 0; i < 2; ++i) {
+        if (i == 1 && ta < 0) break;
+        const int a = i ? ta >> 2 : A, sa = i ? ta & 3 : e;
+        for (int j = 0; j < 2; ++j) {
+            if (j == 1 && tb < 0) break;
+            const int b = j ? tb >> 2 : B, sb = j ? tb & 3 : f;
+            if (a >= b) continue;
+            if ((i | j) && classes_meet(i ? TA : VA, j ? TB : VB)) continue;
+            fn(a, b, 3 * sa + sb);
+        }
+    }
+}
+
 // Calls fn(a, b, type) for every pair that has sub-test k of pair (A, B) (A < B, live), the
 // pair itself included, and returns true; returns false without a call when the sub-test
 // is solved by each of its pairs.  VA, VB: W.vid[A], W.vid[B].
@@ -733,26 +756,12 @@ __device__ __forceinline__ bool weld_members(const Weld& W, int A, int B, int k,
     // (edges without a twin: the pair is the sub-test's only one)
     const int ka = twin_kind(VA, e), kb = twin_kind(VB, f);
     if (ka == 2 || kb == 2 || (ka | kb) == 0) return false;
-    // edge {01, 02, 12}[e]: corners e > 1 ? 1 : 0 and e > 0 ? 2 : 1
-    const int ua = int4_at(VA, e > 1), ub = int4_at(VA, e > 0 ? 2 : 1);
-    const int wa = int4_at(VB, f > 1), wb = int4_at(VB, f > 0 ? 2 : 1);
-    if ((ua | ub | wa | wb) & CLS_NODEDUP) return false;
-    const int ta = ka ? int4_at(__ldg(W.twin + A), e) : TWIN_NONE;
-    const int tb = kb ? int4_at(__ldg(W.twin + B), f) : TWIN_NONE;
-    // the twins' classes: the edge's two and their third corner's
-    const int4 TA = make_int4(ua, ub, ta >= 0 ? int4_at(__ldg(W.third + A), e) : 0, 0);
-    const int4 TB = make_int4(wa, wb, tb >= 0 ? int4_at(__ldg(W.third + B), f) : 0, 0);
-    for (int i = 0; i < 2; ++i) {
-        if (i == 1 && ta < 0) break;
-        const int a = i ? ta >> 2 : A, sa = i ? ta & 3 : e;
-        for (int j = 0; j < 2; ++j) {
-            if (j == 1 && tb < 0) break;
-            const int b = j ? tb >> 2 : B, sb = j ? tb & 3 : f;
-            if (a >= b) continue;
-            if ((i | j) && classes_meet(i ? TA : VA, j ? TB : VB)) continue;
-            fn(a, b, 3 * sa + sb);
-        }
-    }
+    if ((int4_at(VA, e > 1) | int4_at(VA, e > 0 ? 2 : 1) | int4_at(VB, f > 1) | int4_at(VB, f > 0 ? 2 : 1)) &
+        CLS_NODEDUP)
+        return false;
+    weld_ee_members(A, B, e, f, VA, VB, ka ? int4_at(__ldg(W.twin + A), e) : TWIN_NONE,
+                    kb ? int4_at(__ldg(W.twin + B), f) : TWIN_NONE, ka ? int4_at(__ldg(W.third + A), e) : 0,
+                    kb ? int4_at(__ldg(W.third + B), f) : 0, fn);
     return true;
 }
 
@@ -827,91 +836,199 @@ __device__ __forceinline__ int warp_inclusive_scan(int v, int lane) {
     return v;
 }
 
-// Staging of the resident engine's candidate pairs for k_ccd_narrow (Weld.live), in two
-// kernels so that each runs at the occupancy its work needs:
-//  * k_ccd_stage_mask: per pair, 0 when the triangles share a vertex (a corner class in
-//    common, the same relation as the reference's coordinate test), else the sub-box mask
-//    with the exact leaf-box test (the engine's candidates come from fp32 boxes rounded
-//    outward); hdr->subtests counts the sub-tests of the masks;
-//  * k_ccd_stage_solvers: the mask cut to the sub-tests the pair solves (weld_solves), with
-//    the shared ones marked in bits 15..29, appended to the list of pairs with work; each
-//    warp spreads its 32 pairs' sub-tests over its lanes, and few registers keep enough
-//    warps resident for the latency-bound scans of the corner classes.
+// Staging of the resident engine's candidate pairs for k_ccd_narrow: the list Weld.live of
+// the pairs with sub-tests to solve, in two kernels.
+//  * k_ccd_stage_mask: pairs whose triangles share a vertex (a corner class in common, the
+//    same relation as the reference's coordinate test) are dropped; the others queue per
+//    warp in shared memory and are taken 32 at a time, for the sub-box mask with the exact
+//    leaf-box test (the engine's candidates come from fp32 boxes rounded outward) and the
+//    choice of the pair that solves each sub-test wherever the triangles' own records tell
+//    it: every edge-edge sub-test (classes, twins and the twins' third corners) and the
+//    vertex-face sub-tests that are not shared.  A pair left with shared vertex-face
+//    sub-tests goes to the pending list, the others with work to the live list.
+//    hdr->subtests counts the sub-tests of the masks.
+//  * k_ccd_stage_pending: the pending pairs' vertex-face sub-tests, spread over the lanes
+//    of a warp (a scan of the vertex's class each); then the pairs go to the live list.
+// Records: (slot i, slot j, the sub-tests to solve in bits 0..14 with the shared ones in
+// bits 15..29, pending vertex-face sub-tests).
 static constexpr int STAGE_THREADS = 256;
+static constexpr int STAGE_WARPS = STAGE_THREADS / 32;
+
+// the pair that solves edge-edge sub-test k of pair (A, B) from the records of A and B
+__device__ __forceinline__ bool weld_ee_solves(int A, int B, int k, int4 VA, int4 VB, int4 TWA, int4 TWB, int4 THA,
+                                               int4 THB, bool* shared) {
+    const int e = k / 3, f = k - 3 * e;
+    const int ka = twin_kind(VA, e), kb = twin_kind(VB, f);
+    *shared = false;
+    if (ka == 2 || kb == 2 || (ka | kb) == 0) return true;
+    if ((int4_at(VA, e > 1) | int4_at(VA, e > 0 ? 2 : 1) | int4_at(VB, f > 1) | int4_at(VB, f > 0 ? 2 : 1)) &
+        CLS_NODEDUP)
+        return true;
+    *shared = true;
+    int ma = A, mb = B, mk = k;
+    weld_ee_members(A, B, e, f, VA, VB, ka ? int4_at(TWA, e) : TWIN_NONE, kb ? int4_at(TWB, f) : TWIN_NONE,
+                    int4_at(THA, e), int4_at(THB, f), [&](int a, int b, int kk) {
+                        if (a < ma || (a == ma && (b < mb || (b == mb && kk < mk)))) {
+                            ma = a;
+                            mb = b;
+                            mk = kk;
+                        }
+                    });
+    return ma == A && mb == B && mk == k;
+}
+
+// a record to the live list (work, no pending) or the pending list, warp-aggregated
+__device__ __forceinline__ void stage_emit(WsHeader* hdr, int4* live, int4* pending, int2 pr, unsigned word,
+                                           unsigned pend, bool valid) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const bool to_live = valid && pend == 0u && word != 0u, to_pend = valid && pend != 0u;
+    const unsigned ml = __ballot_sync(FULL, to_live), mp = __ballot_sync(FULL, to_pend);
+    int bl = 0, bp = 0;
+    if (lane == 0 && ml) bl = atomicAdd(&hdr->live_count, __popc(ml));
+    if (lane == 0 && mp) bp = atomicAdd(&hdr->pending_count, __popc(mp));
+    bl = __shfl_sync(FULL, bl, 0) + __popc(ml & lt);
+    bp = __shfl_sync(FULL, bp, 0) + __popc(mp & lt);
+    // (at most one record per candidate in either list)
+    if (to_live) live[bl] = make_int4(pr.x, pr.y, (int)word, 0);
+    if (to_pend) pending[bp] = make_int4(pr.x, pr.y, (int)word, (int)pend);
+}
+
 template <class T>
 __global__ void __launch_bounds__(STAGE_THREADS, 2)
 k_ccd_stage_mask(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ x0,
-                 const T* __restrict__ x1, Weld W, unsigned* __restrict__ stage) {
+                 const T* __restrict__ x1, Weld W, int4* __restrict__ live, int4* __restrict__ pending) {
+    __shared__ int2 q_pr[STAGE_WARPS][64];
+    __shared__ int4 q_va[STAGE_WARPS][64], q_vb[STAGE_WARPS][64];
     const int n = min(*(volatile int*)&hdr->cand_count, cand_cap);
-    int masked = 0;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-        const int2 pr = cand[c];
-        unsigned bits = 0;
-        if (!classes_meet(__ldg(W.vid + pr.x), __ldg(W.vid + pr.y))) {
-            bits = ccd_pair_subbox_mask<T, true>(x0, x1, pr.x, pr.y, true);
-            masked += __popc(bits);
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const int warps = gridDim.x * STAGE_WARPS;
+    int masked = 0, qn = 0;             // qn: queued live pairs of this warp (warp-uniform)
+    for (int base = (blockIdx.x * STAGE_WARPS + wq) * 32;; base += warps * 32) {
+        const bool more = base < n;
+        if (!more && qn == 0) break;
+        if (more) {
+            const int c = base + lane;
+            int2 pr = make_int2(0, 0);
+            int4 VA = make_int4(0, 0, 0, 0), VB = VA;
+            bool lv = false;
+            if (c < n) {
+                pr = cand[c];
+                VA = __ldg(W.vid + pr.x);
+                VB = __ldg(W.vid + pr.y);
+                lv = !classes_meet(VA, VB);
+            }
+            const unsigned m = __ballot_sync(FULL, lv);
+            if (lv) {
+                const int at = qn + __popc(m & lt);
+                q_pr[wq][at] = pr;
+                q_va[wq][at] = VA;
+                q_vb[wq][at] = VB;
+            }
+            qn += __popc(m);
+            __syncwarp();
         }
-        stage[c] = bits;
+        while (qn >= 32 || (!more && qn > 0)) {
+            const bool valid = lane < qn;
+            int2 pr = make_int2(0, 0);
+            unsigned word = 0u, pend = 0u;
+            if (valid) {
+                pr = q_pr[wq][lane];
+                const int4 VA = q_va[wq][lane], VB = q_vb[wq][lane];
+                const unsigned bits = ccd_pair_subbox_mask<T, true>(x0, x1, pr.x, pr.y, true);
+                masked += __popc(bits);
+                const unsigned ee = bits & 0x1ffu;
+                int4 TWA = make_int4(0, 0, 0, 0), TWB = TWA, THA = TWA, THB = TWA;
+                if (ee && ((VA.w | VB.w) >> 15)) {
+                    TWA = __ldg(W.twin + pr.x);
+                    TWB = __ldg(W.twin + pr.y);
+                    THA = __ldg(W.third + pr.x);
+                    THB = __ldg(W.third + pr.y);
+                }
+                for (unsigned b = bits; b; b &= b - 1) {
+                    const int k = __ffs(b) - 1;
+                    bool sh = false, solve = true;
+                    if (k < 9) {
+                        solve = weld_ee_solves(pr.x, pr.y, k, VA, VB, TWA, TWB, THA, THB, &sh);
+                    } else {
+                        const bool vf = k >= 12;
+                        const int4 Vface = vf ? VB : VA, Vvert = vf ? VA : VB;
+                        const int c = vf ? k - 12 : k - 9;
+                        if (!((int4_at(Vvert, c) | Vface.x | Vface.y | Vface.z) & CLS_NODEDUP) &&
+                            class_size(Vvert, c) >= 2) {
+                            pend |= 1u << k;
+                            solve = false;
+                        }
+                    }
+                    if (solve) word |= (1u << k) | (sh ? 1u << (15 + k) : 0u);
+                }
+            }
+            stage_emit(hdr, live, pending, pr, word, pend, valid);
+            // the queue's second half moves to the front
+            __syncwarp();
+            if (lane + 32 < qn) {
+                q_pr[wq][lane] = q_pr[wq][lane + 32];
+                q_va[wq][lane] = q_va[wq][lane + 32];
+                q_vb[wq][lane] = q_vb[wq][lane + 32];
+            }
+            qn = qn > 32 ? qn - 32 : 0;
+            __syncwarp();
+        }
     }
-    masked = __reduce_add_sync(0xffffffffu, masked);
-    if ((threadIdx.x & 31) == 0 && masked) atomicAdd(&hdr->subtests, masked);
+    masked = __reduce_add_sync(FULL, masked);
+    if (lane == 0 && masked) atomicAdd(&hdr->subtests, masked);
 }
 
 static __global__ void __launch_bounds__(STAGE_THREADS)
-k_ccd_stage_solvers(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, Weld W,
-                    const unsigned* __restrict__ stage, int4* __restrict__ live) {
-    // per warp: 32 pairs, their slots, classes, masks, the prefix of their sub-test counts
-    // and the sub-tests they solve; the warp's lanes take the pairs' sub-tests 32 at a time
+k_ccd_stage_pending(int cand_cap, WsHeader* hdr, Weld W, const int4* __restrict__ pending, int4* __restrict__ live) {
+    // per warp: 32 pending pairs, their classes, pending sub-tests, the prefix of their
+    // counts and the sub-tests they solve; the lanes take the sub-tests 32 at a time
     __shared__ int2 s_pr[STAGE_THREADS];
     __shared__ int4 s_va[STAGE_THREADS], s_vb[STAGE_THREADS];
     __shared__ unsigned s_bits[STAGE_THREADS], s_word[STAGE_THREADS];
     __shared__ int s_pre[STAGE_THREADS];
-    const int n = min(*(volatile int*)&hdr->cand_count, cand_cap);
+    const int n = min(*(volatile int*)&hdr->pending_count, cand_cap);
     const int tid = threadIdx.x, lane = tid & 31, w0 = tid & ~31;
     const unsigned FULL = 0xffffffffu;
-    const int warps = gridDim.x * (STAGE_THREADS / 32);
-    for (int base = (blockIdx.x * (STAGE_THREADS / 32) + (tid >> 5)) * 32; base < n; base += warps * 32) {
+    const int warps = gridDim.x * STAGE_WARPS;
+    for (int base = (blockIdx.x * STAGE_WARPS + (tid >> 5)) * 32; base < n; base += warps * 32) {
         const int c = base + lane;
-        const unsigned bits = c < n ? stage[c] : 0u;
+        unsigned pend = 0u, word = 0u;
         int2 pr = make_int2(0, 0);
-        if (bits) {
-            pr = cand[c];
+        if (c < n) {
+            const int4 rec = pending[c];
+            pr = make_int2(rec.x, rec.y);
+            word = (unsigned)rec.z;
+            pend = (unsigned)rec.w;
             s_va[tid] = __ldg(W.vid + pr.x);
             s_vb[tid] = __ldg(W.vid + pr.y);
         }
         s_pr[tid] = pr;
-        s_word[tid] = 0u;
-        // edge-edge sub-tests first, vertex-face ones after, so that a round of 32 runs one
-        // of the two scans
-#pragma unroll 1
-        for (int kind = 0; kind < 2; ++kind) {
-            const unsigned kb = bits & (kind ? 0x7e00u : 0x01ffu);
-            s_bits[tid] = kb;
-            const int incl = warp_inclusive_scan(__popc(kb), lane);
-            s_pre[tid] = incl;
-            const int total = __shfl_sync(FULL, incl, 31);
-            __syncwarp();
-            for (int r = lane; r < total; r += 32) {
-                int lo = 0, hi = 31;                       // the pair: first prefix above r
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if (s_pre[w0 + mid] > r) hi = mid;
-                    else lo = mid + 1;
-                }
-                const int p = w0 + lo;
-                const int k = __fns(s_bits[p], 0, r - (lo ? s_pre[p - 1] : 0) + 1);
-                bool sh = false;
-                if (weld_solves(W, s_pr[p].x, s_pr[p].y, k, s_va[p], s_vb[p], &sh))
-                    atomicOr(&s_word[p], (1u << k) | (sh ? 1u << (15 + k) : 0u));
+        s_bits[tid] = pend;
+        s_word[tid] = word;
+        const int incl = warp_inclusive_scan(__popc(pend), lane);
+        s_pre[tid] = incl;
+        const int total = __shfl_sync(FULL, incl, 31);
+        __syncwarp();
+        for (int r = lane; r < total; r += 32) {
+            int lo = 0, hi = 31;                       // the pair: first prefix above r
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (s_pre[w0 + mid] > r) hi = mid;
+                else lo = mid + 1;
             }
-            __syncwarp();
+            const int p = w0 + lo;
+            const int k = __fns(s_bits[p], 0, r - (lo ? s_pre[p - 1] : 0) + 1);
+            bool sh = false;
+            if (weld_solves(W, s_pr[p].x, s_pr[p].y, k, s_va[p], s_vb[p], &sh))
+                atomicOr(&s_word[p], (1u << k) | (sh ? 1u << (15 + k) : 0u));
         }
-        const unsigned word = s_word[tid];
-        const unsigned has = __ballot_sync(FULL, word != 0u);
-        int at = 0;
-        if (lane == 0 && has) at = atomicAdd(&hdr->live_count, __popc(has));
-        at = __shfl_sync(FULL, at, 0) + __popc(has & ((1u << lane) - 1u));
-        if (word) live[at] = make_int4(pr.x, pr.y, (int)word, 0);     // (at most one per candidate)
+        __syncwarp();
+        word = s_word[tid];
+        stage_emit(hdr, live, nullptr, pr, word, 0u, c < n);
         __syncwarp();
     }
 }
