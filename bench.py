@@ -29,7 +29,9 @@ plain per-mesh path, with exact pair sets and p50 / p99 latency.
   copies overlapping the neighbouring steps' kernels.
 * ``roofline`` — the dominant kernel (CUDA-event timing of the same step run ungraphed)
   against MEASURED_PEAKS.json; ``refit_roofline`` / ``build_roofline`` the tree kernels;
-  ``fp64`` the narrow phase's arithmetic rate.
+  ``fp64`` the narrow kernel's arithmetic rate over the sub-tests it solves, and
+  ``narrow_phase`` the staging and narrow kernels together over every sub-test (a repeated
+  sub-test is solved once for all the pairs that have it).
 * ``cpu_baseline`` — the oracle (C++ restatement of the reference pipeline, OpenMP) on a
   bounded sample of the batched meshes on the host cores.
 
@@ -60,11 +62,12 @@ UNIT = "triangle-steps/s"
 MAXC, MAXCOL = 32, 16            # no candidate overflow on any of the 64 meshes
 FP64_PEAK_NOMINAL_GFLOPS = 37000.0   # B200 FP64 datasheet figure (not measured here)
 FLOPS_PER_SUBTEST = 252          # coefficients 162 + Cardano and filter 90 (transcendentals as 1)
-# DRAM bytes (read + write) of one k_ccd_narrow launch per candidate pair, from ncu's
-# dram__bytes_read.sum + dram__bytes_write.sum on the 16-mesh batched step (74.6 MB + 4.8 MB
-# for 3,091,227 pairs); the 64-mesh launch is too large for a full capture, so its traffic
-# is this figure times its own pair count.
-NARROW_DRAM_BYTES_PER_PAIR = (74.574848e6 + 4.76416e6) / 3091227
+# DRAM bytes (read + write) of one k_ccd_narrow launch per sub-test solved, from ncu's
+# dram__bytes_read.sum + dram__bytes_write.sum on the 32-mesh batched step; the 64-mesh
+# launch is too large for a full capture, so its traffic is this figure times its own count.
+NARROW_DRAM_BYTES_PER_SOLVED = (239520768 + 57656064) / 11536974
+# the kernels of the narrow phase: staging (masks, solver choice), then the solves
+NARROW_PHASE = ("k_ccd_stage_mask", "k_ccd_stage_pending", "k_ccd_narrow")
 
 
 def parse():
@@ -373,7 +376,9 @@ def run_ours(args, rank, world, dev):
     peak, peak_kind = load_peaks()
     dname, (dms, dcount) = max(kern.items(), key=lambda kv: kv[1][0])
     per_launch = dms / dcount
-    narrow_bytes = cnt["candidates"] * (8 + 2 * 2 * 72) + int(sum(nrow)) * 32
+    # k_ccd_narrow reads a 16-byte record per pair with work and gathers both triangles at
+    # both ends of the step (2 x 2 x 72 bytes); it writes 32 bytes per row
+    narrow_bytes = cnt["live_pairs"] * (16 + 2 * 2 * 72) + int(sum(nrow)) * 32
     achieved = narrow_bytes / (per_launch / 1e3) / 1e9 if dname == "k_ccd_narrow" else None
     # the refit is two passes (block-local, then the climbs that leave a block)
     r1 = kern.get("k_engine_refit", (float("nan"), 1))
@@ -381,7 +386,10 @@ def run_ours(args, rank, world, dev):
     refit_ms = r1[0] / r1[1] + r2[0] / r2[1]
     rb = sum(refit_bytes(f) for f in Fs)
     bb_ = sum(build_bytes(f) for f in Fs)
-    fp64_gflops = cnt["subtests"] * FLOPS_PER_SUBTEST / (kern["k_ccd_narrow"][0] / kern["k_ccd_narrow"][1] / 1e3) / 1e9
+    narrow_ms = kern["k_ccd_narrow"][0] / kern["k_ccd_narrow"][1]
+    fp64_gflops = cnt["solved"] * FLOPS_PER_SUBTEST / (narrow_ms / 1e3) / 1e9
+    phase_ms = sum(kern[k][0] / kern[k][1] for k in NARROW_PHASE if k in kern)
+    phase_gflops = cnt["subtests"] * FLOPS_PER_SUBTEST / (phase_ms / 1e3) / 1e9
     eng.close()
 
     result = None
@@ -396,7 +404,7 @@ def run_ours(args, rank, world, dev):
             "config": workload_config(meshes, world),
             "roofline": {"kernel": dname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                         "traffic": (NARROW_DRAM_BYTES_PER_PAIR * cnt["candidates"]) if dname == "k_ccd_narrow"
+                         "traffic": (NARROW_DRAM_BYTES_PER_SOLVED * cnt["solved"]) if dname == "k_ccd_narrow"
                          else None,
                          "alg_bytes_per_launch": narrow_bytes, "launch_ms": per_launch},
             "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
@@ -405,12 +413,16 @@ def run_ours(args, rank, world, dev):
                     "path": "engine.StepPipeline from pinned host memory, rows + times back",
                     "rows_equal_batched": bool(e2e_equal)},
             "work": {"autotuned_shape": shape, "candidates": cnt["candidates"], "subtests": cnt["subtests"],
+                     "subtests_solved": cnt["solved"], "pairs_with_work": cnt["live_pairs"],
                      "roots_in_unit_interval": cnt["roots"], "collision_rows": int(sum(nrow)), "status": cnt["status"],
                      "tree_boxes": "fp32"},
             "kernel_ms_per_step": {k: r3(v[0] / v[1]) for k, v in kern.items()},
-            "fp64": {"kernel": "k_ccd_narrow", "achieved_gflops": r3(fp64_gflops),
+            "fp64": {"kernel": "k_ccd_narrow", "units": "sub-tests solved", "achieved_gflops": r3(fp64_gflops),
                      "peak_gflops": FP64_PEAK_NOMINAL_GFLOPS, "peak_source": "nominal (B200 datasheet)",
                      "frac": r3(fp64_gflops / FP64_PEAK_NOMINAL_GFLOPS)},
+            "narrow_phase": {"kernels": list(NARROW_PHASE), "ms": r3(phase_ms), "units": "every sub-test",
+                             "effective_gflops": r3(phase_gflops),
+                             "frac": r3(phase_gflops / FP64_PEAK_NOMINAL_GFLOPS)},
             "refit_roofline": {"alg_bytes": rb, "ms": r3(refit_ms), "achieved": r3(rb / (refit_ms / 1e3) / 1e9),
                                "peak": peak, "unit": "GB/s", "frac": r3(rb / (refit_ms / 1e3) / 1e9 / peak)},
             "build_roofline": {"alg_bytes": bb_, "ms": r3(build_ms), "achieved": r3(bb_ / (build_ms / 1e3) / 1e9),

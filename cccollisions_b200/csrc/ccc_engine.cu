@@ -823,6 +823,7 @@ int ccc_engine_counters(ccc_engine* e, int32_t* out, void* stream) {
     out[2] = h.subtests;
     out[3] = h.roots;
     out[4] = h.solved;
+    out[5] = h.live_count;
     return CCC_OK;
 }
 

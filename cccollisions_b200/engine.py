@@ -214,12 +214,13 @@ class Engine:
 
     def counters(self) -> dict:
         """Synchronises; work counters of the last step: status word, candidate pairs,
-        sub-tests with overlapping sub-boxes, roots in [0, 1] filtered, and sub-tests solved
-        (each repeated sub-test is solved once for all the pairs that have it)."""
-        out = (ctypes.c_int32 * 5)()
+        sub-tests with overlapping sub-boxes, roots in [0, 1] filtered, sub-tests solved
+        (each repeated sub-test is solved once for all the pairs that have it) and the
+        candidate pairs with sub-tests to solve."""
+        out = (ctypes.c_int32 * 6)()
         N.check(N.lib().ccc_engine_counters(self.handle, out, _stream(self.device)), "ccc_engine_counters")
         return {"status": int(out[0]), "candidates": int(out[1]), "subtests": int(out[2]), "roots": int(out[3]),
-                "solved": int(out[4])}
+                "solved": int(out[4]), "live_pairs": int(out[5])}
 
     def pack_rows(self, out_rows: torch.Tensor, out_times: torch.Tensor, out_meta: torch.Tensor):
         """Packs the last ccd()'s rows of every active mesh back to back on the device (no

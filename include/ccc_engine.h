@@ -135,12 +135,12 @@ int ccc_engine_read_state(ccc_engine* e, const int32_t* slot_ids, int64_t n, int
 int ccc_engine_pack_rows(ccc_engine* e, int64_t* out_rows, void* out_times, int64_t capacity, int32_t* out_meta,
                          void* stream);
 
-/* Synchronise the stream and read the work counters of the last step into out[5]: status
+/* Synchronise the stream and read the work counters of the last step into out[6]: status
  * word, candidate pairs, continuous sub-tests (pair, type) whose swept sub-boxes overlap,
- * roots in [0, 1] filtered, and sub-tests solved.  A sub-test that several pairs of a mesh
- * have with the same tetrahedron (a vertex-face test over the triangles around the vertex,
- * an edge-edge test over the two triangles of an edge) is solved once, and its rows or
- * contacts are written for each of those pairs. */
+ * roots in [0, 1] filtered, sub-tests solved, and candidate pairs with sub-tests to solve.
+ * A sub-test that several pairs of a mesh have with the same tetrahedron (a vertex-face
+ * test over the triangles around the vertex, an edge-edge test over the two triangles of an
+ * edge) is solved once, and its rows or contacts are written for each of those pairs. */
 int ccc_engine_counters(ccc_engine* e, int32_t* out, void* stream);
 
 #ifdef __cplusplus
