@@ -348,7 +348,7 @@ template <class T> int ccd_step(ccc_engine* e, cudaStream_t s) {
     if (rc) return rc;
     int g = num_sms() * CCD_MIN_BLOCKS * SHAPES[e->shape].narrow;
     cudaError_t le = cudaSuccess;
-    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV>(
+    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV, true>(
         g, s, e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f,
         e->at<long long>(e->L.rows), e->at<T>(e->L.times), (int)e->maxcol, e->at<int>(e->L.mesh_cnt), engine_weld(e),
         CornerSink<T>{})));
@@ -373,7 +373,7 @@ template <class T> int loop_step(ccc_engine* e, int max_iter, cudaStream_t s) {
     int g = num_sms() * CCD_MIN_BLOCKS * SHAPES[e->shape].narrow;
     LoopSink<T> sink{e->at<T>(e->L.masses), e->at<int>(e->L.faces), t.vt, e->at<long long>(e->L.acc), contacts};
     cudaError_t le = cudaSuccess;
-    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIBV>(
+    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIBV, true>(
         g, s, e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f, nullptr,
         nullptr, 0, e->at<int>(e->L.mesh_cnt), engine_weld(e), sink)));
     if (le != cudaSuccess) return CCC_ERR_CUDA;
@@ -470,10 +470,10 @@ bool active_built(const ccc_engine* e) {
 // shared-memory attributes of the narrow-phase kernels an engine launches, set before any
 // stream capture
 template <class T> bool prepare_kernels() {
-    return prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_REFERENCE>() == cudaSuccess &&
-           prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_PORTABLE>() == cudaSuccess &&
-           prepare_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIB_REFERENCE>() == cudaSuccess &&
-           prepare_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIB_PORTABLE>() == cudaSuccess;
+    return prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_REFERENCE, true>() == cudaSuccess &&
+           prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_PORTABLE, true>() == cudaSuccess &&
+           prepare_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIB_REFERENCE, true>() == cudaSuccess &&
+           prepare_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIB_PORTABLE, true>() == cudaSuccess;
 }
 
 int run_op(ccc_engine* e, int op, int max_iter, cudaStream_t s) {

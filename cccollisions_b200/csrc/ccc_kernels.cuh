@@ -1039,14 +1039,14 @@ k_ccd_stage_pending(int cand_cap, WsHeader* hdr, Weld W, const int4* __restrict_
 // every operation of this library's own in it is contraction-proof (mulrn / addrn / subrn,
 // fmaT).  The other units see only the launcher's declaration; ccc_narrow.cu instantiates
 // the (type, mode, sink, math library) combinations the library launches.
-template <class T, int MODE, class Sink, int LIB>
+template <class T, int MODE, class Sink, int LIB, bool STAGED>
 cudaError_t launch_ccd_narrow(int grid, cudaStream_t s, const int2* cand, int cand_cap, WsHeader* hdr, const T* x0,
                               const T* x1, Forest F, long long* rows, T* times, int max_per_tri, int* mesh_counters,
                               Weld W, Sink sink);
-template <class T, int MODE, class Sink, int LIB> cudaError_t prepare_ccd_narrow();
+template <class T, int MODE, class Sink, int LIB, bool STAGED> cudaError_t prepare_ccd_narrow();
 
 #ifdef CCC_NARROW_TU
-template <class T, int MODE, class Sink, int LIB>
+template <class T, int MODE, class Sink, int LIB, bool STAGED>
 __global__ void __launch_bounds__(CCD_BLOCK, CCD_MIN_BLOCKS)
 k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ x0,
              const T* __restrict__ x1, Forest F, long long* __restrict__ rows, T* __restrict__ times, int max_per_tri,
@@ -1070,7 +1070,7 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned FULL = 0xffffffffu;
     const unsigned lt = (1u << lane) - 1u;
-    const int n = min(*(volatile int*)(W.live ? &hdr->live_count : &hdr->cand_count), cand_cap);
+    const int n = min(*(volatile int*)(STAGED ? &hdr->live_count : &hdr->cand_count), cand_cap);
     int head = 0, queued = 0;           // ring queue of sub-tests (block-uniform)
     int masked = 0;                     // this thread's sub-tests before repeats are shared
     // class counts and root count of a batch, two sets used by alternate batches: a batch
@@ -1088,7 +1088,7 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
             int2 pr = make_int2(0, 0);
             uint32_t bits = 0;
             unsigned shared_bits = 0;
-            if (W.live) {
+            if constexpr (STAGED) {
                 // the resident engine's pairs come staged by k_ccd_stage_*: the pairs with
                 // sub-tests to solve, which ones, and which of them stand for their repeats
                 const long long c = base + tid;
@@ -1250,17 +1250,22 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                     const T tv = root_val[j];
                     // every pair of a shared sub-test is in the mesh of (qx, qy)
                     const OutRegion R = out_region(F, M, qx, max_per_tri);
-                    int ma[WELD_FANCAP], mb[WELD_FANCAP], mk[WELD_FANCAP];
-                    const int nm = weld_list(W, qx, qy, k, (it.x >> 28) & 1, ma, mb, mk);
-                    for (int i = 0; i < nm; ++i) {
+                    auto row = [&](int a, int b, int kk) {
                         long long r = append_row(mesh_counters, F, R.m, R.cap, &hdr->status);
                         if (r >= 0) {
                             long long o = (long long)R.po * max_per_tri + r;
-                            rows[o * 3 + 0] = ma[i] - R.po;
-                            rows[o * 3 + 1] = mb[i] - R.po;
-                            rows[o * 3 + 2] = mk[i];
+                            rows[o * 3 + 0] = a - R.po;
+                            rows[o * 3 + 1] = b - R.po;
+                            rows[o * 3 + 2] = kk;
                             times[o] = tv;
                         }
+                    };
+                    if constexpr (STAGED) {
+                        int ma[WELD_FANCAP], mb[WELD_FANCAP], mk[WELD_FANCAP];
+                        const int nm = weld_list(W, qx, qy, k, (it.x >> 28) & 1, ma, mb, mk);
+                        for (int i = 0; i < nm; ++i) row(ma[i], mb[i], mk[i]);
+                    } else {
+                        row(qx, qy, k);
                     }
                 };
                 for (int b0 = warp * 32; b0 < nroots; b0 += CCD_BLOCK) {
@@ -1298,8 +1303,14 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                     MTet<T> tet = load_tet(x0, x1, q.x, q.y, k);
                     if (!ccd_filter(tet, k, root)) continue;
                     // the contact of every pair with this sub-test (its own corner masses)
-                    int ma[WELD_FANCAP], mb[WELD_FANCAP], mk[WELD_FANCAP];
-                    const int nm = weld_list(W, q.x, q.y, k, (it.x >> 28) & 1, ma, mb, mk);
+                    int ma[STAGED ? WELD_FANCAP : 1], mb[STAGED ? WELD_FANCAP : 1], mk[STAGED ? WELD_FANCAP : 1];
+                    int nm = 1;
+                    if constexpr (STAGED) nm = weld_list(W, q.x, q.y, k, (it.x >> 28) & 1, ma, mb, mk);
+                    else {
+                        ma[0] = q.x;
+                        mb[0] = q.y;
+                        mk[0] = k;
+                    }
                     for (int i = 0; i < nm; ++i) {
                         const int a = ma[i], b = mb[i], kk = mk[i];
                         T mq[4];
@@ -1330,24 +1341,24 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
 // instantiation and device; prepare_ccd_narrow does it ahead of any stream capture).
 // The flags are atomic because host threads may launch on different streams at once; two
 // first calls may both set the attribute, which is harmless.
-template <class T, int MODE, class Sink, int LIB> cudaError_t prepare_ccd_narrow() {
+template <class T, int MODE, class Sink, int LIB, bool STAGED> cudaError_t prepare_ccd_narrow() {
     static std::atomic<bool> done[64];
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && done[dev].load(std::memory_order_acquire)) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(k_ccd_narrow<T, MODE, Sink, LIB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_ccd_narrow<T, MODE, Sink, LIB, STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)CcdLayout<T>::bytes);
     if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev].store(true, std::memory_order_release);
     return e;
 }
 
-template <class T, int MODE, class Sink, int LIB>
+template <class T, int MODE, class Sink, int LIB, bool STAGED>
 cudaError_t launch_ccd_narrow(int grid, cudaStream_t s, const int2* cand, int cand_cap, WsHeader* hdr, const T* x0,
                               const T* x1, Forest F, long long* rows, T* times, int max_per_tri, int* mesh_counters,
                               Weld W, Sink sink) {
-    cudaError_t e = prepare_ccd_narrow<T, MODE, Sink, LIB>();
+    cudaError_t e = prepare_ccd_narrow<T, MODE, Sink, LIB, STAGED>();
     if (e != cudaSuccess) return e;
-    k_ccd_narrow<T, MODE, Sink, LIB><<<grid, CCD_BLOCK, CcdLayout<T>::bytes, s>>>(
+    k_ccd_narrow<T, MODE, Sink, LIB, STAGED><<<grid, CCD_BLOCK, CcdLayout<T>::bytes, s>>>(
         cand, cand_cap, hdr, x0, x1, F, rows, times, max_per_tri, mesh_counters, W, sink);
     return cudaSuccess;
 }
