@@ -169,13 +169,15 @@ struct Ranges {
 };
 
 // launch shapes: traversal blocks per SM, narrow-phase blocks per SM (one is resident at
-// a time; more blocks split the work finer), and the traversal's schedule (0: one query
-// per thread, k_traverse_q; 1: 32 queries per warp walking together, k_traverse_w)
+// a time; more blocks split the work finer), the traversal's schedule (0: one query per
+// thread, k_traverse_q; 1: 32 queries per warp walking together, k_traverse_w) and, for
+// k_traverse_q, the tree levels below the root each block copies into shared memory (0-2)
 struct Shape {
-    int trav, narrow, warp;
+    int trav, narrow, warp, stage;
 };
-constexpr Shape SHAPES[] = {{4, 1, 0}, {8, 1, 0}, {16, 1, 0}, {4, 2, 0}, {8, 2, 0}, {16, 2, 0}, {8, 4, 0},
-                            {16, 4, 0}, {32, 8, 0}, {4, 2, 1},  {8, 2, 1}, {16, 2, 1}, {32, 2, 1}};
+constexpr Shape SHAPES[] = {{4, 1, 0, 0},  {8, 1, 0, 0},  {16, 1, 0, 0}, {4, 2, 0, 0},  {8, 2, 0, 0},  {16, 2, 0, 0},
+                            {8, 4, 0, 0},  {16, 4, 0, 0}, {32, 8, 0, 0}, {4, 2, 1, 0},  {8, 2, 1, 0},  {16, 2, 1, 0},
+                            {32, 2, 1, 0}, {16, 2, 0, 1}, {16, 2, 0, 2}, {32, 8, 0, 1}, {32, 8, 0, 2}};
 constexpr int NSHAPES = sizeof(SHAPES) / sizeof(SHAPES[0]);
 constexpr int DEFAULT_SHAPE = 4;
 
@@ -278,8 +280,16 @@ template <class T> int traverse(ccc_engine* e, const Tables& t, const int* flags
         CCC_LAUNCH("k_traverse", s, k_traverse_w<<<g, TRAV_THREADS, 0, s>>>(
             e->at<QNode>(e->L.qnodes), e->at<int>(e->L.qleaf), e->at<int>(e->L.leaf_tri), t.f, e->at<int2>(e->L.cand),
             (int)e->L.cand_cap, e->hdr(), flags));
+    else if (SHAPES[e->shape].stage == 0)
+        CCC_LAUNCH("k_traverse", s, k_traverse_q<0><<<g, TRAV_THREADS, 0, s>>>(
+            e->at<QNode>(e->L.qnodes), e->at<int>(e->L.qleaf), e->at<int>(e->L.leaf_tri), t.f, e->at<int2>(e->L.cand),
+            (int)e->L.cand_cap, e->hdr(), flags));
+    else if (SHAPES[e->shape].stage == 1)
+        CCC_LAUNCH("k_traverse", s, k_traverse_q<1><<<g, TRAV_THREADS, 0, s>>>(
+            e->at<QNode>(e->L.qnodes), e->at<int>(e->L.qleaf), e->at<int>(e->L.leaf_tri), t.f, e->at<int2>(e->L.cand),
+            (int)e->L.cand_cap, e->hdr(), flags));
     else
-        CCC_LAUNCH("k_traverse", s, k_traverse_q<<<g, TRAV_THREADS, 0, s>>>(
+        CCC_LAUNCH("k_traverse", s, k_traverse_q<2><<<g, TRAV_THREADS, 0, s>>>(
             e->at<QNode>(e->L.qnodes), e->at<int>(e->L.qleaf), e->at<int>(e->L.leaf_tri), t.f, e->at<int2>(e->L.cand),
             (int)e->L.cand_cap, e->hdr(), flags));
     CCC_LAUNCH_CHECK();
@@ -778,6 +788,7 @@ int ccc_engine_schedule_info(int32_t choice, int32_t* out) {
     out[0] = SHAPES[choice].trav;
     out[1] = SHAPES[choice].narrow;
     out[2] = SHAPES[choice].warp;
+    out[3] = SHAPES[choice].stage;
     return CCC_OK;
 }
 

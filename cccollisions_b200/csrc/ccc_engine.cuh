@@ -905,94 +905,168 @@ static __global__ void k_engine_refit_front(Forest F, const int* __restrict__ np
 // so each unordered pair is found once) and emits (min id, max id) in data slots.  Candidates
 // are the pairs whose fp32 boxes overlap, a superset of the exact ones; the continuous
 // narrow phase re-tests every pair's swept sub-boxes exactly.
+//
+// SD > 0: the top SD + 1 levels of the mesh of a block's first query (at most 1 + 4 + 16
+// QNodes) are copied into shared memory at every step of the block's loop, breadth first,
+// and every reference from one copied node to another is rewritten to TRAV_STAGED | its
+// index among the copies; the block's queries of that mesh start at the copied root and read
+// those nodes from shared memory.  The other queries (a block spanning two meshes) walk
+// the global nodes.
+static constexpr int TRAV_STAGED = 1 << 30;
+__device__ __forceinline__ int trav_stage_count(int sd) { return sd == 0 ? 0 : (sd == 1 ? 5 : 21); }
+
+template <int SD>
 static __global__ void __launch_bounds__(TRAV_THREADS)
 k_traverse_q(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, const int* __restrict__ leaf_tri,
              Forest F, int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const int* __restrict__ mflags) {
     int stack[STACK_DEPTH];          // per-thread, in local memory (L1): shared memory holds the buffer
     __shared__ int2 cbuf[TRAV_BUF][TRAV_THREADS];     // candidate buffer (see flush_candidates)
+    __shared__ QNode top[SD > 0 ? (SD == 1 ? 5 : 21) : 1];
+    __shared__ int top_src[SD > 0 ? (SD == 1 ? 5 : 21) : 1];    // global index of each copy
+    __shared__ int top_n, top_mesh;
     int nbuf = 0;
     const int tid = threadIdx.x;
     const int M = forest_size(F);
     const int total = __ldg(F.voff + M);
-    for (int v = blockIdx.x * blockDim.x + tid; v < total; v += gridDim.x * blockDim.x) {
-        int m = find_mesh(F.voff, M, v, 0);
-        int vo = __ldg(F.voff + m), po = __ldg(F.poff + m);
-        int n = __ldg(F.voff + m + 1) - vo;
-        int p = v - vo;
-        if (n < 2) continue;
-        if (mflags && (__ldg(mflags + __ldg(F.sid + m)) & MF_DONE)) continue;
-        const QNode* qn = qnodes + po;
-        const int qid = __ldg(leaf_tri + po + p);
-        const int lq = __ldg(qleaf + po + p);
-        if (qid < 0 || qid >= n || lq < 0 || (lq >> 2) >= n - 1) {
-            atomicOr(&hdr->status, ST_MALFORMED_TREE);
-            continue;
-        }
-        float qlo[3], qhi[3];
-        {
-            const float* f = reinterpret_cast<const float*>(qn + (lq >> 2));
-            const int sl = lq & 3;
-            qlo[0] = __ldg(f + 0 + sl);
-            qlo[1] = __ldg(f + 4 + sl);
-            qlo[2] = __ldg(f + 8 + sl);
-            qhi[0] = __ldg(f + 12 + sl);
-            qhi[1] = __ldg(f + 16 + sl);
-            qhi[2] = __ldg(f + 20 + sl);
-        }
-        int sp = 0;
-        int node = 0;
-        const int limit = 2 * n + 64;
-        for (int it = 0;; ++it) {
-            if (it > limit) { atomicOr(&hdr->status, ST_MALFORMED_TREE); break; }
-            const float4* f = reinterpret_cast<const float4*>(qn + node);
-            const float4 LX = __ldg(f + 0), LY = __ldg(f + 1), LZ = __ldg(f + 2);
-            const float4 HX = __ldg(f + 3), HY = __ldg(f + 4), HZ = __ldg(f + 5);
-            const int4 R = __ldg(reinterpret_cast<const int4*>(f + 6));
-            const int4 A = __ldg(reinterpret_cast<const int4*>(f + 7));
-            const float lx[4] = {LX.x, LX.y, LX.z, LX.w}, ly[4] = {LY.x, LY.y, LY.z, LY.w};
-            const float lz[4] = {LZ.x, LZ.y, LZ.z, LZ.w}, hx[4] = {HX.x, HX.y, HX.z, HX.w};
-            const float hy[4] = {HY.x, HY.y, HY.z, HY.w}, hz[4] = {HZ.x, HZ.y, HZ.z, HZ.w};
-            const int rr[4] = {R.x, R.y, R.z, R.w}, aa[4] = {A.x, A.y, A.z, A.w};
-            int next = -1;
-            bool bad = false, deep = false;
-#pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                const int ref = rr[s];
-                if (ref == Q_EMPTY) continue;
-                if (ref >= n - 1 || (ref < 0 && ~ref >= n)) { bad = true; continue; }
-                bool hit = (qlo[0] <= hx[s]) && (qhi[0] >= lx[s]) && (qlo[1] <= hy[s]) && (qhi[1] >= ly[s]) &&
-                           (qlo[2] <= hz[s]) && (qhi[2] >= lz[s]);
-                const int rightmost = ref < 0 ? ~ref : aa[s];
-                if (p >= rightmost) hit = false;
-                if (!hit) continue;
-                if (ref < 0) {
-                    const int cid = aa[s];
-                    cbuf[nbuf++][tid] = make_int2(po + min(qid, cid), po + max(qid, cid));
-                    if (nbuf == TRAV_BUF) {
-                        cg::coalesced_group grp = cg::coalesced_threads();
-                        int base = 0;
-                        if (grp.thread_rank() == 0) base = atomicAdd(&hdr->cand_count, TRAV_BUF * (int)grp.size());
-                        base = grp.shfl(base, 0) + TRAV_BUF * (int)grp.thread_rank();
-                        flush_candidates(cbuf, tid, TRAV_BUF, base, cand, cand_cap, hdr);
-                        nbuf = 0;
-                    }
-                } else if (next < 0) {
-                    next = ref;
-                } else if (sp < STACK_DEPTH) {
-                    stack[sp++] = ref;
-                } else {
-                    deep = true;
+    for (int base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
+        if (SD > 0) {
+            // copy the top levels of the first query's mesh (block-uniform steps)
+            __syncthreads();       // the previous step's walks are done with the copies
+            if (tid == 0) {
+                const int m0 = find_mesh(F.voff, M, base, 0);
+                const int n0 = __ldg(F.voff + m0 + 1) - __ldg(F.voff + m0);
+                const bool ok = n0 >= 2 && !(mflags && (__ldg(mflags + __ldg(F.sid + m0)) & MF_DONE));
+                top_mesh = ok ? m0 : -1;
+                top_n = ok ? 1 : 0;
+                top_src[0] = 0;
+            }
+            __syncthreads();
+            const int m0 = top_mesh;
+            const QNode* qn0 = qnodes + (m0 >= 0 ? __ldg(F.poff + m0) : 0);
+            const int n0 = m0 >= 0 ? __ldg(F.voff + m0 + 1) - __ldg(F.voff + m0) : 0;
+            int lo = 0;                                 // first copy of the current level
+#pragma unroll 1
+            for (int lev = 0; lev <= SD && m0 >= 0; ++lev) {
+                const int hi = top_n;                   // copies [lo, hi) are this level's
+                // copy the level's nodes, 8 threads a node (16 bytes each)
+                for (int w = tid; w < (hi - lo) * 8; w += blockDim.x) {
+                    const int i = lo + w / 8, part = w % 8;
+                    reinterpret_cast<int4*>(top + i)[part] =
+                        __ldg(reinterpret_cast<const int4*>(qn0 + top_src[i]) + part);
                 }
+                __syncthreads();
+                if (lev < SD && tid == 0) {
+                    // the next level: the copies' internal children, rewritten to their copies
+                    int cnt = hi;
+                    for (int i = lo; i < hi; ++i) {
+                        int* rr = reinterpret_cast<int*>(&top[i].ref);
+                        for (int sl = 0; sl < 4; ++sl) {
+                            const int r = rr[sl];
+                            if (r == Q_EMPTY || r < 0 || r >= n0 - 1) continue;    // leaf, empty or bad
+                            top_src[cnt] = r;
+                            rr[sl] = TRAV_STAGED | cnt;
+                            ++cnt;
+                        }
+                    }
+                    top_n = cnt;
+                }
+                __syncthreads();
+                lo = hi;
             }
-            if (bad || deep) {
-                atomicOr(&hdr->status, bad ? ST_MALFORMED_TREE : ST_STACK_OVERFLOW);
-                break;
+        }
+        const int v = base + tid;
+        if (v < total) {
+            const int m = find_mesh(F.voff, M, v, 0);
+            const int vo = __ldg(F.voff + m), po = __ldg(F.poff + m);
+            const int n = __ldg(F.voff + m + 1) - vo;
+            const int p = v - vo;
+            bool go = n >= 2 && !(mflags && (__ldg(mflags + __ldg(F.sid + m)) & MF_DONE));
+            const QNode* qn = qnodes + po;
+            const int qid = go ? __ldg(leaf_tri + po + p) : 0;
+            const int lq = go ? __ldg(qleaf + po + p) : 0;
+            if (go && (qid < 0 || qid >= n || lq < 0 || (lq >> 2) >= n - 1)) {
+                atomicOr(&hdr->status, ST_MALFORMED_TREE);
+                go = false;
             }
-            if (next >= 0) {
-                node = next;
-            } else {
-                if (sp == 0) break;
-                node = stack[--sp];
+            if (go) {
+                float qlo[3], qhi[3];
+                {
+                    const float* f = reinterpret_cast<const float*>(qn + (lq >> 2));
+                    const int sl = lq & 3;
+                    qlo[0] = __ldg(f + 0 + sl);
+                    qlo[1] = __ldg(f + 4 + sl);
+                    qlo[2] = __ldg(f + 8 + sl);
+                    qhi[0] = __ldg(f + 12 + sl);
+                    qhi[1] = __ldg(f + 16 + sl);
+                    qhi[2] = __ldg(f + 20 + sl);
+                }
+                int sp = 0;
+                int node = (SD > 0 && m == top_mesh) ? TRAV_STAGED : 0;
+                const int limit = 2 * n + 64;
+                for (int it = 0;; ++it) {
+                    if (it > limit) {
+                        atomicOr(&hdr->status, ST_MALFORMED_TREE);
+                        break;
+                    }
+                    float4 LX, LY, LZ, HX, HY, HZ;
+                    int4 R, A;
+                    if (SD > 0 && (node & TRAV_STAGED)) {
+                        const QNode& t = top[node & 0xff];
+                        LX = t.lox; LY = t.loy; LZ = t.loz; HX = t.hix; HY = t.hiy; HZ = t.hiz; R = t.ref; A = t.aux;
+                    } else {
+                        const float4* f = reinterpret_cast<const float4*>(qn + node);
+                        LX = __ldg(f + 0); LY = __ldg(f + 1); LZ = __ldg(f + 2);
+                        HX = __ldg(f + 3); HY = __ldg(f + 4); HZ = __ldg(f + 5);
+                        R = __ldg(reinterpret_cast<const int4*>(f + 6));
+                        A = __ldg(reinterpret_cast<const int4*>(f + 7));
+                    }
+                    const float lx[4] = {LX.x, LX.y, LX.z, LX.w}, ly[4] = {LY.x, LY.y, LY.z, LY.w};
+                    const float lz[4] = {LZ.x, LZ.y, LZ.z, LZ.w}, hx[4] = {HX.x, HX.y, HX.z, HX.w};
+                    const float hy[4] = {HY.x, HY.y, HY.z, HY.w}, hz[4] = {HZ.x, HZ.y, HZ.z, HZ.w};
+                    const int rr[4] = {R.x, R.y, R.z, R.w}, aa[4] = {A.x, A.y, A.z, A.w};
+                    int next = -1;
+                    bool bad = false, deep = false;
+#pragma unroll
+                    for (int s = 0; s < 4; ++s) {
+                        const int ref = rr[s];
+                        if (ref == Q_EMPTY) continue;
+                        const bool staged = SD > 0 && ref >= 0 && (ref & TRAV_STAGED);
+                        if (!staged && (ref >= n - 1 || (ref < 0 && ~ref >= n))) { bad = true; continue; }
+                        bool hit = (qlo[0] <= hx[s]) && (qhi[0] >= lx[s]) && (qlo[1] <= hy[s]) && (qhi[1] >= ly[s]) &&
+                                   (qlo[2] <= hz[s]) && (qhi[2] >= lz[s]);
+                        const int rightmost = ref < 0 ? ~ref : aa[s];
+                        if (p >= rightmost) hit = false;
+                        if (!hit) continue;
+                        if (ref < 0) {
+                            const int cid = aa[s];
+                            cbuf[nbuf++][tid] = make_int2(po + min(qid, cid), po + max(qid, cid));
+                            if (nbuf == TRAV_BUF) {
+                                cg::coalesced_group grp = cg::coalesced_threads();
+                                int b0 = 0;
+                                if (grp.thread_rank() == 0) b0 = atomicAdd(&hdr->cand_count, TRAV_BUF * (int)grp.size());
+                                b0 = grp.shfl(b0, 0) + TRAV_BUF * (int)grp.thread_rank();
+                                flush_candidates(cbuf, tid, TRAV_BUF, b0, cand, cand_cap, hdr);
+                                nbuf = 0;
+                            }
+                        } else if (next < 0) {
+                            next = ref;
+                        } else if (sp < STACK_DEPTH) {
+                            stack[sp++] = ref;
+                        } else {
+                            deep = true;
+                        }
+                    }
+                    if (bad || deep) {
+                        atomicOr(&hdr->status, bad ? ST_MALFORMED_TREE : ST_STACK_OVERFLOW);
+                        break;
+                    }
+                    if (next >= 0) {
+                        node = next;
+                    } else {
+                        if (sp == 0) break;
+                        node = stack[--sp];
+                    }
+                }
             }
         }
     }

@@ -187,13 +187,15 @@ class Engine:
     @staticmethod
     def schedules() -> list[dict]:
         """The autotuner's candidate schedules: traversal blocks per SM, narrow-phase blocks
-        per SM (in units of the resident count) and the traversal form (0 one query per
-        thread, 1 32 queries per warp)."""
+        per SM (in units of the resident count), the traversal form (0 one query per
+        thread, 1 32 queries per warp) and the tree levels below the root that each
+        traversal block keeps in shared memory (0-2, one query per thread)."""
         out = []
         for i in range(N.lib().ccc_engine_schedule_count()):
-            a = (ctypes.c_int32 * 3)()
+            a = (ctypes.c_int32 * 4)()
             N.check(N.lib().ccc_engine_schedule_info(i, a), "ccc_engine_schedule_info")
-            out.append({"traversal_blocks_per_sm": a[0], "narrow_blocks": a[1], "warp_traversal": a[2]})
+            out.append({"traversal_blocks_per_sm": a[0], "narrow_blocks": a[1], "warp_traversal": a[2],
+                        "staged_levels": a[3]})
         return out
 
     def set_schedule(self, choice: int):
