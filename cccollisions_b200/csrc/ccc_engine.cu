@@ -171,13 +171,16 @@ struct Ranges {
 // launch shapes: traversal blocks per SM, narrow-phase blocks per SM (one is resident at
 // a time; more blocks split the work finer), the traversal's schedule (0: one query per
 // thread, k_traverse_q; 1: 32 queries per warp walking together, k_traverse_w) and, for
-// k_traverse_q, the tree levels below the root each block copies into shared memory (0-2)
+// k_traverse_q, the tree levels below the root each block copies into shared memory (0-2),
+// and the narrow phase's batch (1: 256 sub-tests, 2: 512)
 struct Shape {
-    int trav, narrow, warp, stage;
+    int trav, narrow, warp, stage, batch;
 };
-constexpr Shape SHAPES[] = {{4, 1, 0, 0},  {8, 1, 0, 0},  {16, 1, 0, 0}, {4, 2, 0, 0},  {8, 2, 0, 0},  {16, 2, 0, 0},
-                            {8, 4, 0, 0},  {16, 4, 0, 0}, {32, 8, 0, 0}, {4, 2, 1, 0},  {8, 2, 1, 0},  {16, 2, 1, 0},
-                            {32, 2, 1, 0}, {16, 2, 0, 1}, {16, 2, 0, 2}, {32, 8, 0, 1}, {32, 8, 0, 2}};
+constexpr Shape SHAPES[] = {{4, 1, 0, 0, 1},  {8, 1, 0, 0, 1},  {16, 1, 0, 0, 1}, {4, 2, 0, 0, 1},  {8, 2, 0, 0, 1},
+                            {16, 2, 0, 0, 1}, {8, 4, 0, 0, 1},  {16, 4, 0, 0, 1}, {32, 8, 0, 0, 1}, {4, 2, 1, 0, 1},
+                            {8, 2, 1, 0, 1},  {16, 2, 1, 0, 1}, {32, 2, 1, 0, 1}, {16, 2, 0, 1, 1}, {16, 2, 0, 2, 1},
+                            {32, 8, 0, 1, 1}, {32, 8, 0, 2, 1}, {16, 1, 0, 0, 2}, {16, 2, 0, 0, 2}, {32, 4, 0, 0, 2},
+                            {32, 8, 0, 0, 2}};
 constexpr int NSHAPES = sizeof(SHAPES) / sizeof(SHAPES[0]);
 constexpr int DEFAULT_SHAPE = 4;
 
@@ -358,10 +361,16 @@ template <class T> int ccd_step(ccc_engine* e, cudaStream_t s) {
     if (rc) return rc;
     int g = num_sms() * CCD_MIN_BLOCKS * SHAPES[e->shape].narrow;
     cudaError_t le = cudaSuccess;
-    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV, true>(
-        g, s, e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f,
-        e->at<long long>(e->L.rows), e->at<T>(e->L.times), (int)e->maxcol, e->at<int>(e->L.mesh_cnt), engine_weld(e),
-        CornerSink<T>{})));
+    if (SHAPES[e->shape].batch == 2)
+        CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV, true, 2>(
+            g, s, e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f,
+            e->at<long long>(e->L.rows), e->at<T>(e->L.times), (int)e->maxcol, e->at<int>(e->L.mesh_cnt),
+            engine_weld(e), CornerSink<T>{})));
+    else
+        CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV, true>(
+            g, s, e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f,
+            e->at<long long>(e->L.rows), e->at<T>(e->L.times), (int)e->maxcol, e->at<int>(e->L.mesh_cnt),
+            engine_weld(e), CornerSink<T>{})));
     if (le != cudaSuccess) return CCC_ERR_CUDA;
     CCC_LAUNCH_CHECK();
     return CCC_OK;
@@ -383,9 +392,14 @@ template <class T> int loop_step(ccc_engine* e, int max_iter, cudaStream_t s) {
     int g = num_sms() * CCD_MIN_BLOCKS * SHAPES[e->shape].narrow;
     LoopSink<T> sink{e->at<T>(e->L.masses), e->at<int>(e->L.faces), t.vt, e->at<long long>(e->L.acc), contacts};
     cudaError_t le = cudaSuccess;
-    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIBV, true>(
-        g, s, e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f, nullptr,
-        nullptr, 0, e->at<int>(e->L.mesh_cnt), engine_weld(e), sink)));
+    if (SHAPES[e->shape].batch == 2)
+        CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIBV, true, 2>(
+            g, s, e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f,
+            nullptr, nullptr, 0, e->at<int>(e->L.mesh_cnt), engine_weld(e), sink)));
+    else
+        CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIBV, true>(
+            g, s, e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f,
+            nullptr, nullptr, 0, e->at<int>(e->L.mesh_cnt), engine_weld(e), sink)));
     if (le != cudaSuccess) return CCC_ERR_CUDA;
     CCC_LAUNCH_CHECK();
     CCC_LAUNCH("k_loop_update", s, k_loop_update<<<grid_for(e->mesh_cap, ITEM_THREADS), ITEM_THREADS, 0, s>>>(
@@ -483,7 +497,11 @@ template <class T> bool prepare_kernels() {
     return prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_REFERENCE, true>() == cudaSuccess &&
            prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_PORTABLE, true>() == cudaSuccess &&
            prepare_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIB_REFERENCE, true>() == cudaSuccess &&
-           prepare_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIB_PORTABLE, true>() == cudaSuccess;
+           prepare_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIB_PORTABLE, true>() == cudaSuccess &&
+           prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_REFERENCE, true, 2>() == cudaSuccess &&
+           prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_PORTABLE, true, 2>() == cudaSuccess &&
+           prepare_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIB_REFERENCE, true, 2>() == cudaSuccess &&
+           prepare_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIB_PORTABLE, true, 2>() == cudaSuccess;
 }
 
 int run_op(ccc_engine* e, int op, int max_iter, cudaStream_t s) {
@@ -789,6 +807,7 @@ int ccc_engine_schedule_info(int32_t choice, int32_t* out) {
     out[1] = SHAPES[choice].narrow;
     out[2] = SHAPES[choice].warp;
     out[3] = SHAPES[choice].stage;
+    out[4] = SHAPES[choice].batch;
     return CCC_OK;
 }
 

@@ -619,24 +619,25 @@ template <class T> struct CornerSink {
 static constexpr int CCD_BLOCK = CCC_CCD_BLOCK;
 static constexpr int CCD_MIN_BLOCKS = CCC_CCD_MIN_BLOCKS;      // resident blocks per SM
 static constexpr int CCD_BATCH = CCC_CCD_BATCH_MULT * CCD_BLOCK;
-static constexpr int CCD_QUEUE = CCD_BATCH + 15 * CCD_BLOCK;  // a partial batch plus a chunk's worst case
 static_assert(CCD_BLOCK % 32 == 0 && CCD_BLOCK <= 1024 && 3 * CCD_BATCH <= 65536, "CCD_BLOCK");
 
 constexpr size_t align16(size_t x) { return (x + 15) / 16 * 16; }
 
-// dynamic shared memory of one block (byte offsets)
-template <class T> struct CcdLayout {
-    static constexpr size_t rec = 0;                                                   // double [6][BATCH]
-    static constexpr size_t root_val = rec + 6 * CCD_BATCH * sizeof(double);           // T [3 BATCH]
-    static constexpr size_t items = align16(root_val + 3 * CCD_BATCH * sizeof(T));     // int2 [QUEUE]
-    static constexpr size_t clist = items + CCD_QUEUE * sizeof(int2);                  // u16 [BATCH]
-    static constexpr size_t root_rec = clist + CCD_BATCH * 2;                          // u16 [3 BATCH]
-    static constexpr size_t rec_cls = root_rec + 3 * CCD_BATCH * 2;                    // u8 [BATCH]
-    static constexpr size_t rec_pos = align16(rec_cls + CCD_BATCH);                    // u16 [BATCH]
-    static constexpr size_t spairs = align16(rec_pos + CCD_BATCH * 2);                 // int2 [BLOCK]
+// dynamic shared memory of one block (byte offsets) for batches of NB sub-tests
+template <class T, int NB = CCD_BATCH> struct CcdLayout {
+    static constexpr int QUEUE = NB + 15 * CCD_BLOCK;     // a partial batch plus a chunk's worst case
+    static constexpr size_t rec = 0;                                                   // double [6][NB]
+    static constexpr size_t root_val = rec + 6 * NB * sizeof(double);                  // T [3 NB]
+    static constexpr size_t items = align16(root_val + 3 * NB * sizeof(T));            // int2 [QUEUE]
+    static constexpr size_t clist = items + QUEUE * sizeof(int2);                      // u16 [NB]
+    static constexpr size_t root_rec = clist + NB * 2;                                 // u16 [3 NB]
+    static constexpr size_t rec_cls = root_rec + 3 * NB * 2;                           // u8 [NB]
+    static constexpr size_t rec_pos = align16(rec_cls + NB);                           // u16 [NB]
+    static constexpr size_t spairs = align16(rec_pos + NB * 2);                        // int2 [BLOCK]
     static constexpr size_t pbuf = spairs + CCD_BLOCK * sizeof(int2);                   // u16 [BLOCK / 32][64]
     static constexpr size_t ints = align16(pbuf + (CCD_BLOCK / 32) * 64 * 2);          // int [64]
     static constexpr size_t bytes = ints + 64 * sizeof(int);
+    static_assert(3 * NB <= 65536, "batch indices are 16-bit");
 };
 
 // slots of the small int area
@@ -1039,20 +1040,20 @@ k_ccd_stage_pending(int cand_cap, WsHeader* hdr, Weld W, const int4* __restrict_
 // every operation of this library's own in it is contraction-proof (mulrn / addrn / subrn,
 // fmaT).  The other units see only the launcher's declaration; ccc_narrow.cu instantiates
 // the (type, mode, sink, math library) combinations the library launches.
-template <class T, int MODE, class Sink, int LIB, bool STAGED>
+template <class T, int MODE, class Sink, int LIB, bool STAGED, int BM = 1>
 cudaError_t launch_ccd_narrow(int grid, cudaStream_t s, const int2* cand, int cand_cap, WsHeader* hdr, const T* x0,
                               const T* x1, Forest F, long long* rows, T* times, int max_per_tri, int* mesh_counters,
                               Weld W, Sink sink);
-template <class T, int MODE, class Sink, int LIB, bool STAGED> cudaError_t prepare_ccd_narrow();
+template <class T, int MODE, class Sink, int LIB, bool STAGED, int BM = 1> cudaError_t prepare_ccd_narrow();
 
 #ifdef CCC_NARROW_TU
-template <class T, int MODE, class Sink, int LIB, bool STAGED>
+template <class T, int MODE, class Sink, int LIB, bool STAGED, int BM>
 __global__ void __launch_bounds__(CCD_BLOCK, CCD_MIN_BLOCKS)
 k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ x0,
              const T* __restrict__ x1, Forest F, long long* __restrict__ rows, T* __restrict__ times, int max_per_tri,
              int* __restrict__ mesh_counters, Weld W, Sink sink) {
     extern __shared__ __align__(16) unsigned char smem[];
-    using L = CcdLayout<T>;
+    using L = CcdLayout<T, BM * CCD_BLOCK>;
     double* rec = reinterpret_cast<double*>(smem + L::rec);
     T* root_val = reinterpret_cast<T*>(smem + L::root_val);
     int2* items = reinterpret_cast<int2*>(smem + L::items);
@@ -1064,8 +1065,8 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
     unsigned short* pbuf = reinterpret_cast<unsigned short*>(smem + L::pbuf);
     int* ints = reinterpret_cast<int*>(smem + L::ints);
     constexpr int NW = CCD_BLOCK / 32;
-    constexpr int NB = CCD_BATCH;
-    constexpr int Q = CCD_QUEUE;
+    constexpr int NB = BM * CCD_BLOCK;
+    constexpr int Q = L::QUEUE;
     const int M = forest_size(F);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned FULL = 0xffffffffu;
@@ -1341,24 +1342,25 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
 // instantiation and device; prepare_ccd_narrow does it ahead of any stream capture).
 // The flags are atomic because host threads may launch on different streams at once; two
 // first calls may both set the attribute, which is harmless.
-template <class T, int MODE, class Sink, int LIB, bool STAGED> cudaError_t prepare_ccd_narrow() {
+template <class T, int MODE, class Sink, int LIB, bool STAGED, int BM> cudaError_t prepare_ccd_narrow() {
     static std::atomic<bool> done[64];
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && done[dev].load(std::memory_order_acquire)) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(k_ccd_narrow<T, MODE, Sink, LIB, STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)CcdLayout<T>::bytes);
+    cudaError_t e = cudaFuncSetAttribute(k_ccd_narrow<T, MODE, Sink, LIB, STAGED, BM>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)CcdLayout<T, BM * CCD_BLOCK>::bytes);
     if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev].store(true, std::memory_order_release);
     return e;
 }
 
-template <class T, int MODE, class Sink, int LIB, bool STAGED>
+template <class T, int MODE, class Sink, int LIB, bool STAGED, int BM>
 cudaError_t launch_ccd_narrow(int grid, cudaStream_t s, const int2* cand, int cand_cap, WsHeader* hdr, const T* x0,
                               const T* x1, Forest F, long long* rows, T* times, int max_per_tri, int* mesh_counters,
                               Weld W, Sink sink) {
-    cudaError_t e = prepare_ccd_narrow<T, MODE, Sink, LIB, STAGED>();
+    cudaError_t e = prepare_ccd_narrow<T, MODE, Sink, LIB, STAGED, BM>();
     if (e != cudaSuccess) return e;
-    k_ccd_narrow<T, MODE, Sink, LIB, STAGED><<<grid, CCD_BLOCK, CcdLayout<T>::bytes, s>>>(
+    k_ccd_narrow<T, MODE, Sink, LIB, STAGED, BM><<<grid, CCD_BLOCK, CcdLayout<T, BM * CCD_BLOCK>::bytes, s>>>(
         cand, cand_cap, hdr, x0, x1, F, rows, times, max_per_tri, mesh_counters, W, sink);
     return cudaSuccess;
 }

@@ -188,14 +188,15 @@ class Engine:
     def schedules() -> list[dict]:
         """The autotuner's candidate schedules: traversal blocks per SM, narrow-phase blocks
         per SM (in units of the resident count), the traversal form (0 one query per
-        thread, 1 32 queries per warp) and the tree levels below the root that each
-        traversal block keeps in shared memory (0-2, one query per thread)."""
+        thread, 1 32 queries per warp), the tree levels below the root that each traversal
+        block keeps in shared memory (0-2, one query per thread) and the narrow phase's
+        batch in units of 256 sub-tests (1 or 2)."""
         out = []
         for i in range(N.lib().ccc_engine_schedule_count()):
-            a = (ctypes.c_int32 * 4)()
+            a = (ctypes.c_int32 * 5)()
             N.check(N.lib().ccc_engine_schedule_info(i, a), "ccc_engine_schedule_info")
             out.append({"traversal_blocks_per_sm": a[0], "narrow_blocks": a[1], "warp_traversal": a[2],
-                        "staged_levels": a[3]})
+                        "staged_levels": a[3], "narrow_batch": a[4]})
         return out
 
     def set_schedule(self, choice: int):

@@ -107,16 +107,17 @@ int ccc_engine_replay(ccc_engine* e, int op, void* stream);
 
 /* Launch-shape autotuner: times the collision step of the active set for each candidate
  * schedule (traversal and narrow-phase grid sizes, traversal form, tree levels staged in
- * shared memory), keeps the fastest and returns its index.  It only recomputes collision
- * rows.  Choices are cached per (dtype, size class). */
+ * shared memory, narrow-phase batch size), keeps the fastest and returns its index.  It
+ * only recomputes collision rows.  Choices are cached per (dtype, size class). */
 int ccc_engine_autotune(ccc_engine* e, void* stream, int32_t* choice);
 
 /* The autotuner's candidate schedules (no counterpart in the reference): their number;
- * the parameters of one in out[4] (out[0] traversal blocks per SM, out[1] narrow-phase
+ * the parameters of one in out[5] (out[0] traversal blocks per SM, out[1] narrow-phase
  * blocks per SM in units of the resident count, out[2] traversal form: 0 one query per
  * thread, 1 32 queries per warp walking the tree together, out[3] tree levels below the
- * root that each block of the one-query-per-thread form copies into shared memory, 0-2);
- * and fixing the engine to one of them. */
+ * root that each block of the one-query-per-thread form copies into shared memory, 0-2,
+ * out[4] the narrow phase's batch in units of 256 sub-tests, 1 or 2); and fixing the
+ * engine to one of them. */
 int ccc_engine_schedule_count(void);
 int ccc_engine_schedule_info(int32_t choice, int32_t* out);
 int ccc_engine_set_schedule(ccc_engine* e, int32_t choice);

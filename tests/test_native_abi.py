@@ -203,22 +203,24 @@ def test_reference_module_name_imports_the_drop_in(native_lib):
 
 
 def test_engine_schedules_are_described(native_lib):
-    """The autotuner's candidates cover both traversal forms and 0-2 tree levels staged in
-    shared memory; out-of-range choices are argument errors (no engine or device needed)."""
+    """The autotuner's candidates cover both traversal forms, 0-2 tree levels staged in
+    shared memory and both narrow batch sizes; out-of-range choices are argument errors (no
+    engine or device needed)."""
     import ctypes
 
     from cccollisions_b200 import _native as N
     n = native_lib.ccc_engine_schedule_count()
     assert n >= 2
-    forms, stages = set(), set()
+    forms, stages, batches = set(), set(), set()
     for i in range(n):
-        a = (ctypes.c_int32 * 4)()
+        a = (ctypes.c_int32 * 5)()
         assert native_lib.ccc_engine_schedule_info(i, a) == 0
-        assert a[0] > 0 and a[1] > 0 and a[2] in (0, 1) and a[3] in (0, 1, 2)
+        assert a[0] > 0 and a[1] > 0 and a[2] in (0, 1) and a[3] in (0, 1, 2) and a[4] in (1, 2)
         assert a[3] == 0 or a[2] == 0
         forms.add(a[2])
         stages.add(a[3])
-    assert forms == {0, 1} and stages == {0, 1, 2}
-    a = (ctypes.c_int32 * 4)()
+        batches.add(a[4])
+    assert forms == {0, 1} and stages == {0, 1, 2} and batches == {1, 2}
+    a = (ctypes.c_int32 * 5)()
     assert native_lib.ccc_engine_schedule_info(n, a) == N.CCC_ERR_INVALID_ARG
     assert native_lib.ccc_engine_set_schedule(None, 0) == N.CCC_ERR_INVALID_ARG
