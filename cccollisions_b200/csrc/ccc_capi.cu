@@ -277,7 +277,7 @@ int ccd_impl(const void* bboxes, const int64_t* tree, const void* x0, const void
     rc = run_broad_phase<T>(bboxes, tree, mask, B, F, (T)0, is_f32<T>(), P, s);
     if (rc) return rc;
     cudaError_t le = cudaSuccess;
-    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV, false>(
+    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV, SRC_CANDIDATES>(
         num_sms() * CCD_MIN_BLOCKS, s, P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, (long long*)rows,
         (T*)times, (int)maxcol, P.mesh_cnt, Weld{}, CornerSink<T>{})));
     if (le != cudaSuccess) return CCC_ERR_CUDA;
@@ -294,7 +294,7 @@ int mincol_impl(const void* bboxes, const int64_t* tree, const void* x0, const v
     rc = run_broad_phase<T>(bboxes, tree, nullptr, B, F, (T)0, is_f32<T>(), P, s);
     if (rc) return rc;
     cudaError_t le = cudaSuccess;
-    CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_MINCOL, CornerSink<T>, LIB_PORTABLE, false>(
+    CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_MINCOL, CornerSink<T>, LIB_PORTABLE, SRC_CANDIDATES>(
         num_sms() * CCD_MIN_BLOCKS, s, P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, (long long*)rows,
         nullptr, (int)(maxc * 15), P.mesh_cnt, Weld{}, CornerSink<T>{}));
     if (le != cudaSuccess) return CCC_ERR_CUDA;
@@ -327,7 +327,7 @@ int impulses_impl(const void* bboxes, const int64_t* tree, const void* x0, const
     rc = run_broad_phase<T>(bboxes, tree, mask, B, F, (T)0, is_f32<T>(), P, s);
     if (rc) return rc;
     cudaError_t le = cudaSuccess;
-    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_IMPULSES, CornerSink<T>, LIBV, false>(
+    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_IMPULSES, CornerSink<T>, LIBV, SRC_CANDIDATES>(
         num_sms() * CCD_MIN_BLOCKS, s, P.cand, (int)P.L.cand_cap, P.hdr, (const T*)x0, (const T*)x1, P.forest, nullptr, nullptr, 0,
         P.mesh_cnt, Weld{}, CornerSink<T>{(const T*)masses, (T*)dv, (T*)dx, (int*)cnt})));
     if (le != cudaSuccess) return CCC_ERR_CUDA;

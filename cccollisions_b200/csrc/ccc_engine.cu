@@ -362,12 +362,12 @@ template <class T> int ccd_step(ccc_engine* e, cudaStream_t s) {
     int g = num_sms() * CCD_MIN_BLOCKS * SHAPES[e->shape].narrow;
     cudaError_t le = cudaSuccess;
     if (SHAPES[e->shape].batch == 2)
-        CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV, true, 2>(
+        CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV, SRC_STAGED, 2>(
             g, s, e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f,
             e->at<long long>(e->L.rows), e->at<T>(e->L.times), (int)e->maxcol, e->at<int>(e->L.mesh_cnt),
             engine_weld(e), CornerSink<T>{})));
     else
-        CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV, true>(
+        CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV, SRC_STAGED>(
             g, s, e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f,
             e->at<long long>(e->L.rows), e->at<T>(e->L.times), (int)e->maxcol, e->at<int>(e->L.mesh_cnt),
             engine_weld(e), CornerSink<T>{})));
@@ -381,25 +381,20 @@ template <class T> int loop_step(ccc_engine* e, int max_iter, cudaStream_t s) {
     Tables t = e->active();
     int* flags = e->at<int>(e->L.flags);
     int* contacts = e->at<int>(e->L.contacts);
-    int rc = weld<T>(e, t, s);
-    if (rc) return rc;
-    rc = refit<T>(e, t, flags, s);
+    // (repeated sub-tests are not shared here: a loop iteration's narrow phase is mostly
+    // contacts, which every pair computes with its own masses, and the class rebuild and
+    // staging cost more than the solves they save)
+    int rc = refit<T>(e, t, flags, s);
     if (rc) return rc;
     rc = traverse<T>(e, t, flags, s);
     if (rc) return rc;
-    rc = stage<T>(e, s);
-    if (rc) return rc;
     int g = num_sms() * CCD_MIN_BLOCKS * SHAPES[e->shape].narrow;
+    const Weld W{};
     LoopSink<T> sink{e->at<T>(e->L.masses), e->at<int>(e->L.faces), t.vt, e->at<long long>(e->L.acc), contacts};
     cudaError_t le = cudaSuccess;
-    if (SHAPES[e->shape].batch == 2)
-        CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIBV, true, 2>(
-            g, s, e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f,
-            nullptr, nullptr, 0, e->at<int>(e->L.mesh_cnt), engine_weld(e), sink)));
-    else
-        CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIBV, true>(
-            g, s, e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f,
-            nullptr, nullptr, 0, e->at<int>(e->L.mesh_cnt), engine_weld(e), sink)));
+    CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIBV, SRC_EXACT>(
+        g, s, e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), t.f,
+        nullptr, nullptr, 0, e->at<int>(e->L.mesh_cnt), W, sink)));
     if (le != cudaSuccess) return CCC_ERR_CUDA;
     CCC_LAUNCH_CHECK();
     CCC_LAUNCH("k_loop_update", s, k_loop_update<<<grid_for(e->mesh_cap, ITEM_THREADS), ITEM_THREADS, 0, s>>>(
@@ -494,14 +489,12 @@ bool active_built(const ccc_engine* e) {
 // shared-memory attributes of the narrow-phase kernels an engine launches, set before any
 // stream capture
 template <class T> bool prepare_kernels() {
-    return prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_REFERENCE, true>() == cudaSuccess &&
-           prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_PORTABLE, true>() == cudaSuccess &&
-           prepare_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIB_REFERENCE, true>() == cudaSuccess &&
-           prepare_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIB_PORTABLE, true>() == cudaSuccess &&
-           prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_REFERENCE, true, 2>() == cudaSuccess &&
-           prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_PORTABLE, true, 2>() == cudaSuccess &&
-           prepare_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIB_REFERENCE, true, 2>() == cudaSuccess &&
-           prepare_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIB_PORTABLE, true, 2>() == cudaSuccess;
+    return prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_REFERENCE, SRC_STAGED>() == cudaSuccess &&
+           prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_PORTABLE, SRC_STAGED>() == cudaSuccess &&
+           prepare_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIB_REFERENCE, SRC_EXACT>() == cudaSuccess &&
+           prepare_ccd_narrow<T, CCD_IMPULSES, LoopSink<T>, LIB_PORTABLE, SRC_EXACT>() == cudaSuccess &&
+           prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_REFERENCE, SRC_STAGED, 2>() == cudaSuccess &&
+           prepare_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIB_PORTABLE, SRC_STAGED, 2>() == cudaSuccess;
 }
 
 int run_op(ccc_engine* e, int op, int max_iter, cudaStream_t s) {

@@ -288,12 +288,9 @@ __device__ __forceinline__ bool ccd_pair_shares_vertex(const T* __restrict__ x0,
 
 // The mask of sub-tests whose swept boxes overlap, for a pair that shares no vertex
 // (REJECT_RIGID: 0 as well for a pair whose sub-tests can have no root, see the end).
-// leaf_box: 0 as well unless the pair's leaf boxes (each triangle's boxes at x0 and x1
-// merged, MergeTriBoundingBoxes, build_bvh.cu:452-460) overlap (checkOverlap, aabb.cu:
-// 107-111), for candidate pairs found on boxes rounded outward.
 template <class T, bool REJECT_RIGID = true>
 __device__ __forceinline__ uint32_t ccd_pair_subbox_mask(const T* __restrict__ x0, const T* __restrict__ x1,
-                                                         long long i, long long j, bool leaf_box = false) {
+                                                         long long i, long long j) {
     const T* a0 = x0 + i * 9;
     const T* a1 = x1 + i * 9;
     const T* b0 = x0 + j * 9;
@@ -303,32 +300,19 @@ __device__ __forceinline__ uint32_t ccd_pair_subbox_mask(const T* __restrict__ x
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
         T alo[3], ahi[3], blo[3], bhi[3], dv[6];
-        // the leaf boxes: Triangle::ComputeBBox at both ends (figures.cu:37-41), merged; fmin
-        // and fmax skip NaN and the comparisons below do not tell -0 from +0, so the order
-        // of the reductions does not change the overlap test
-        T la = 0, ha = 0, lb = 0, hb = 0;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             T av = __ldg(a0 + 3 * c + ax);
-            T a1v = __ldg(a1 + 3 * c + ax);
-            dv[c] = a1v - av;
+            dv[c] = __ldg(a1 + 3 * c + ax) - av;
             T ae = av + dv[c];
             alo[c] = fmn(av, ae);
             ahi[c] = fmx(av, ae);
             T bv = __ldg(b0 + 3 * c + ax);
-            T b1v = __ldg(b1 + 3 * c + ax);
-            dv[3 + c] = b1v - bv;
+            dv[3 + c] = __ldg(b1 + 3 * c + ax) - bv;
             T be = bv + dv[3 + c];
             blo[c] = fmn(bv, be);
             bhi[c] = fmx(bv, be);
-            if (leaf_box) {
-                la = c ? fmn(la, fmn(av, a1v)) : fmn(av, a1v);
-                ha = c ? fmx(ha, fmx(av, a1v)) : fmx(av, a1v);
-                lb = c ? fmn(lb, fmn(bv, b1v)) : fmn(bv, b1v);
-                hb = c ? fmx(hb, fmx(bv, b1v)) : fmx(bv, b1v);
-            }
         }
-        if (leaf_box && !(la <= hb && ha >= lb)) m = 0u;
         // finite displacement, and start positions below half the largest finite value so that
         // every difference of two of them is finite too
         const T half_max = sizeof(T) == 4 ? T(1.7e38) : T(8.9e307);
@@ -365,6 +349,31 @@ __device__ __forceinline__ uint32_t ccd_pair_subbox_mask(const T* __restrict__ x
     // root of that linear case (collisions_continuous.cu:531-535), so no sub-test of the pair
     // can give a row or a contact.
     return REJECT_RIGID && rigid ? 0u : m;
+}
+
+// Whether the pair's leaf boxes (each triangle's boxes at x0 and x1 merged,
+// MergeTriBoundingBoxes, build_bvh.cu:452-460) overlap (checkOverlap, aabb.cu:107-111), one
+// axis at a time; fmin / fmax skip NaN and the comparisons do not tell -0 from +0, so the
+// order of the reductions does not change the answer.
+template <class T>
+__device__ __forceinline__ bool ccd_pair_leaf_overlap(const T* __restrict__ x0, const T* __restrict__ x1, long long i,
+                                                      long long j) {
+    bool ov = true;
+#pragma unroll 1
+    for (int ax = 0; ax < 3; ++ax) {
+        T la = __ldg(x0 + i * 9 + ax), ha = la, lb = __ldg(x0 + j * 9 + ax), hb = lb;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const T a0 = __ldg(x0 + i * 9 + 3 * c + ax), a1 = __ldg(x1 + i * 9 + 3 * c + ax);
+            const T b0 = __ldg(x0 + j * 9 + 3 * c + ax), b1 = __ldg(x1 + j * 9 + 3 * c + ax);
+            la = fmn(la, fmn(a0, a1));
+            ha = fmx(ha, fmx(a0, a1));
+            lb = fmn(lb, fmn(b0, b1));
+            hb = fmx(hb, fmx(b0, b1));
+        }
+        ov = ov && la <= hb && ha >= lb;
+    }
+    return ov;
 }
 
 // 0 when the triangles share a vertex, else ccd_pair_subbox_mask

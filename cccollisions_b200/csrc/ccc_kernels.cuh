@@ -578,6 +578,11 @@ k_te_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T*
 }
 
 enum CcdMode { CCD_ROWS = 0, CCD_IMPULSES = 1, CCD_MINCOL = 2 };
+// where the continuous narrow phase takes its pairs from: the candidate buffer (the
+// reference-format operations), the candidate buffer with the pairs' exact leaf boxes
+// tested as well (the engine's impulse loop, whose candidates come from fp32 boxes rounded
+// outward), or the engine's staged list (shared sub-tests)
+enum CcdSource { SRC_CANDIDATES = 0, SRC_EXACT = 1, SRC_STAGED = 2 };
 
 // Receiver of the impulses of CCD_IMPULSES: per-corner sums and counters (F, 3, 3) / (F, 3)
 // of the reference's compute_impulses.  Per-corner masses (F, 3) feed the contact.
@@ -939,7 +944,8 @@ k_ccd_stage_mask(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, con
             if (valid) {
                 pr = q_pr[wq][lane];
                 const int4 VA = q_va[wq][lane], VB = q_vb[wq][lane];
-                const unsigned bits = ccd_pair_subbox_mask<T, true>(x0, x1, pr.x, pr.y, true);
+                const unsigned bits = ccd_pair_leaf_overlap<T>(x0, x1, pr.x, pr.y)
+                                          ? ccd_pair_subbox_mask<T, true>(x0, x1, pr.x, pr.y) : 0u;
                 masked += __popc(bits);
                 const unsigned ee = bits & 0x1ffu;
                 int4 TWA = make_int4(0, 0, 0, 0), TWB = TWA, THA = TWA, THB = TWA;
@@ -1040,20 +1046,21 @@ k_ccd_stage_pending(int cand_cap, WsHeader* hdr, Weld W, const int4* __restrict_
 // every operation of this library's own in it is contraction-proof (mulrn / addrn / subrn,
 // fmaT).  The other units see only the launcher's declaration; ccc_narrow.cu instantiates
 // the (type, mode, sink, math library) combinations the library launches.
-template <class T, int MODE, class Sink, int LIB, bool STAGED, int BM = 1>
+template <class T, int MODE, class Sink, int LIB, int SRC, int BM = 1>
 cudaError_t launch_ccd_narrow(int grid, cudaStream_t s, const int2* cand, int cand_cap, WsHeader* hdr, const T* x0,
                               const T* x1, Forest F, long long* rows, T* times, int max_per_tri, int* mesh_counters,
                               Weld W, Sink sink);
-template <class T, int MODE, class Sink, int LIB, bool STAGED, int BM = 1> cudaError_t prepare_ccd_narrow();
+template <class T, int MODE, class Sink, int LIB, int SRC, int BM = 1> cudaError_t prepare_ccd_narrow();
 
 #ifdef CCC_NARROW_TU
-template <class T, int MODE, class Sink, int LIB, bool STAGED, int BM>
+template <class T, int MODE, class Sink, int LIB, int SRC, int BM>
 __global__ void __launch_bounds__(CCD_BLOCK, CCD_MIN_BLOCKS)
 k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ x0,
              const T* __restrict__ x1, Forest F, long long* __restrict__ rows, T* __restrict__ times, int max_per_tri,
              int* __restrict__ mesh_counters, Weld W, Sink sink) {
     extern __shared__ __align__(16) unsigned char smem[];
     using L = CcdLayout<T, BM * CCD_BLOCK>;
+    constexpr bool STAGED = SRC == SRC_STAGED;
     double* rec = reinterpret_cast<double*>(smem + L::rec);
     T* root_val = reinterpret_cast<T*>(smem + L::root_val);
     int2* items = reinterpret_cast<int2*>(smem + L::items);
@@ -1107,7 +1114,8 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                 bool live = false;
                 if (c < n) {
                     pr = cand[c];
-                    live = !ccd_pair_shares_vertex<T>(x0, pr.x, pr.y);
+                    live = !ccd_pair_shares_vertex<T>(x0, pr.x, pr.y) &&
+                           (SRC != SRC_EXACT || ccd_pair_leaf_overlap<T>(x0, x1, pr.x, pr.y));
                 }
                 const unsigned lb = __ballot_sync(FULL, live);
                 int lbase = 0;
@@ -1342,25 +1350,25 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
 // instantiation and device; prepare_ccd_narrow does it ahead of any stream capture).
 // The flags are atomic because host threads may launch on different streams at once; two
 // first calls may both set the attribute, which is harmless.
-template <class T, int MODE, class Sink, int LIB, bool STAGED, int BM> cudaError_t prepare_ccd_narrow() {
+template <class T, int MODE, class Sink, int LIB, int SRC, int BM> cudaError_t prepare_ccd_narrow() {
     static std::atomic<bool> done[64];
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && done[dev].load(std::memory_order_acquire)) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(k_ccd_narrow<T, MODE, Sink, LIB, STAGED, BM>,
+    cudaError_t e = cudaFuncSetAttribute(k_ccd_narrow<T, MODE, Sink, LIB, SRC, BM>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)CcdLayout<T, BM * CCD_BLOCK>::bytes);
     if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev].store(true, std::memory_order_release);
     return e;
 }
 
-template <class T, int MODE, class Sink, int LIB, bool STAGED, int BM>
+template <class T, int MODE, class Sink, int LIB, int SRC, int BM>
 cudaError_t launch_ccd_narrow(int grid, cudaStream_t s, const int2* cand, int cand_cap, WsHeader* hdr, const T* x0,
                               const T* x1, Forest F, long long* rows, T* times, int max_per_tri, int* mesh_counters,
                               Weld W, Sink sink) {
-    cudaError_t e = prepare_ccd_narrow<T, MODE, Sink, LIB, STAGED, BM>();
+    cudaError_t e = prepare_ccd_narrow<T, MODE, Sink, LIB, SRC, BM>();
     if (e != cudaSuccess) return e;
-    k_ccd_narrow<T, MODE, Sink, LIB, STAGED, BM><<<grid, CCD_BLOCK, CcdLayout<T, BM * CCD_BLOCK>::bytes, s>>>(
+    k_ccd_narrow<T, MODE, Sink, LIB, SRC, BM><<<grid, CCD_BLOCK, CcdLayout<T, BM * CCD_BLOCK>::bytes, s>>>(
         cand, cand_cap, hdr, x0, x1, F, rows, times, max_per_tri, mesh_counters, W, sink);
     return cudaSuccess;
 }

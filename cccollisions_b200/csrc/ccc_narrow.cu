@@ -19,29 +19,28 @@
 namespace ccc {
 
 // the combinations the library launches: (type, mode, sink, math library)
-#define CCC_NARROW_INSTANCE(T, MODE, SINK, LIB, STAGED, BM)                                                         \
-    template cudaError_t launch_ccd_narrow<T, MODE, SINK, LIB, STAGED, BM>(int, cudaStream_t, const int2*, int,        \
+#define CCC_NARROW_INSTANCE(T, MODE, SINK, LIB, SRC, BM)                                                         \
+    template cudaError_t launch_ccd_narrow<T, MODE, SINK, LIB, SRC, BM>(int, cudaStream_t, const int2*, int,        \
                                                                            WsHeader*, const T*, const T*, Forest,      \
                                                                            long long*, T*, int, int*, Weld, SINK);     \
-    template cudaError_t prepare_ccd_narrow<T, MODE, SINK, LIB, STAGED, BM>();
-#define CCC_NARROW_TYPES(MODE, SINK, LIB, STAGED, BM)                                                              \
-    CCC_NARROW_INSTANCE(float, MODE, SINK<float>, LIB, STAGED, BM)                                                  \
-    CCC_NARROW_INSTANCE(double, MODE, SINK<double>, LIB, STAGED, BM)
+    template cudaError_t prepare_ccd_narrow<T, MODE, SINK, LIB, SRC, BM>();
+#define CCC_NARROW_TYPES(MODE, SINK, LIB, SRC, BM)                                                              \
+    CCC_NARROW_INSTANCE(float, MODE, SINK<float>, LIB, SRC, BM)                                                  \
+    CCC_NARROW_INSTANCE(double, MODE, SINK<double>, LIB, SRC, BM)
 // the reference-format operations (pairs from the candidate buffer), batches of 256
-CCC_NARROW_TYPES(CCD_ROWS, CornerSink, LIB_REFERENCE, false, 1)
-CCC_NARROW_TYPES(CCD_ROWS, CornerSink, LIB_PORTABLE, false, 1)
-CCC_NARROW_TYPES(CCD_IMPULSES, CornerSink, LIB_REFERENCE, false, 1)
-CCC_NARROW_TYPES(CCD_IMPULSES, CornerSink, LIB_PORTABLE, false, 1)
-CCC_NARROW_TYPES(CCD_MINCOL, CornerSink, LIB_PORTABLE, false, 1)
-// the resident engine (staged pairs, shared sub-tests), batches of 256 or 512
-CCC_NARROW_TYPES(CCD_ROWS, CornerSink, LIB_REFERENCE, true, 1)
-CCC_NARROW_TYPES(CCD_ROWS, CornerSink, LIB_PORTABLE, true, 1)
-CCC_NARROW_TYPES(CCD_IMPULSES, LoopSink, LIB_REFERENCE, true, 1)
-CCC_NARROW_TYPES(CCD_IMPULSES, LoopSink, LIB_PORTABLE, true, 1)
-CCC_NARROW_TYPES(CCD_ROWS, CornerSink, LIB_REFERENCE, true, 2)
-CCC_NARROW_TYPES(CCD_ROWS, CornerSink, LIB_PORTABLE, true, 2)
-CCC_NARROW_TYPES(CCD_IMPULSES, LoopSink, LIB_REFERENCE, true, 2)
-CCC_NARROW_TYPES(CCD_IMPULSES, LoopSink, LIB_PORTABLE, true, 2)
+CCC_NARROW_TYPES(CCD_ROWS, CornerSink, LIB_REFERENCE, SRC_CANDIDATES, 1)
+CCC_NARROW_TYPES(CCD_ROWS, CornerSink, LIB_PORTABLE, SRC_CANDIDATES, 1)
+CCC_NARROW_TYPES(CCD_IMPULSES, CornerSink, LIB_REFERENCE, SRC_CANDIDATES, 1)
+CCC_NARROW_TYPES(CCD_IMPULSES, CornerSink, LIB_PORTABLE, SRC_CANDIDATES, 1)
+CCC_NARROW_TYPES(CCD_MINCOL, CornerSink, LIB_PORTABLE, SRC_CANDIDATES, 1)
+// the resident engine's collision step (staged pairs, shared sub-tests), batches of 256 or
+// 512, and its impulse loop (candidate buffer, the exact leaf-box test)
+CCC_NARROW_TYPES(CCD_ROWS, CornerSink, LIB_REFERENCE, SRC_STAGED, 1)
+CCC_NARROW_TYPES(CCD_ROWS, CornerSink, LIB_PORTABLE, SRC_STAGED, 1)
+CCC_NARROW_TYPES(CCD_ROWS, CornerSink, LIB_REFERENCE, SRC_STAGED, 2)
+CCC_NARROW_TYPES(CCD_ROWS, CornerSink, LIB_PORTABLE, SRC_STAGED, 2)
+CCC_NARROW_TYPES(CCD_IMPULSES, LoopSink, LIB_REFERENCE, SRC_EXACT, 1)
+CCC_NARROW_TYPES(CCD_IMPULSES, LoopSink, LIB_PORTABLE, SRC_EXACT, 1)
 
 // Element-wise evaluation of the solver's arithmetic building blocks, for tests that compare
 // them bit for bit with the CPU oracle and against CUDA's own elementary functions.

@@ -1,11 +1,13 @@
-"""Repeated sub-tests in the resident engine: each tetrahedron that several triangle pairs
-of a mesh share is solved once and its rows (or contacts) are written for every pair.
+"""Repeated sub-tests in the resident engine's collision step: each tetrahedron that several
+triangle pairs of a mesh share is solved once and its rows are written for every pair.
 
 The meshes here hold every case the corner classes must get right, and each is compared
 with the oracle, which solves every pair's sub-tests on its own: corners at one start
 position that move apart (a cut), +0 and -0 at a shared vertex, coordinates that do not
 come back from their displacement (x0 + (x1 - x0) != x1), edges of three triangles, a
-vertex of more triangles than a class may hold, and triangles with two equal corners.
+vertex of more triangles than a class may hold, and triangles with two equal corners.  The
+impulse loop, which solves every pair's sub-tests and tests the exact leaf boxes of the
+engine's candidates, runs the same cases against the oracle's loop.
 """
 from collections import Counter
 
@@ -200,7 +202,7 @@ def _loop_cases():
     return out
 
 
-def test_shared_sub_tests_in_the_impulse_loop_match_oracle(cuda, oracle):
+def test_edge_case_meshes_in_the_impulse_loop_match_oracle(cuda, oracle):
     from cccollisions_b200 import _native as N
     from cccollisions_b200.engine import Engine
     meshes = _loop_cases()
