@@ -268,7 +268,8 @@ template <class T> int refit(ccc_engine* e, const Tables& t, const int* flags, c
     CCC_LAUNCH("k_engine_refit", s, k_engine_refit_local<T><<<refit_grid(e), REFIT_THREADS, 0, s>>>(
         t.f, e->at<T>(e->L.x0), e->at<T>(e->L.x1), e->at<int>(e->L.leaf_tri), e->at<int>(e->L.lparent),
         e->at<int>(e->L.nparent), e->at<int>(e->L.qcode), e->at<int>(e->L.qleaf), e->at<int2>(e->L.nrange),
-        e->at<QNode>(e->L.qnodes), e->at<int2>(e->L.front), (int)e->tri_cap, flags, e->hdr()));
+        e->at<TNode>(e->L.nodes), e->at<QNode>(e->L.qnodes), e->at<int2>(e->L.front), (int)e->tri_cap, flags,
+        e->hdr()));
     CCC_LAUNCH_CHECK();
     CCC_LAUNCH("k_engine_refit_front", s, k_engine_refit_front<<<num_sms() * 8, 256, 0, s>>>(
         t.f, e->at<int>(e->L.nparent), e->at<int>(e->L.qcode), e->at<QNode>(e->L.qnodes),

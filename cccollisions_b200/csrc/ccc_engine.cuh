@@ -746,106 +746,148 @@ __device__ __forceinline__ float hmax4(float4 v) { return fmaxf(fmaxf(v.x, v.y),
 // climbs; at each binary node the second arrival (the one that finds the node's other
 // subtree done) unions the children and goes on, the first stops.  Two passes:
 //  * pass 1 (k_engine_refit_local): a block takes REFIT_THREADS consecutive leaf positions
-//    and refits every node whose leaf range lies inside them, with arrival counters in
-//    shared memory and block-scope fences; a climb that reaches a node reaching outside the
-//    block stops and hands that arrival to pass 2 through the frontier list;
+//    and refits every node whose leaf range lies inside them, in shared memory, round by
+//    round; an item whose parent reaches outside the block hands that arrival to pass 2
+//    through the frontier list;
 //  * pass 2 (k_engine_refit_front) finishes those climbs with device-scope fences, global
 //    arrival counters and L2 reads.  The global counters only ever grow and the arrival
 //    that finds an odd count is the second one, so they are never cleared (a node refit in
 //    pass 1 leaves its counter alone).  The kernel boundary makes every box written in
 //    pass 1 visible to pass 2.
-// Most nodes lie inside one block's range, so most arrivals cost a shared-memory atomic
-// instead of a device fence and an L2 round trip.  Meshes with MF_DONE set in mflags (when
+// Most nodes lie inside one block's range, so most of the refit is shared-memory work
+// instead of device fences and L2 round trips.  Meshes with MF_DONE set in mflags (when
 // given) are skipped.
 static constexpr int REFIT_THREADS = 256;
 
-template <class T>
-__device__ __forceinline__ void refit_leaf_local(int v, int base, const Forest& F, int M, const T* __restrict__ x0,
-                                                 const T* __restrict__ x1, const int* __restrict__ leaf_tri,
-                                                 const int* __restrict__ lparent, const int* __restrict__ nparent,
-                                                 const int* __restrict__ qcode, const int* __restrict__ qleaf,
-                                                 const int2* __restrict__ nrange, QNode* qnodes, unsigned* scnt,
-                                                 int2* __restrict__ front, int front_cap,
-                                                 const int* __restrict__ mflags, WsHeader* hdr) {
-    const int m = find_mesh(F.voff, M, v, 0);
-    const int vo = __ldg(F.voff + m), po = __ldg(F.poff + m);
-    const int n = __ldg(F.voff + m + 1) - vo;
-    if (n < 2) return;
-    if (mflags && (__ldg(mflags + __ldg(F.sid + m)) & MF_DONE)) return;
-    const int p = v - vo;
-    const int t = __ldg(leaf_tri + po + p);
-    if (t < 0 || t >= n) { atomicOr(&hdr->status, ST_MALFORMED_TREE); return; }
-    const long long slot = (long long)po + t;
-    Box<T> b = merge(tri_box(load_tri(x0, slot)), tri_box(load_tri(x1, slot)));
-    float lo[3], hi[3];
-    box_outward_f32(b, lo, hi);
-    QNode* qn = qnodes + po;
-    const int lq = __ldg(qleaf + po + p);
-    if (lq < 0 || (lq >> 2) >= n - 1) { atomicOr(&hdr->status, ST_MALFORMED_TREE); return; }
-    write_qslot(qn, lq, lo, hi);
-    // the block's leaf positions in this mesh
-    const int blo = base - vo, bhi = base + REFIT_THREADS - 1 - vo;
-    int code = __ldg(lparent + po + p);
-    for (int guard = 0; guard < n; ++guard) {
-        const int node = code >> 1;
-        if (code < 0 || node >= n - 1) { atomicOr(&hdr->status, ST_MALFORMED_TREE); return; }
-        const int2 r = __ldg(nrange + po + node);
-        if (r.x < blo || r.y > bhi) {
-            // the node reaches outside the block: pass 2 takes this arrival
-            const int f = atomicAdd(&hdr->front, 1);
-            if (f < front_cap) front[f] = make_int2(m, code);
-            else atomicOr(&hdr->status, ST_MALFORMED_TREE);
-            return;
-        }
-        __threadfence_block();
-        if (atomicAdd(scnt + (node - blo), 1u) == 0u) return;           // first arrival
-        __threadfence_block();
-        const int qc = __ldg(qcode + po + node);
-        if (qc <= QCODE_ODD) {
-            const int c0 = QCODE_ODD - qc;
-            if ((c0 >> 2) >= n - 1 || (c0 & 3) > 2) { atomicOr(&hdr->status, ST_MALFORMED_TREE); return; }
-            // slots written by threads of this block: plain loads after the block fence
-            const float* f = reinterpret_cast<const float*>(qn + (c0 >> 2));
-            const int sl = c0 & 3;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                lo[c] = fminf(f[4 * c + sl], f[4 * c + sl + 1]);
-                hi[c] = fmaxf(f[12 + 4 * c + sl], f[12 + 4 * c + sl + 1]);
-            }
-        } else {
-            const float4* f = reinterpret_cast<const float4*>(qn + node);
-            lo[0] = hmin4(f[0]);
-            lo[1] = hmin4(f[1]);
-            lo[2] = hmin4(f[2]);
-            hi[0] = hmax4(f[3]);
-            hi[1] = hmax4(f[4]);
-            hi[2] = hmax4(f[5]);
-            if (qc == QCODE_ROOT) return;
-            if (qc < 0 || (qc >> 2) >= n - 1) { atomicOr(&hdr->status, ST_MALFORMED_TREE); return; }
-            write_qslot(qn, qc, lo, hi);
-        }
-        code = __ldg(nparent + po + node);
-        if (code < 0) return;
-    }
-}
-
+// pass 1: a block's leaf positions [base, base + REFIT_THREADS) and the internal nodes of
+// each mesh whose leaf range lies inside them ("local" nodes; a node's index lies in its
+// range, so these are the nodes at the same positions).  The boxes live in shared memory,
+// indexed by position - base: the leaves' from the soups, the local nodes' computed in
+// rounds (a node whose two children were done in earlier rounds takes the union of their
+// boxes; fminf / fmaxf skip NaN, so the order of the unions does not matter).  Then every
+// leaf and every local even-depth node writes its box into its QNode slot, and each whose
+// parent is not local hands that arrival to pass 2 through the frontier list.
 template <class T>
 __global__ void __launch_bounds__(REFIT_THREADS)
 k_engine_refit_local(Forest F, const T* __restrict__ x0, const T* __restrict__ x1, const int* __restrict__ leaf_tri,
                      const int* __restrict__ lparent, const int* __restrict__ nparent,
                      const int* __restrict__ qcode, const int* __restrict__ qleaf, const int2* __restrict__ nrange,
-                     QNode* qnodes, int2* __restrict__ front, int front_cap, const int* __restrict__ mflags,
-                     WsHeader* hdr) {
-    __shared__ unsigned scnt[REFIT_THREADS];
+                     const TNode* __restrict__ nodes, QNode* qnodes, int2* __restrict__ front, int front_cap,
+                     const int* __restrict__ mflags, WsHeader* hdr) {
+    __shared__ float s_llo[3][REFIT_THREADS], s_lhi[3][REFIT_THREADS];    // leaf boxes
+    __shared__ float s_nlo[3][REFIT_THREADS], s_nhi[3][REFIT_THREADS];    // local node boxes
+    __shared__ unsigned short s_done[REFIT_THREADS];    // round a local node was done in (0: not yet)
     const int M = forest_size(F);
     const int total = __ldg(F.voff + M);
+    const int t = threadIdx.x;
     for (int base = blockIdx.x * REFIT_THREADS; base < total; base += gridDim.x * REFIT_THREADS) {
-        scnt[threadIdx.x] = 0u;
+        const int v = base + t;
+        bool live = false, node_local = false;
+        int m = 0, vo = 0, po = 0, n = 0, p = 0, cl = 0, cr = 0;
+        if (v < total) {
+            m = find_mesh(F.voff, M, v, 0);
+            vo = __ldg(F.voff + m);
+            po = __ldg(F.poff + m);
+            n = __ldg(F.voff + m + 1) - vo;
+            p = v - vo;
+            live = n >= 2 && !(mflags && (__ldg(mflags + __ldg(F.sid + m)) & MF_DONE));
+        }
+        const int blo = base - vo, bhi = base + REFIT_THREADS - 1 - vo;     // the block in mesh positions
+        if (live) {
+            // the leaf at position p
+            const int tri = __ldg(leaf_tri + po + p);
+            if (tri < 0 || tri >= n) {
+                atomicOr(&hdr->status, ST_MALFORMED_TREE);
+                live = false;
+            } else {
+                const long long slot = (long long)po + tri;
+                const Box<T> b = merge(tri_box(load_tri(x0, slot)), tri_box(load_tri(x1, slot)));
+                float lo[3], hi[3];
+                box_outward_f32(b, lo, hi);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    s_llo[c][t] = lo[c];
+                    s_lhi[c][t] = hi[c];
+                }
+            }
+            // the internal node at position p, when its range lies inside the block
+            if (live && p < n - 1) {
+                const int2 r = __ldg(nrange + po + p);
+                if (r.x >= blo && r.y <= bhi) {
+                    const int4 d = __ldg(&nodes[po + p].d);
+                    cl = d.x;
+                    cr = d.y;
+                    node_local = (cl < 0 ? ~cl < n : cl < n - 1) && (cr < 0 ? ~cr < n : cr < n - 1);
+                    if (!node_local) atomicOr(&hdr->status, ST_MALFORMED_TREE);
+                }
+            }
+        }
+        s_done[t] = 0;
         __syncthreads();
-        const int v = base + threadIdx.x;
-        if (v < total)
-            refit_leaf_local<T>(v, base, F, M, x0, x1, leaf_tri, lparent, nparent, qcode, qleaf, nrange, qnodes, scnt,
-                                front, front_cap, mflags, hdr);
+        // rounds: children indices (position - base) of a local node lie in the block
+        const int il = node_local ? (cl < 0 ? vo + ~cl : vo + cl) - base : 0;
+        const int ir = node_local ? (cr < 0 ? vo + ~cr : vo + cr) - base : 0;
+        bool pending = node_local;
+#pragma unroll 1
+        for (int round = 1; round <= REFIT_THREADS; ++round) {
+            if (pending) {
+                const bool dl = cl < 0 || (s_done[il] != 0 && s_done[il] < round);
+                const bool dr = cr < 0 || (s_done[ir] != 0 && s_done[ir] < round);
+                if (dl && dr) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const float a0 = cl < 0 ? s_llo[c][il] : s_nlo[c][il], a1 = cl < 0 ? s_lhi[c][il] : s_nhi[c][il];
+                        const float b0 = cr < 0 ? s_llo[c][ir] : s_nlo[c][ir], b1 = cr < 0 ? s_lhi[c][ir] : s_nhi[c][ir];
+                        s_nlo[c][t] = fminf(a0, b0);
+                        s_nhi[c][t] = fmaxf(a1, b1);
+                    }
+                    s_done[t] = (unsigned short)round;
+                    pending = false;
+                }
+            }
+            if (!__syncthreads_or(pending)) break;
+        }
+        if (pending) atomicOr(&hdr->status, ST_MALFORMED_TREE);     // (a cycle: not reached)
+        // slots and the hand-over to pass 2
+        if (live) {
+            QNode* qn = qnodes + po;
+            const int lq = __ldg(qleaf + po + p);
+            if (lq < 0 || (lq >> 2) >= n - 1) {
+                atomicOr(&hdr->status, ST_MALFORMED_TREE);
+            } else {
+                const float lo[3] = {s_llo[0][t], s_llo[1][t], s_llo[2][t]};
+                const float hi[3] = {s_lhi[0][t], s_lhi[1][t], s_lhi[2][t]};
+                write_qslot(qn, lq, lo, hi);
+            }
+            // each item whose parent is not local hands the arrival at the parent to pass 2
+            for (int item = 0; item < 2; ++item) {
+                if (item == 1 && (!node_local || pending)) break;
+                if (item == 1) {
+                    const int qc = __ldg(qcode + po + p);
+                    if (qc >= 0) {
+                        if ((qc >> 2) >= n - 1) {
+                            atomicOr(&hdr->status, ST_MALFORMED_TREE);
+                        } else {
+                            const float lo[3] = {s_nlo[0][t], s_nlo[1][t], s_nlo[2][t]};
+                            const float hi[3] = {s_nhi[0][t], s_nhi[1][t], s_nhi[2][t]};
+                            write_qslot(qn, qc, lo, hi);
+                        }
+                    }
+                }
+                const int code = __ldg((item ? nparent : lparent) + po + p);
+                if (code < 0) continue;                           // the root
+                const int par = code >> 1;
+                if (par >= n - 1) {
+                    atomicOr(&hdr->status, ST_MALFORMED_TREE);
+                    continue;
+                }
+                const int2 r = __ldg(nrange + po + par);
+                if (r.x >= blo && r.y <= bhi) continue;           // a local parent: done here
+                const int f = atomicAdd(&hdr->front, 1);
+                if (f < front_cap) front[f] = make_int2(m, code);
+                else atomicOr(&hdr->status, ST_MALFORMED_TREE);
+            }
+        }
         __syncthreads();
     }
 }
