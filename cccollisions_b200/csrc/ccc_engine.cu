@@ -278,24 +278,25 @@ template <class T> int refit(ccc_engine* e, const Tables& t, const int* flags, c
     return CCC_OK;
 }
 
-template <class T> int traverse(ccc_engine* e, const Tables& t, const int* flags, cudaStream_t s) {
+// vid: the corner classes of the step (pairs sharing a vertex are not emitted), or null
+template <class T> int traverse(ccc_engine* e, const Tables& t, const int* flags, const int4* vid, cudaStream_t s) {
     int g = num_sms() * SHAPES[e->shape].trav;
     if (SHAPES[e->shape].warp)
         CCC_LAUNCH("k_traverse", s, k_traverse_w<<<g, TRAV_THREADS, 0, s>>>(
             e->at<QNode>(e->L.qnodes), e->at<int>(e->L.qleaf), e->at<int>(e->L.leaf_tri), t.f, e->at<int2>(e->L.cand),
-            (int)e->L.cand_cap, e->hdr(), flags));
+            (int)e->L.cand_cap, e->hdr(), flags, vid));
     else if (SHAPES[e->shape].stage == 0)
         CCC_LAUNCH("k_traverse", s, k_traverse_q<0><<<g, TRAV_THREADS, 0, s>>>(
             e->at<QNode>(e->L.qnodes), e->at<int>(e->L.qleaf), e->at<int>(e->L.leaf_tri), t.f, e->at<int2>(e->L.cand),
-            (int)e->L.cand_cap, e->hdr(), flags));
+            (int)e->L.cand_cap, e->hdr(), flags, vid));
     else if (SHAPES[e->shape].stage == 1)
         CCC_LAUNCH("k_traverse", s, k_traverse_q<1><<<g, TRAV_THREADS, 0, s>>>(
             e->at<QNode>(e->L.qnodes), e->at<int>(e->L.qleaf), e->at<int>(e->L.leaf_tri), t.f, e->at<int2>(e->L.cand),
-            (int)e->L.cand_cap, e->hdr(), flags));
+            (int)e->L.cand_cap, e->hdr(), flags, vid));
     else
         CCC_LAUNCH("k_traverse", s, k_traverse_q<2><<<g, TRAV_THREADS, 0, s>>>(
             e->at<QNode>(e->L.qnodes), e->at<int>(e->L.qleaf), e->at<int>(e->L.leaf_tri), t.f, e->at<int2>(e->L.cand),
-            (int)e->L.cand_cap, e->hdr(), flags));
+            (int)e->L.cand_cap, e->hdr(), flags, vid));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }
@@ -356,7 +357,7 @@ template <class T> int ccd_step(ccc_engine* e, cudaStream_t s) {
     if (rc) return rc;
     rc = refit<T>(e, t, nullptr, s);
     if (rc) return rc;
-    rc = traverse<T>(e, t, nullptr, s);
+    rc = traverse<T>(e, t, nullptr, e->at<int4>(e->L.vid4), s);
     if (rc) return rc;
     rc = stage<T>(e, s);
     if (rc) return rc;
@@ -387,7 +388,7 @@ template <class T> int loop_step(ccc_engine* e, int max_iter, cudaStream_t s) {
     // staging cost more than the solves they save)
     int rc = refit<T>(e, t, flags, s);
     if (rc) return rc;
-    rc = traverse<T>(e, t, flags, s);
+    rc = traverse<T>(e, t, flags, nullptr, s);
     if (rc) return rc;
     int g = num_sms() * CCD_MIN_BLOCKS * SHAPES[e->shape].narrow;
     const Weld W{};

@@ -946,7 +946,9 @@ static __global__ void k_engine_refit_front(Forest F, const int* __restrict__ np
 // order rule (a slot is skipped when its rightmost leaf position is not after the query's,
 // so each unordered pair is found once) and emits (min id, max id) in data slots.  Candidates
 // are the pairs whose fp32 boxes overlap, a superset of the exact ones; the continuous
-// narrow phase re-tests every pair's swept sub-boxes exactly.
+// narrow phase re-tests every pair's swept sub-boxes exactly.  With the corner classes
+// (vid, the collision step), pairs whose triangles share a vertex, which the narrow phase
+// drops, are not emitted.
 //
 // SD > 0: the top SD + 1 levels of the mesh of a block's first query (at most 1 + 4 + 16
 // QNodes) are copied into shared memory at every step of the block's loop, breadth first,
@@ -960,7 +962,8 @@ __device__ __forceinline__ int trav_stage_count(int sd) { return sd == 0 ? 0 : (
 template <int SD>
 static __global__ void __launch_bounds__(TRAV_THREADS)
 k_traverse_q(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, const int* __restrict__ leaf_tri,
-             Forest F, int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const int* __restrict__ mflags) {
+             Forest F, int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const int* __restrict__ mflags,
+             const int4* __restrict__ vid) {
     int stack[STACK_DEPTH];          // per-thread, in local memory (L1): shared memory holds the buffer
     __shared__ int2 cbuf[TRAV_BUF][TRAV_THREADS];     // candidate buffer (see flush_candidates)
     __shared__ QNode top[SD > 0 ? (SD == 1 ? 5 : 21) : 1];
@@ -1031,6 +1034,8 @@ k_traverse_q(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, co
                 go = false;
             }
             if (go) {
+                // (the query triangle's corner classes: pairs that share a vertex are not emitted)
+                const int4 VQ = vid ? __ldg(vid + po + qid) : make_int4(0, 0, 0, 0);
                 float qlo[3], qhi[3];
                 {
                     const float* f = reinterpret_cast<const float*>(qn + (lq >> 2));
@@ -1081,6 +1086,7 @@ k_traverse_q(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, co
                         if (!hit) continue;
                         if (ref < 0) {
                             const int cid = aa[s];
+                            if (vid && classes_meet(VQ, __ldg(vid + po + cid))) continue;
                             cbuf[nbuf++][tid] = make_int2(po + min(qid, cid), po + max(qid, cid));
                             if (nbuf == TRAV_BUF) {
                                 cg::coalesced_group grp = cg::coalesced_threads();
@@ -1129,7 +1135,8 @@ k_traverse_q(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, co
 // leaves lie in two meshes walk mesh by mesh.
 static __global__ void __launch_bounds__(TRAV_THREADS)
 k_traverse_w(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, const int* __restrict__ leaf_tri,
-             Forest F, int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const int* __restrict__ mflags) {
+             Forest F, int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const int* __restrict__ mflags,
+             const int4* __restrict__ vid) {
     __shared__ int2 cbuf[TRAV_BUF][TRAV_THREADS];     // candidate buffer (see flush_candidates)
     __shared__ __align__(16) int nbuf_s[TRAV_THREADS / 32][32];    // each warp's staged QNode
     const unsigned FULL = 0xffffffffu;
@@ -1158,6 +1165,7 @@ k_traverse_w(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, co
             const int p = v - vo;
             bool act = mine;
             int qid = 0;
+            int4 VQ = make_int4(0, 0, 0, 0);
             float qlo[3] = {0.f, 0.f, 0.f}, qhi[3] = {0.f, 0.f, 0.f};
             if (act) {
                 qid = __ldg(leaf_tri + po + p);
@@ -1166,6 +1174,7 @@ k_traverse_w(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, co
                     atomicOr(&hdr->status, ST_MALFORMED_TREE);
                     act = false;
                 } else {
+                    if (vid) VQ = __ldg(vid + po + qid);
                     const float* f = reinterpret_cast<const float*>(qn + (lq >> 2));
                     const int sl = lq & 3;
                     qlo[0] = __ldg(f + 0 + sl);
@@ -1207,7 +1216,7 @@ k_traverse_w(const QNode* __restrict__ qnodes, const int* __restrict__ qleaf, co
                     const bool hit = act && p < rightmost && (qlo[0] <= hx[s]) && (qhi[0] >= lx[s]) &&
                                      (qlo[1] <= hy[s]) && (qhi[1] >= ly[s]) && (qlo[2] <= hz[s]) && (qhi[2] >= lz[s]);
                     if (ref < 0) {
-                        if (hit) {
+                        if (hit && !(vid && classes_meet(VQ, __ldg(vid + po + aa[s])))) {
                             const int cid = aa[s];
                             cbuf[nbuf++][tid] = make_int2(po + min(qid, cid), po + max(qid, cid));
                             if (nbuf == TRAV_BUF) {

@@ -216,8 +216,9 @@ class Engine:
         return {"status": int(st.value), "rows": rows, "contacts": con, "iterations": it, "flags": fl}
 
     def counters(self) -> dict:
-        """Synchronises; work counters of the last step: status word, candidate pairs,
-        sub-tests with overlapping sub-boxes, roots in [0, 1] filtered, sub-tests solved
+        """Synchronises; work counters of the last step: status word, candidate pairs (in a
+        collision step, those whose triangles share no vertex), sub-tests with overlapping
+        sub-boxes, roots in [0, 1] filtered, sub-tests solved
         (each repeated sub-test is solved once for all the pairs that have it) and the
         candidate pairs with sub-tests to solve."""
         out = (ctypes.c_int32 * 6)()

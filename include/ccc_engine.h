@@ -140,7 +140,9 @@ int ccc_engine_pack_rows(ccc_engine* e, int64_t* out_rows, void* out_times, int6
                          void* stream);
 
 /* Synchronise the stream and read the work counters of the last step into out[6]: status
- * word, candidate pairs, continuous sub-tests (pair, type) whose swept sub-boxes overlap,
+ * word, candidate pairs (in a collision step, those whose triangles share no vertex: the
+ * others are dropped during the traversal), continuous sub-tests (pair, type) whose swept
+ * sub-boxes overlap,
  * roots in [0, 1] filtered, sub-tests solved, and candidate pairs with sub-tests to solve.
  * A sub-test that several pairs of a mesh have with the same tetrahedron (a vertex-face
  * test over the triangles around the vertex, an edge-edge test over the two triangles of an
