@@ -361,7 +361,7 @@ template <class T> int ccd_step(ccc_engine* e, cudaStream_t s) {
     if (rc) return rc;
     rc = stage<T>(e, s);
     if (rc) return rc;
-    int g = num_sms() * CCD_MIN_BLOCKS * SHAPES[e->shape].narrow;
+    int g = num_sms() * ccd_min_blocks(SRC_STAGED, SHAPES[e->shape].batch) * SHAPES[e->shape].narrow;
     cudaError_t le = cudaSuccess;
     if (SHAPES[e->shape].batch == 2)
         CCC_WITH_LIB(CCC_LAUNCH("k_ccd_narrow", s, le = launch_ccd_narrow<T, CCD_ROWS, CornerSink<T>, LIBV, SRC_STAGED, 2>(

@@ -623,6 +623,12 @@ template <class T> struct CornerSink {
 #endif
 static constexpr int CCD_BLOCK = CCC_CCD_BLOCK;
 static constexpr int CCD_MIN_BLOCKS = CCC_CCD_MIN_BLOCKS;      // resident blocks per SM
+// the engine's staged kernel with batches of 256 needs no more than 64 registers, so four
+// of its blocks fit an SM
+static constexpr int CCD_MIN_BLOCKS_STAGED = 4;
+constexpr int ccd_min_blocks(int src, int bm) {
+    return src == SRC_STAGED && bm == 1 ? CCD_MIN_BLOCKS_STAGED : CCD_MIN_BLOCKS;
+}
 static constexpr int CCD_BATCH = CCC_CCD_BATCH_MULT * CCD_BLOCK;
 static_assert(CCD_BLOCK % 32 == 0 && CCD_BLOCK <= 1024 && 3 * CCD_BATCH <= 65536, "CCD_BLOCK");
 
@@ -1054,7 +1060,7 @@ template <class T, int MODE, class Sink, int LIB, int SRC, int BM = 1> cudaError
 
 #ifdef CCC_NARROW_TU
 template <class T, int MODE, class Sink, int LIB, int SRC, int BM>
-__global__ void __launch_bounds__(CCD_BLOCK, CCD_MIN_BLOCKS)
+__global__ void __launch_bounds__(CCD_BLOCK, ccd_min_blocks(SRC, BM))
 k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ x0,
              const T* __restrict__ x1, Forest F, long long* __restrict__ rows, T* __restrict__ times, int max_per_tri,
              int* __restrict__ mesh_counters, Weld W, Sink sink) {
