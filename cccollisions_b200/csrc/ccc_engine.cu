@@ -201,6 +201,10 @@ struct ccc_engine {
     int* h_stage = nullptr;      // pinned staging of the two tables
     char* h_state = nullptr;     // pinned copy of the state span
     cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+    // second stream of a collision step: the corner classes are rebuilt on it while the
+    // refit runs on the caller's stream (fork and join through the two events)
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int64_t graph_kernels[2] = {0, 0};
     int graph_max_iter = 0;
@@ -353,10 +357,16 @@ template <class T> int stage(ccc_engine* e, cudaStream_t s) {
 template <class T> int ccd_step(ccc_engine* e, cudaStream_t s) {
     if (cudaMemsetAsync(e->base, 0, e->L.zero_bytes, s) != cudaSuccess) return CCC_ERR_CUDA;
     Tables t = e->active();
-    int rc = weld<T>(e, t, s);
+    // the corner classes on the side stream, the refit on s (independent); joined before
+    // the traversal, which drops pairs by class
+    if (cudaEventRecord(e->fork_ev, s) != cudaSuccess || cudaStreamWaitEvent(e->side, e->fork_ev, 0) != cudaSuccess)
+        return CCC_ERR_CUDA;
+    int rc = weld<T>(e, t, e->side);
     if (rc) return rc;
     rc = refit<T>(e, t, nullptr, s);
     if (rc) return rc;
+    if (cudaEventRecord(e->join_ev, e->side) != cudaSuccess || cudaStreamWaitEvent(s, e->join_ev, 0) != cudaSuccess)
+        return CCC_ERR_CUDA;
     rc = traverse<T>(e, t, nullptr, e->at<int4>(e->L.vid4), s);
     if (rc) return rc;
     rc = stage<T>(e, s);
@@ -552,7 +562,10 @@ int ccc_engine_create(int dtype, int64_t tc, int64_t vc, int64_t mc, int64_t max
     bool ok = cudaHostAlloc((void**)&e->h_stage, 2 * words * 4, cudaHostAllocDefault) == cudaSuccess &&
               cudaHostAlloc((void**)&e->h_state, e->L.state_end, cudaHostAllocDefault) == cudaSuccess &&
               cudaEventCreateWithFlags(&e->stage_ev[0], cudaEventDisableTiming) == cudaSuccess &&
-              cudaEventCreateWithFlags(&e->stage_ev[1], cudaEventDisableTiming) == cudaSuccess;
+              cudaEventCreateWithFlags(&e->stage_ev[1], cudaEventDisableTiming) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&e->fork_ev, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&e->join_ev, cudaEventDisableTiming) == cudaSuccess;
     if (ok) ok = dtype ? prepare_kernels<double>() : prepare_kernels<float>();
     if (ok) {
         memset(e->h_stage, 0, 2 * words * 4);
@@ -579,6 +592,12 @@ int ccc_engine_destroy(ccc_engine* e) {
             cudaEventDestroy(e->stage_ev[i]);
         }
     }
+    if (e->side) {
+        cudaStreamSynchronize(e->side);
+        cudaStreamDestroy(e->side);
+    }
+    if (e->fork_ev) cudaEventDestroy(e->fork_ev);
+    if (e->join_ev) cudaEventDestroy(e->join_ev);
     if (e->h_stage) cudaFreeHost(e->h_stage);
     if (e->h_state) cudaFreeHost(e->h_state);
     delete e;
