@@ -94,7 +94,9 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while active."""
+    """nvidia-smi clocks and throttle reasons sampled every 20 ms while active; entering
+    waits (up to 3 s) for the first sample, so that sampling covers the timed region that
+    follows."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -111,10 +113,23 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "20"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (FileNotFoundError, OSError):
             self.proc = None
+        t0 = time.perf_counter()
+        while self.proc is not None and time.perf_counter() - t0 < 3.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.01)
+        self.start_lines = self._lines()
         return self
+
+    def _lines(self):
+        try:
+            with open(self.path) as f:
+                return sum(1 for _ in f)
+        except OSError:
+            return 0
 
     def __exit__(self, *a):
         if self.proc is not None:
@@ -130,7 +145,11 @@ class ClockSampler:
             return out
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        # the samples taken after the timed region began (the first ones came before it)
+        lines = open(self.path).read().splitlines()
+        if len(lines) > getattr(self, "start_lines", 0):
+            lines = lines[getattr(self, "start_lines", 0):]
+        for line in lines:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -413,7 +432,8 @@ def run_ours(args, rank, world, dev):
                          "traffic": (NARROW_DRAM_BYTES_PER_SOLVED * cnt["solved"]) if dname == "k_ccd_narrow"
                          else None,
                          "alg_bytes_per_launch": narrow_bytes, "launch_ms": per_launch},
-            "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+            "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"],
+                       "samples": clocks["samples"]},
             "e2e": {"value": world * total / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "path": "engine.StepPipeline from pinned host memory, rows + times back",

@@ -44,6 +44,8 @@ int g_ntimed = 0;
 cudaEvent_t g_pool[2 * MAX_TIMED];
 int g_pool_init = 0;
 
+bool timing_active() { return g_timing; }
+
 void timing_before(const char* name, cudaStream_t s, int* slot) {
     *slot = -1;
     if (!g_timing || g_ntimed >= MAX_TIMED) return;

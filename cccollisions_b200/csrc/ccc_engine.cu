@@ -358,14 +358,18 @@ template <class T> int ccd_step(ccc_engine* e, cudaStream_t s) {
     if (cudaMemsetAsync(e->base, 0, e->L.zero_bytes, s) != cudaSuccess) return CCC_ERR_CUDA;
     Tables t = e->active();
     // the corner classes on the side stream, the refit on s (independent); joined before
-    // the traversal, which drops pairs by class
-    if (cudaEventRecord(e->fork_ev, s) != cudaSuccess || cudaStreamWaitEvent(e->side, e->fork_ev, 0) != cudaSuccess)
+    // the traversal, which drops pairs by class.  Under per-kernel timing both run on s, so
+    // that each kernel is timed alone.
+    const bool fork = !timing_active();
+    if (fork && (cudaEventRecord(e->fork_ev, s) != cudaSuccess ||
+                 cudaStreamWaitEvent(e->side, e->fork_ev, 0) != cudaSuccess))
         return CCC_ERR_CUDA;
-    int rc = weld<T>(e, t, e->side);
+    int rc = weld<T>(e, t, fork ? e->side : s);
     if (rc) return rc;
     rc = refit<T>(e, t, nullptr, s);
     if (rc) return rc;
-    if (cudaEventRecord(e->join_ev, e->side) != cudaSuccess || cudaStreamWaitEvent(s, e->join_ev, 0) != cudaSuccess)
+    if (fork && (cudaEventRecord(e->join_ev, e->side) != cudaSuccess ||
+                 cudaStreamWaitEvent(s, e->join_ev, 0) != cudaSuccess))
         return CCC_ERR_CUDA;
     rc = traverse<T>(e, t, nullptr, e->at<int4>(e->L.vid4), s);
     if (rc) return rc;

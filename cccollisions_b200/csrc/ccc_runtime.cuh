@@ -20,6 +20,8 @@ extern int g_math_lib;
 
 void timing_before(const char* name, cudaStream_t s, int* slot);
 void timing_after(int slot, cudaStream_t s);
+// per-kernel timing is on: work that would overlap on a second stream runs in order
+bool timing_active();
 int num_sms();
 
 inline int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
