@@ -344,7 +344,7 @@ Weld engine_weld(ccc_engine* e) {
 
 // the sub-tests of every candidate pair, for the narrow phase (k_ccd_stage_*)
 template <class T> int stage(ccc_engine* e, cudaStream_t s) {
-    CCC_LAUNCH("k_ccd_stage_mask", s, k_ccd_stage_mask<T><<<num_sms() * 2, STAGE_THREADS, 0, s>>>(
+    CCC_LAUNCH("k_ccd_stage_mask", s, k_ccd_stage_mask<T><<<num_sms() * 3, STAGE_THREADS, 0, s>>>(
         e->at<int2>(e->L.cand), (int)e->L.cand_cap, e->hdr(), e->at<T>(e->L.x0), e->at<T>(e->L.x1), engine_weld(e),
         e->at<int4>(e->L.live), e->at<int4>(e->L.pending)));
     CCC_LAUNCH_CHECK();

@@ -287,8 +287,10 @@ __device__ __forceinline__ bool ccd_pair_shares_vertex(const T* __restrict__ x0,
 }
 
 // The mask of sub-tests whose swept boxes overlap, for a pair that shares no vertex
-// (REJECT_RIGID: 0 as well for a pair whose sub-tests can have no root, see the end).
-template <class T, bool REJECT_RIGID = true>
+// (REJECT_RIGID: 0 as well for a pair whose sub-tests can have no root, see the end; LEAF: 0
+// as well for a pair whose leaf boxes do not overlap, the test of ccd_pair_leaf_overlap
+// made from the same loads).
+template <class T, bool REJECT_RIGID = true, bool LEAF = false>
 __device__ __forceinline__ uint32_t ccd_pair_subbox_mask(const T* __restrict__ x0, const T* __restrict__ x1,
                                                          long long i, long long j) {
     const T* a0 = x0 + i * 9;
@@ -297,22 +299,32 @@ __device__ __forceinline__ uint32_t ccd_pair_subbox_mask(const T* __restrict__ x
     const T* b1 = x1 + j * 9;
     uint32_t m = 0x7fffu;
     bool rigid = true;          // every vertex moves by the same displacement (on all axes so far)
-#pragma unroll
-    for (int ax = 0; ax < 3; ++ax) {
+    bool leaf = true;           // the leaf boxes overlap (on all axes so far)
+    auto axis = [&](int ax) {
         T alo[3], ahi[3], blo[3], bhi[3], dv[6];
+        T la = T(0), ha = T(0), lb = T(0), hb = T(0);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             T av = __ldg(a0 + 3 * c + ax);
-            dv[c] = __ldg(a1 + 3 * c + ax) - av;
+            const T aw = __ldg(a1 + 3 * c + ax);
+            dv[c] = aw - av;
             T ae = av + dv[c];
             alo[c] = fmn(av, ae);
             ahi[c] = fmx(av, ae);
             T bv = __ldg(b0 + 3 * c + ax);
-            dv[3 + c] = __ldg(b1 + 3 * c + ax) - bv;
+            const T bw = __ldg(b1 + 3 * c + ax);
+            dv[3 + c] = bw - bv;
             T be = bv + dv[3 + c];
             blo[c] = fmn(bv, be);
             bhi[c] = fmx(bv, be);
+            if constexpr (LEAF) {
+                la = c ? fmn(la, fmn(av, aw)) : fmn(av, aw);
+                ha = c ? fmx(ha, fmx(av, aw)) : fmx(av, aw);
+                lb = c ? fmn(lb, fmn(bv, bw)) : fmn(bv, bw);
+                hb = c ? fmx(hb, fmx(bv, bw)) : fmx(bv, bw);
+            }
         }
+        if constexpr (LEAF) leaf = leaf && la <= hb && ha >= lb;
         // finite displacement, and start positions below half the largest finite value so that
         // every difference of two of them is finite too
         const T half_max = sizeof(T) == 4 ? T(1.7e38) : T(8.9e307);
@@ -341,6 +353,15 @@ __device__ __forceinline__ uint32_t ccd_pair_subbox_mask(const T* __restrict__ x
             if (alo[c] <= fbhi && ahi[c] >= fblo) ma |= 1u << (12 + c);
         }
         m &= ma;
+    };
+    // (with the leaf test the axes go one at a time, which keeps the registers of a kernel
+    // with several blocks an SM)
+    if constexpr (LEAF) {
+#pragma unroll 1
+        for (int ax = 0; ax < 3; ++ax) axis(ax);
+    } else {
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) axis(ax);
     }
     // A pair whose six vertices all move by the same finite displacement (a static or rigidly
     // translating piece), with finite position differences, has in every sub-test
@@ -348,7 +369,7 @@ __device__ __forceinline__ uint32_t ccd_pair_subbox_mask(const T* __restrict__ x
     // (every term has such a factor and finite other factors), and the reference drops the
     // root of that linear case (collisions_continuous.cu:531-535), so no sub-test of the pair
     // can give a row or a contact.
-    return REJECT_RIGID && rigid ? 0u : m;
+    return (REJECT_RIGID && rigid) || !leaf ? 0u : m;
 }
 
 // Whether the pair's leaf boxes (each triangle's boxes at x0 and x1 merged,

@@ -908,7 +908,7 @@ __device__ __forceinline__ void stage_emit(WsHeader* hdr, int4* live, int4* pend
 }
 
 template <class T>
-__global__ void __launch_bounds__(STAGE_THREADS, 2)
+__global__ void __launch_bounds__(STAGE_THREADS, 3)
 k_ccd_stage_mask(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T* __restrict__ x0,
                  const T* __restrict__ x1, Weld W, int4* __restrict__ live, int4* __restrict__ pending) {
     __shared__ int2 q_pr[STAGE_WARPS][64];
@@ -950,8 +950,7 @@ k_ccd_stage_mask(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, con
             if (valid) {
                 pr = q_pr[wq][lane];
                 const int4 VA = q_va[wq][lane], VB = q_vb[wq][lane];
-                const unsigned bits = ccd_pair_leaf_overlap<T>(x0, x1, pr.x, pr.y)
-                                          ? ccd_pair_subbox_mask<T, true>(x0, x1, pr.x, pr.y) : 0u;
+                const unsigned bits = ccd_pair_subbox_mask<T, true, true>(x0, x1, pr.x, pr.y);
                 masked += __popc(bits);
                 const unsigned ee = bits & 0x1ffu;
                 int4 TWA = make_int4(0, 0, 0, 0), TWB = TWA, THA = TWA, THB = TWA;
