@@ -432,13 +432,17 @@ template <class T> int build_trees(ccc_engine* e, int64_t ntri, int64_t nb, cuda
     unsigned* bounds = e->at<unsigned>(e->L.bounds);
     CCC_LAUNCH("k_reset_bounds", s, k_reset_bounds<<<grid_for(e->mesh_cap, ITEM_THREADS), ITEM_THREADS, 0, s>>>(t.f, bounds));
     CCC_LAUNCH_CHECK();
-    CCC_LAUNCH("k_mesh_bounds", s, k_mesh_bounds<T><<<item_grid(), ITEM_THREADS, 0, s>>>(t.f, e->at<T>(e->L.x0),
-                                                                                        e->at<T>(e->L.x1), bounds));
-    CCC_LAUNCH_CHECK();
     unsigned long long* keys[2] = {e->at<unsigned long long>(e->L.keys0), e->at<unsigned long long>(e->L.keys1)};
     int* vals[2] = {e->at<int>(e->L.vals0), e->at<int>(e->L.vals1)};
-    CCC_LAUNCH("k_morton", s, k_morton<T><<<item_grid(), ITEM_THREADS, 0, s>>>(t.f, e->at<T>(e->L.x0), e->at<T>(e->L.x1),
-                                                                              bounds, keys[0], vals[0]));
+    // the centroids pass from k_mesh_bounds to k_morton in the second key and value buffers
+    // (8 + 4 bytes an item), which the sort first writes after k_morton
+    float2* cxy = reinterpret_cast<float2*>(keys[1]);
+    float* cz = reinterpret_cast<float*>(vals[1]);
+    CCC_LAUNCH("k_mesh_bounds", s, k_mesh_bounds<T><<<item_grid(), ITEM_THREADS, 0, s>>>(t.f, e->at<T>(e->L.x0),
+                                                                                        e->at<T>(e->L.x1), bounds,
+                                                                                        cxy, cz));
+    CCC_LAUNCH_CHECK();
+    CCC_LAUNCH("k_morton", s, k_morton<<<item_grid(), ITEM_THREADS, 0, s>>>(t.f, cxy, cz, bounds, keys[0], vals[0]));
     CCC_LAUNCH_CHECK();
     int mesh_bits = 0;
     while (((int64_t)1 << mesh_bits) < nb) ++mesh_bits;

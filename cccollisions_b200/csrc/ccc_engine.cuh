@@ -55,50 +55,67 @@ template <class T> __device__ __forceinline__ float3 swept_centroid(const T* x0,
 }
 
 // per-mesh centroid bounds (6 ordered words per slot id: min xyz, max xyz; the caller sets
-// the min words to 0xffffffff and the max words to 0 first)
+// the min words to 0xffffffff and the max words to 0 first), and the centroids of the work
+// items for k_morton (x, y in cxy, z in cz).  Each warp takes BOUNDS_CHUNK consecutive items;
+// a lane keeps running bounds while its mesh stays the same (the items are in mesh order),
+// and the warp's lanes are reduced once a chunk, so that the words see one atomic a chunk
+// rather than one a warp of items.
+static constexpr int BOUNDS_CHUNK = 256;
 template <class T>
 __global__ void k_mesh_bounds(Forest F, const T* __restrict__ x0, const T* __restrict__ x1,
-                              unsigned* __restrict__ bounds) {
+                              unsigned* __restrict__ bounds, float2* __restrict__ cxy, float* __restrict__ cz) {
     const int M = forest_size(F);
     const int total = __ldg(F.voff + M);
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
-        int m = find_mesh(F.voff, M, v, 0);
-        long long slot = (long long)__ldg(F.poff + m) + (v - __ldg(F.voff + m));
-        float3 c = swept_centroid(x0, x1, slot);
-        float lo[3] = {c.x, c.y, c.z}, hi[3] = {c.x, c.y, c.z};
-        cg::coalesced_group act = cg::coalesced_threads();
-        if (act.size() == 32 && __all_sync(0xffffffffu, m == __shfl_sync(0xffffffffu, m, 0))) {
-            // whole warp in one mesh: butterfly reduction, one atomic per word
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+    auto flush = [&](int m, const float* lo, const float* hi) {
+        unsigned* b = bounds + 6 * __ldg(F.sid + m);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            atomicMin(b + d, f2ord(lo[d]));
+            atomicMax(b + 3 + d, f2ord(hi[d]));
+        }
+    };
+    for (long long base = (long long)((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * BOUNDS_CHUNK; base < total;
+         base += nwarps * BOUNDS_CHUNK) {
+        int cm = -1;                         // the mesh of this lane's running bounds
+        float lo[3] = {0.f, 0.f, 0.f}, hi[3] = {0.f, 0.f, 0.f};
+        for (int r = 0; r < BOUNDS_CHUNK / 32; ++r) {
+            const long long v = base + r * 32 + lane;
+            if (v >= total) break;
+            const int m = find_mesh(F.voff, M, v, 0);
+            const float3 c = swept_centroid(x0, x1, (long long)__ldg(F.poff + m) + (v - __ldg(F.voff + m)));
+            cxy[v] = make_float2(c.x, c.y);
+            cz[v] = c.z;
+            const float cc[3] = {c.x, c.y, c.z};
+            if (m != cm) {
+                if (cm >= 0) flush(cm, lo, hi);
+                cm = m;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) lo[d] = hi[d] = cc[d];
+            } else {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    lo[d] = fminf(lo[d], cc[d]);
+                    hi[d] = fmaxf(hi[d], cc[d]);
+                }
+            }
+        }
+        // (every lane takes part in the shuffle: a lane past the end has cm < 0)
+        const int m0 = __shfl_sync(FULL, cm, 0);
+        if (__all_sync(FULL, cm >= 0 && cm == m0)) {
+            // the whole warp in one mesh: butterfly reduction, one atomic per word
 #pragma unroll
             for (int o = 16; o >= 1; o >>= 1)
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
-                    lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
-                    hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+                    lo[d] = fminf(lo[d], __shfl_xor_sync(FULL, lo[d], o));
+                    hi[d] = fmaxf(hi[d], __shfl_xor_sync(FULL, hi[d], o));
                 }
-            if ((threadIdx.x & 31) == 0) {
-                unsigned* b = bounds + 6 * __ldg(F.sid + m);
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    atomicMin(b + d, f2ord(lo[d]));
-                    atomicMax(b + 3 + d, f2ord(hi[d]));
-                }
-            }
-            continue;
-        }
-        cg::coalesced_group grp = cg::labeled_partition(act, m);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            lo[d] = cg::reduce(grp, lo[d], cg::less<float>());
-            hi[d] = cg::reduce(grp, hi[d], cg::greater<float>());
-        }
-        if (grp.thread_rank() == 0) {
-            unsigned* b = bounds + 6 * __ldg(F.sid + m);
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                atomicMin(b + d, f2ord(lo[d]));
-                atomicMax(b + 3 + d, f2ord(hi[d]));
-            }
+            if (lane == 0) flush(cm, lo, hi);
+        } else if (cm >= 0) {
+            flush(cm, lo, hi);
         }
     }
 }
@@ -120,9 +137,9 @@ __device__ __forceinline__ unsigned quantize1024(float c, float lo, float hi) {
     return (unsigned)q;
 }
 
-// sort keys (mesh index << 30 | Morton code) and values (mesh-local triangle id)
-template <class T>
-__global__ void k_morton(Forest F, const T* __restrict__ x0, const T* __restrict__ x1,
+// sort keys (mesh index << 30 | Morton code) and values (mesh-local triangle id), from the
+// centroids that k_mesh_bounds left
+static __global__ void k_morton(Forest F, const float2* __restrict__ cxy, const float* __restrict__ cz,
                          const unsigned* __restrict__ bounds, unsigned long long* __restrict__ keys,
                          int* __restrict__ vals) {
     const int M = forest_size(F);
@@ -130,7 +147,8 @@ __global__ void k_morton(Forest F, const T* __restrict__ x0, const T* __restrict
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
         int m = find_mesh(F.voff, M, v, 0);
         int local = v - __ldg(F.voff + m);
-        float3 c = swept_centroid(x0, x1, (long long)__ldg(F.poff + m) + local);
+        const float2 cv = cxy[v];
+        const float3 c = make_float3(cv.x, cv.y, cz[v]);
         const unsigned* b = bounds + 6 * __ldg(F.sid + m);
         unsigned qx = quantize1024(c.x, ord2f(b[0]), ord2f(b[3]));
         unsigned qy = quantize1024(c.y, ord2f(b[1]), ord2f(b[4]));
