@@ -99,7 +99,7 @@ EngineLayout engine_layout(int64_t tsz, int64_t tc, int64_t vc, int64_t mc, int6
     L.vals0 = take(tc * 4);
     L.vals1 = take(tc * 4);
     L.hist_len = 256 * ((tc + SORT_TILE - 1) / SORT_TILE);
-    L.hist = take((L.hist_len + L.hist_len / SCAN_CHUNK + 1) * 4);    // counts, then chunk totals
+    L.hist = take((L.hist_len + 256) * 4);    // tile counts, then the digits' totals
     L.verts0 = take(vc * 3 * tsz);
     L.verts1 = take(vc * 3 * tsz);
     L.vel = take(vc * 3 * tsz);
@@ -455,17 +455,12 @@ template <class T> int build_trees(ccc_engine* e, int64_t ntri, int64_t nb, cuda
         int shift = 8 * p;
         CCC_LAUNCH("k_radix_hist", s, k_radix_hist<<<nblk, SORT_THREADS, 0, s>>>(keys[cur], n, shift, hist, nblk));
         CCC_LAUNCH_CHECK();
-        int len = 256 * nblk;
-        int nchunk = (len + SCAN_CHUNK - 1) / SCAN_CHUNK;
-        int* part = hist + e->L.hist_len;
-        CCC_LAUNCH("k_scan_chunks", s, k_scan_chunks<<<nchunk, SCAN_THREADS, 0, s>>>(hist, len, part));
-        CCC_LAUNCH_CHECK();
-        CCC_LAUNCH("k_exclusive_scan", s, k_exclusive_scan<<<1, 1024, 0, s>>>(part, nchunk));
-        CCC_LAUNCH_CHECK();
-        CCC_LAUNCH("k_scan_add", s, k_scan_add<<<grid_for(len, 256), 256, 0, s>>>(hist, len, part));
+        int* rowtot = hist + e->L.hist_len;
+        CCC_LAUNCH("k_radix_rowscan", s, k_radix_rowscan<<<256, SORT_THREADS, 0, s>>>(hist, nblk, rowtot));
         CCC_LAUNCH_CHECK();
         CCC_LAUNCH("k_radix_scatter", s, k_radix_scatter<<<nblk, SORT_THREADS, 0, s>>>(keys[cur], vals[cur], keys[1 - cur],
-                                                                                   vals[1 - cur], n, shift, hist, nblk));
+                                                                                   vals[1 - cur], n, shift, hist,
+                                                                                   rowtot, nblk));
         CCC_LAUNCH_CHECK();
         cur = 1 - cur;
     }

@@ -179,90 +179,70 @@ k_radix_hist(const unsigned long long* __restrict__ keys, int n, int shift, int*
     counts[(long long)threadIdx.x * nblk + blockIdx.x] = h[threadIdx.x];
 }
 
-// Exclusive prefix sum in three passes: each block scans SCAN_CHUNK elements and writes its
-// total, one block scans the totals, and the totals' prefixes are added back.
-static constexpr int SCAN_THREADS = 256;
-static constexpr int SCAN_ITEMS = 8;
-static constexpr int SCAN_CHUNK = SCAN_THREADS * SCAN_ITEMS;
-
-static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_chunks(int* __restrict__ a, int len, int* __restrict__ part) {
-    __shared__ int wsum[SCAN_THREADS / 32];
-    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-    const long long base = (long long)blockIdx.x * SCAN_CHUNK + (long long)t * SCAN_ITEMS;
-    int v[SCAN_ITEMS];
-    int sum = 0;
-#pragma unroll
-    for (int i = 0; i < SCAN_ITEMS; ++i) {
-        v[i] = base + i < len ? a[base + i] : 0;
-        sum += v[i];
-    }
-    int incl = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-    }
+// exclusive prefix of v over the SORT_THREADS threads of the block, with the block's sum in
+// *total (wsum: SORT_THREADS / 32 + 1 ints of shared memory, free again on return)
+__device__ __forceinline__ int sort_block_exclusive_scan(int v, int* wsum, int* total) {
+    constexpr int WARPS = SORT_THREADS / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int incl = warp_inclusive_scan(v, lane);
     if (lane == 31) wsum[w] = incl;
     __syncthreads();
-    if (t == 0) {
-        int run = 0;
-        for (int i = 0; i < SCAN_THREADS / 32; ++i) {
-            int c = wsum[i];
-            wsum[i] = run;
-            run += c;
-        }
-        part[blockIdx.x] = run;
+    if (w == 0) {
+        const int x = lane < WARPS ? wsum[lane] : 0;
+        const int sc = warp_inclusive_scan(x, lane);
+        if (lane < WARPS) wsum[lane] = sc - x;
+        if (lane == 31) wsum[WARPS] = sc;
     }
     __syncthreads();
-    int run = wsum[w] + incl - sum;
+    const int r = wsum[w] + incl - v;
+    *total = wsum[WARPS];
+    __syncthreads();
+    return r;
+}
+
+// One block a digit d: row d of counts (the tiles' counts of digit d, in tile order) becomes
+// its exclusive prefix, in place, and rowtot[d] the row's sum.  k_radix_scatter adds the
+// prefix of the row sums (the keys of the smaller digits) itself.
+static constexpr int ROWSCAN_ITEMS = 4;
+static __global__ void __launch_bounds__(SORT_THREADS)
+k_radix_rowscan(int* __restrict__ counts, int nblk, int* __restrict__ rowtot) {
+    __shared__ int wsum[SORT_THREADS / 32 + 1];
+    int* row = counts + (long long)blockIdx.x * nblk;
+    int carry = 0;                                   // (the same in every thread)
+    for (int base = 0; base < nblk; base += SORT_THREADS * ROWSCAN_ITEMS) {
+        const int at = base + threadIdx.x * ROWSCAN_ITEMS;
+        int v[ROWSCAN_ITEMS], sum = 0;
 #pragma unroll
-    for (int i = 0; i < SCAN_ITEMS; ++i) {
-        if (base + i < len) a[base + i] = run;
-        run += v[i];
+        for (int i = 0; i < ROWSCAN_ITEMS; ++i) {
+            v[i] = at + i < nblk ? row[at + i] : 0;
+            sum += v[i];
+        }
+        int total;
+        int run = carry + sort_block_exclusive_scan(sum, wsum, &total);
+#pragma unroll
+        for (int i = 0; i < ROWSCAN_ITEMS; ++i) {
+            if (at + i < nblk) row[at + i] = run;
+            run += v[i];
+        }
+        carry += total;
     }
+    if (threadIdx.x == 0) rowtot[blockIdx.x] = carry;
 }
 
-static __global__ void k_scan_add(int* __restrict__ a, int len, const int* __restrict__ part) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < len) a[i] += part[i / SCAN_CHUNK];
-}
-
-// exclusive prefix sum of len ints in place, one block of 1024 threads (short arrays)
-static __global__ void __launch_bounds__(1024) k_exclusive_scan(int* __restrict__ a, int len) {
-    __shared__ int part[1024];
-    const int t = threadIdx.x;
-    const int chunk = (len + 1023) / 1024;
-    const long long lo = (long long)t * chunk;
-    const long long hi = min((long long)len, lo + chunk);
-    int sum = 0;
-    for (long long i = lo; i < hi; ++i) sum += a[i];
-    part[t] = sum;
-    __syncthreads();
-    for (int o = 1; o < 1024; o <<= 1) {
-        int v = t >= o ? part[t - o] : 0;
-        __syncthreads();
-        part[t] += v;
-        __syncthreads();
-    }
-    int run = part[t] - sum;
-    for (long long i = lo; i < hi; ++i) {
-        int c = a[i];
-        a[i] = run;
-        run += c;
-    }
-}
-
-// stable scatter: keys of tile b with digit d go to offs[d * nblk + b] onwards, in input order
+// stable scatter: keys of tile b with digit d go to (the keys of the digits below d) +
+// offs[d * nblk + b] onwards, in input order; offs and rowtot from k_radix_rowscan
 static __global__ void __launch_bounds__(SORT_THREADS)
 k_radix_scatter(const unsigned long long* __restrict__ kin, const int* __restrict__ vin,
                 unsigned long long* __restrict__ kout, int* __restrict__ vout, int n, int shift,
-                const int* __restrict__ offs, int nblk) {
+                const int* __restrict__ offs, const int* __restrict__ rowtot, int nblk) {
     constexpr int WARPS = SORT_THREADS / 32;
     __shared__ int whist[WARPS][256];
     __shared__ int base[256];
     __shared__ int round_total[256];
+    __shared__ int wsum[WARPS + 1];
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-    base[t] = offs[(long long)t * nblk + blockIdx.x];
+    int all;
+    base[t] = sort_block_exclusive_scan(rowtot[t], wsum, &all) + offs[(long long)t * nblk + blockIdx.x];
     const unsigned lt = (1u << lane) - 1u;
     for (int r = 0; r < SORT_ROUNDS; ++r) {
         long long i = (long long)blockIdx.x * SORT_TILE + r * SORT_THREADS + t;
