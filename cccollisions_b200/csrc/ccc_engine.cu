@@ -54,7 +54,7 @@ struct EngineLayout {
     int64_t rows, times, cand;
     int64_t keys0, keys1, vals0, vals1, hist;
     int64_t verts0, verts1, vel, acc;
-    int64_t wtab, vidc, wcnt, fan_end, fan, vid4, twin4, third4, pending, live, end;
+    int64_t wtab, vidc, wcnt, fan_end, fan, fan_tmp, vid4, twin4, third4, pending, live, end;
     int64_t zero_bytes, hist_len, cand_cap;
 };
 
@@ -111,6 +111,7 @@ EngineLayout engine_layout(int64_t tsz, int64_t tc, int64_t vc, int64_t mc, int6
     L.wcnt = take(tc * 4 * 4);
     L.fan_end = take(tc * 4 * 4);
     L.fan = take(tc * 3 * 16);
+    L.fan_tmp = take(tc * 3 * 16);      // the member list in order of arrival
     L.vid4 = take(tc * 16);
     L.twin4 = take(tc * 16);
     L.third4 = take(tc * 16);
@@ -325,9 +326,10 @@ template <class T> int weld(ccc_engine* e, const Tables& t, cudaStream_t s) {
         t.f, vidc, cnt, fan_start, fan_end, e->hdr()));
     CCC_LAUNCH_CHECK();
     CCC_LAUNCH("k_weld_fill", s, k_weld_fill<<<item_grid(), ITEM_THREADS, 0, s>>>(
-        t.f, vidc, fan_start, fan_end, e->at<int4>(L.fan)));
+        t.f, vidc, fan_start, fan_end, e->at<int4>(L.fan_tmp)));
     CCC_LAUNCH_CHECK();
-    CCC_LAUNCH("k_weld_sort", s, k_weld_sort<<<item_grid(), ITEM_THREADS, 0, s>>>(t.f, vidc, cnt, fan_end, e->at<int4>(L.fan)));
+    CCC_LAUNCH("k_weld_rank", s, k_weld_rank<<<item_grid(), ITEM_THREADS, 0, s>>>(
+        t.f, vidc, fan_start, cnt, e->at<int4>(L.fan_tmp), e->at<int4>(L.fan)));
     CCC_LAUNCH_CHECK();
     CCC_LAUNCH("k_weld_tri", s, k_weld_tri<<<item_grid(), ITEM_THREADS, 0, s>>>(
         t.f, vidc, cnt, fan_start, e->at<int4>(L.fan), e->at<int4>(L.vid4), e->at<int4>(L.twin4),

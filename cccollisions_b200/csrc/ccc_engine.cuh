@@ -465,8 +465,8 @@ static __global__ void k_qtree_slots(Forest F, const TNode* __restrict__ nodes, 
 //    of either position or whose coordinates do not come back from their displacement
 //    (x0 + (x1 - x0) != x1);
 //  * k_weld_alloc: each class's range of the member list (a block-wide scan and one atomic
-//    per block), k_weld_fill: the members with their triangles' classes, k_weld_sort: each
-//    class's members in ascending corner id;
+//    per block), k_weld_fill: the members with their triangles' classes, in order of
+//    arrival, k_weld_rank: each class's members in ascending corner id;
 //  * k_weld_tri: each triangle's classes, named by their first entry in the member list,
 //    with CLS_NODEDUP also for classes of more than WELD_FANCAP corners and the three class
 //    sizes, and the twin of each edge with the class of the twin's third corner.
@@ -621,29 +621,25 @@ static __global__ void k_weld_fill(Forest F, const int* __restrict__ vidc, const
 }
 
 // each class's members in ascending corner id (classes of at most WELD_FANCAP corners; the
-// larger ones are not shared)
-static __global__ void k_weld_sort(Forest F, const int* __restrict__ vidc, const int* __restrict__ cnt,
-                                   const int* __restrict__ fan_end, int4* fan) {
+// larger ones, whose order no kernel reads, keep their places): k_weld_fill's entries (tmp)
+// go to the place of their rank in their class, one thread an entry
+static __global__ void k_weld_rank(Forest F, const int* __restrict__ vidc, const int* __restrict__ fan_start,
+                                   const int* __restrict__ cnt, const int4* __restrict__ tmp, int4* __restrict__ fan) {
     const int M = forest_size(F);
-    const int total = __ldg(F.voff + M);
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
-        const long long slot = weld_item(F, M, v).slot;
-        for (int c = 0; c < 3; ++c) {
-            const int id = (int)(4 * slot + c);
-            if (__ldg(vidc + id) != id) continue;
-            const int n = __ldg(cnt + id) & CLS_MASK;
-            if (n < 2 || n > WELD_FANCAP) continue;
-            int4* f = fan + (__ldg(fan_end + id) - n);
-            for (int i = 1; i < n; ++i) {
-                const int4 x = f[i];
-                int j = i - 1;
-                while (j >= 0 && f[j].x > x.x) {
-                    f[j + 1] = f[j];
-                    --j;
-                }
-                f[j + 1] = x;
-            }
+    const long long entries = 3LL * __ldg(F.voff + M);       // every corner is in one class
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < entries;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int4 en = tmp[e];
+        const int rep = __ldg(vidc + en.x);
+        const int n = __ldg(cnt + rep) & CLS_MASK;
+        long long at = e;
+        if (n >= 2 && n <= WELD_FANCAP) {
+            const int s0 = __ldg(fan_start + rep);
+            int rank = 0;
+            for (int j = 0; j < n; ++j) rank += __ldg(&tmp[s0 + j].x) < en.x;
+            at = s0 + rank;
         }
+        fan[at] = en;
     }
 }
 
