@@ -14,6 +14,7 @@
 
 #include <cooperative_groups.h>
 #include <cooperative_groups/reduce.h>
+#include <cooperative_groups/scan.h>
 #include "ccc_geom.cuh"
 
 namespace cg = cooperative_groups;
@@ -1258,7 +1259,8 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                 // run on full warps rather than on the few lanes that passed
                 unsigned short* pb = pbuf + warp * 64;
                 int np = 0;                        // buffered roots of this warp (warp-uniform)
-                auto emit = [&](int j) {
+                // (mask: the lanes that call it together)
+                auto emit = [&](int j, unsigned mask) {
                     const int2 it = items[(head + root_rec[j]) % Q];
                     const int qx = it.x & SLOT_MASK, qy = it.y & SLOT_MASK, k = (it.y >> 28) & 15;
                     const T tv = root_val[j];
@@ -1277,7 +1279,27 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                     if constexpr (STAGED) {
                         int ma[WELD_FANCAP], mb[WELD_FANCAP], mk[WELD_FANCAP];
                         const int nm = weld_list(W, qx, qy, k, (it.x >> 28) & 1, ma, mb, mk);
-                        for (int i = 0; i < nm; ++i) row(ma[i], mb[i], mk[i]);
+                        // the rows of all the lanes in one mesh are reserved with one atomic,
+                        // each lane's from its prefix of the row counts
+                        __syncwarp(mask);
+                        cg::coalesced_group g = cg::labeled_partition(cg::coalesced_threads(), R.m);
+                        const int before = cg::exclusive_scan(g, nm);
+                        const int all = cg::reduce(g, nm, cg::plus<int>());
+                        int base = 0;
+                        if (g.thread_rank() == 0) base = atomicAdd(mesh_counters + __ldg(F.sid + R.m), all);
+                        base = g.shfl(base, 0) + before;
+                        for (int i = 0; i < nm; ++i) {
+                            const long long r = (long long)base + i;
+                            if (r >= R.cap) {
+                                atomicOr(&hdr->status, ST_OUT_OVERFLOW);
+                                break;
+                            }
+                            const long long o = (long long)R.po * max_per_tri + r;
+                            rows[o * 3 + 0] = ma[i] - R.po;
+                            rows[o * 3 + 1] = mb[i] - R.po;
+                            rows[o * 3 + 2] = mk[i];
+                            times[o] = tv;
+                        }
                     } else {
                         row(qx, qy, k);
                     }
@@ -1298,7 +1320,7 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                     np += __popc(pm);
                     if (np >= 32) {
                         __syncwarp();
-                        emit(pb[lane]);
+                        emit(pb[lane], FULL);
                         __syncwarp();
                         if (lane < np - 32) pb[lane] = pb[32 + lane];
                         __syncwarp();
@@ -1306,7 +1328,7 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                     }
                 }
                 __syncwarp();
-                if (lane < np) emit(pb[lane]);
+                if (lane < np) emit(pb[lane], (1u << np) - 1u);     // (np < 32 here)
             } else {
                 for (int jj = tid; jj < nroots; jj += CCD_BLOCK) {
                     const int j = jj < nee ? jj : 3 * NB - 1 - (jj - nee);
