@@ -1280,14 +1280,23 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                         int ma[WELD_FANCAP], mb[WELD_FANCAP], mk[WELD_FANCAP];
                         const int nm = weld_list(W, qx, qy, k, (it.x >> 28) & 1, ma, mb, mk);
                         // the rows of all the lanes in one mesh are reserved with one atomic,
-                        // each lane's from its prefix of the row counts
+                        // each lane's from its prefix of the row counts (a whole warp in one
+                        // mesh, the usual case, with plain warp scans)
                         __syncwarp(mask);
-                        cg::coalesced_group g = cg::labeled_partition(cg::coalesced_threads(), R.m);
-                        const int before = cg::exclusive_scan(g, nm);
-                        const int all = cg::reduce(g, nm, cg::plus<int>());
                         int base = 0;
-                        if (g.thread_rank() == 0) base = atomicAdd(mesh_counters + __ldg(F.sid + R.m), all);
-                        base = g.shfl(base, 0) + before;
+                        const bool one_mesh =
+                            mask == FULL && __all_sync(FULL, R.m == __shfl_sync(FULL, R.m, 0));
+                        if (one_mesh) {
+                            const int incl = warp_inclusive_scan(nm, lane);
+                            if (lane == 31) base = atomicAdd(mesh_counters + __ldg(F.sid + R.m), incl);
+                            base = __shfl_sync(FULL, base, 31) + incl - nm;
+                        } else {
+                            cg::coalesced_group g = cg::labeled_partition(cg::coalesced_threads(), R.m);
+                            const int before = cg::exclusive_scan(g, nm);
+                            const int all = cg::reduce(g, nm, cg::plus<int>());
+                            if (g.thread_rank() == 0) base = atomicAdd(mesh_counters + __ldg(F.sid + R.m), all);
+                            base = g.shfl(base, 0) + before;
+                        }
                         for (int i = 0; i < nm; ++i) {
                             const long long r = (long long)base + i;
                             if (r >= R.cap) {
