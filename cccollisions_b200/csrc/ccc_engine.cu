@@ -340,8 +340,9 @@ template <class T> int weld(ccc_engine* e, const Tables& t, cudaStream_t s) {
 
 Weld engine_weld(ccc_engine* e) {
     const EngineLayout& L = e->L;
+    // (the records for k_ccd_expand take the pending list's space, free once staging ends)
     return Weld{e->at<int4>(L.vid4), e->at<int4>(L.fan), e->at<int4>(L.twin4), e->at<int4>(L.third4),
-                e->at<int4>(L.live)};
+                e->at<int4>(L.live), e->at<int4>(L.pending), (int)L.cand_cap};
 }
 
 // the sub-tests of every candidate pair, for the narrow phase (k_ccd_stage_*)
@@ -390,6 +391,10 @@ template <class T> int ccd_step(ccc_engine* e, cudaStream_t s) {
             e->at<long long>(e->L.rows), e->at<T>(e->L.times), (int)e->maxcol, e->at<int>(e->L.mesh_cnt),
             engine_weld(e), CornerSink<T>{})));
     if (le != cudaSuccess) return CCC_ERR_CUDA;
+    CCC_LAUNCH_CHECK();
+    CCC_LAUNCH("k_ccd_expand", s, k_ccd_expand<T><<<num_sms() * 8, EXPAND_THREADS, 0, s>>>(
+        e->hdr(), engine_weld(e), t.f, e->at<long long>(e->L.rows), e->at<T>(e->L.times), (int)e->maxcol,
+        e->at<int>(e->L.mesh_cnt)));
     CCC_LAUNCH_CHECK();
     return CCC_OK;
 }

@@ -45,7 +45,8 @@ struct WsHeader {
     int fan_cursor;    // engine corner classes: member list slots handed out
     int live_count;    // engine staging: pairs with sub-tests to solve (Weld.live)
     int pending_count; // engine staging: pairs left with vertex-face sub-tests to place
-    int pad[7];
+    int expand_count;  // engine narrow phase: records for k_ccd_expand (Weld.expand)
+    int pad[6];
 };
 
 struct __align__(16) TNode {
@@ -707,6 +708,11 @@ struct Weld {
     const int4* live;      // the pairs with sub-tests to solve (hdr->live_count of them, from
                            // k_ccd_stage_*): slots i, j and the sub-tests it solves (bits
                            // 0..14) with those that stand for their repeats (bits 15..29)
+    int4* expand;          // the shared sub-tests whose roots passed the filter, for
+                           // k_ccd_expand (hdr->expand_count, at most expand_cap): owner slots
+                           // i, j | type << 28, the root as a double (low, high words); null:
+                           // k_ccd_narrow writes every pair's rows itself
+    int expand_cap;
 };
 
 __device__ __forceinline__ int int4_at(int4 v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); }
@@ -847,6 +853,28 @@ __device__ __forceinline__ int warp_inclusive_scan(int v, int lane) {
         if (lane >= o) v += y;
     }
     return v;
+}
+
+// Row reservation for the lanes of mask, which call it together: each lane's nm rows in the
+// region of its mesh m, with one atomic per mesh among them; returns the lane's first row
+// (its prefix of the counts of the lanes in its mesh).  A whole warp in one mesh, the usual
+// case, takes plain warp scans.
+__device__ __forceinline__ int reserve_rows(int* mesh_counters, const Forest& F, int m, int nm, unsigned mask) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    __syncwarp(mask);
+    if (mask == FULL && __all_sync(FULL, m == __shfl_sync(FULL, m, 0))) {
+        const int incl = warp_inclusive_scan(nm, lane);
+        int base = 0;
+        if (lane == 31) base = atomicAdd(mesh_counters + __ldg(F.sid + m), incl);
+        return __shfl_sync(FULL, base, 31) + incl - nm;
+    }
+    cg::coalesced_group g = cg::labeled_partition(cg::coalesced_threads(), m);
+    const int before = cg::exclusive_scan(g, nm);
+    const int all = cg::reduce(g, nm, cg::plus<int>());
+    int base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(mesh_counters + __ldg(F.sid + m), all);
+    return g.shfl(base, 0) + before;
 }
 
 // Staging of the resident engine's candidate pairs for k_ccd_narrow: the list Weld.live of
@@ -1277,26 +1305,32 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                         }
                     };
                     if constexpr (STAGED) {
-                        int ma[WELD_FANCAP], mb[WELD_FANCAP], mk[WELD_FANCAP];
-                        const int nm = weld_list(W, qx, qy, k, (it.x >> 28) & 1, ma, mb, mk);
-                        // the rows of all the lanes in one mesh are reserved with one atomic,
-                        // each lane's from its prefix of the row counts (a whole warp in one
-                        // mesh, the usual case, with plain warp scans)
-                        __syncwarp(mask);
-                        int base = 0;
-                        const bool one_mesh =
-                            mask == FULL && __all_sync(FULL, R.m == __shfl_sync(FULL, R.m, 0));
-                        if (one_mesh) {
-                            const int incl = warp_inclusive_scan(nm, lane);
-                            if (lane == 31) base = atomicAdd(mesh_counters + __ldg(F.sid + R.m), incl);
-                            base = __shfl_sync(FULL, base, 31) + incl - nm;
-                        } else {
-                            cg::coalesced_group g = cg::labeled_partition(cg::coalesced_threads(), R.m);
-                            const int before = cg::exclusive_scan(g, nm);
-                            const int all = cg::reduce(g, nm, cg::plus<int>());
-                            if (g.thread_rank() == 0) base = atomicAdd(mesh_counters + __ldg(F.sid + R.m), all);
-                            base = g.shfl(base, 0) + before;
+                        // a shared sub-test leaves a record for k_ccd_expand, which writes the
+                        // other pairs' rows (the owner's is written here); with the record
+                        // list full, all of them are written here
+                        const bool sh = (it.x >> 28) & 1;
+                        const unsigned shm = __ballot_sync(mask, sh);
+                        int at = -1;
+                        if (shm && W.expand) {
+                            const int leader = __ffs(shm) - 1;
+                            int b0 = 0;
+                            if (lane == leader) b0 = atomicAdd(&hdr->expand_count, __popc(shm));
+                            b0 = __shfl_sync(mask, b0, leader);
+                            if (sh && b0 + __popc(shm & lt) < W.expand_cap) at = b0 + __popc(shm & lt);
                         }
+                        int ma[WELD_FANCAP], mb[WELD_FANCAP], mk[WELD_FANCAP];
+                        int nm = 1;
+                        if (at >= 0) {
+                            const double tw = (double)tv;
+                            W.expand[at] = make_int4(qx, qy | (k << 28), __double2loint(tw), __double2hiint(tw));
+                            ma[0] = qx;
+                            mb[0] = qy;
+                            mk[0] = k;
+                        } else {
+                            nm = weld_list(W, qx, qy, k, sh, ma, mb, mk);
+                        }
+                        // the rows of all the lanes in one mesh are reserved with one atomic
+                        const int base = reserve_rows(mesh_counters, F, R.m, nm, mask);
                         for (int i = 0; i < nm; ++i) {
                             const long long r = (long long)base + i;
                             if (r >= R.cap) {
@@ -1410,6 +1444,61 @@ cudaError_t launch_ccd_narrow(int grid, cudaStream_t s, const int2* cand, int ca
 }
 
 #endif  // CCC_NARROW_TU
+
+// The rows of the other pairs of the shared sub-tests whose roots passed the filter in
+// k_ccd_narrow (its records in Weld.expand; the narrow kernel wrote the owner's row): one
+// record a thread, the rows of a warp's lanes reserved with one atomic per mesh.
+static constexpr int EXPAND_THREADS = 256;
+template <class T>
+__global__ void __launch_bounds__(EXPAND_THREADS)
+k_ccd_expand(WsHeader* hdr, Weld W, Forest F, long long* __restrict__ rows, T* __restrict__ times, int max_per_tri,
+             int* __restrict__ mesh_counters) {
+    const unsigned FULL = 0xffffffffu;
+    const int M = forest_size(F);
+    const int n = min(*(volatile int*)&hdr->expand_count, W.expand_cap);
+    const int lane = threadIdx.x & 31;
+    const int nwarps = gridDim.x * (EXPAND_THREADS / 32);
+    for (int base = ((blockIdx.x * EXPAND_THREADS + threadIdx.x) >> 5) * 32; base < n; base += nwarps * 32) {
+        const int c = base + lane;
+        int ma[WELD_FANCAP], mb[WELD_FANCAP], mk[WELD_FANCAP];
+        int nm = 0, m = 0, po = 0;
+        long long cap = 0;
+        T tv = T(0);
+        if (c < n) {
+            const int4 rec = W.expand[c];
+            const int qx = rec.x, qy = rec.y & SLOT_MASK, k = (rec.y >> 28) & 15;
+            tv = (T)__hiloint2double(rec.w, rec.z);
+            const OutRegion R = out_region(F, M, qx, max_per_tri);
+            m = R.m;
+            po = R.po;
+            cap = R.cap;
+            const int all = weld_list(W, qx, qy, k, true, ma, mb, mk);
+            for (int i = 0; i < all; ++i)
+                if (!(ma[i] == qx && mb[i] == qy && mk[i] == k)) {
+                    ma[nm] = ma[i];
+                    mb[nm] = mb[i];
+                    mk[nm] = mk[i];
+                    ++nm;
+                }
+        }
+        const unsigned has = __ballot_sync(FULL, nm > 0);
+        if (nm > 0) {
+            const int first = reserve_rows(mesh_counters, F, m, nm, has);
+            for (int i = 0; i < nm; ++i) {
+                const long long r = (long long)first + i;
+                if (r >= cap) {
+                    atomicOr(&hdr->status, ST_OUT_OVERFLOW);
+                    break;
+                }
+                const long long o = (long long)po * max_per_tri + r;
+                rows[o * 3 + 0] = ma[i] - po;
+                rows[o * 3 + 1] = mb[i] - po;
+                rows[o * 3 + 2] = mk[i];
+                times[o] = tv;
+            }
+        }
+    }
+}
 
 // proximity (proximity_static.cu:11-508)
 template <class T>
