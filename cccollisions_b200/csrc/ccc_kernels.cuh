@@ -708,10 +708,10 @@ struct Weld {
     const int4* live;      // the pairs with sub-tests to solve (hdr->live_count of them, from
                            // k_ccd_stage_*): slots i, j and the sub-tests it solves (bits
                            // 0..14) with those that stand for their repeats (bits 15..29)
-    int4* expand;          // the shared sub-tests whose roots passed the filter, for
-                           // k_ccd_expand (hdr->expand_count, at most expand_cap): owner slots
-                           // i, j | type << 28, the root as a double (low, high words); null:
-                           // k_ccd_narrow writes every pair's rows itself
+    int4* expand;          // the roots that passed the filter, for k_ccd_expand
+                           // (hdr->expand_count, at most expand_cap): slots i | shared << 28,
+                           // j | type << 28, the root as a double (low, high words); null:
+                           // k_ccd_narrow writes the rows itself
     int expand_cap;
 };
 
@@ -1305,32 +1305,27 @@ k_ccd_narrow(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, const T
                         }
                     };
                     if constexpr (STAGED) {
-                        // a shared sub-test leaves a record for k_ccd_expand, which writes the
-                        // other pairs' rows (the owner's is written here); with the record
-                        // list full, all of them are written here
-                        const bool sh = (it.x >> 28) & 1;
-                        const unsigned shm = __ballot_sync(mask, sh);
-                        int at = -1;
-                        if (shm && W.expand) {
-                            const int leader = __ffs(shm) - 1;
+                        // each passing root leaves a record for k_ccd_expand, which writes its
+                        // rows (every pair's, for a shared sub-test); the roots that do not
+                        // fit in the record list are written here
+                        unsigned rest = mask;
+                        if (W.expand) {
+                            const int leader = __ffs(mask) - 1;
                             int b0 = 0;
-                            if (lane == leader) b0 = atomicAdd(&hdr->expand_count, __popc(shm));
-                            b0 = __shfl_sync(mask, b0, leader);
-                            if (sh && b0 + __popc(shm & lt) < W.expand_cap) at = b0 + __popc(shm & lt);
+                            if (lane == leader) b0 = atomicAdd(&hdr->expand_count, __popc(mask));
+                            b0 = __shfl_sync(mask, b0, leader) + __popc(mask & lt);
+                            const bool fits = b0 < W.expand_cap;
+                            rest = __ballot_sync(mask, !fits);
+                            if (fits) {
+                                const double tw = (double)tv;
+                                W.expand[b0] = make_int4(it.x, it.y, __double2loint(tw), __double2hiint(tw));
+                                return;
+                            }
                         }
                         int ma[WELD_FANCAP], mb[WELD_FANCAP], mk[WELD_FANCAP];
-                        int nm = 1;
-                        if (at >= 0) {
-                            const double tw = (double)tv;
-                            W.expand[at] = make_int4(qx, qy | (k << 28), __double2loint(tw), __double2hiint(tw));
-                            ma[0] = qx;
-                            mb[0] = qy;
-                            mk[0] = k;
-                        } else {
-                            nm = weld_list(W, qx, qy, k, sh, ma, mb, mk);
-                        }
+                        const int nm = weld_list(W, qx, qy, k, (it.x >> 28) & 1, ma, mb, mk);
                         // the rows of all the lanes in one mesh are reserved with one atomic
-                        const int base = reserve_rows(mesh_counters, F, R.m, nm, mask);
+                        const int base = reserve_rows(mesh_counters, F, R.m, nm, rest);
                         for (int i = 0; i < nm; ++i) {
                             const long long r = (long long)base + i;
                             if (r >= R.cap) {
@@ -1445,9 +1440,9 @@ cudaError_t launch_ccd_narrow(int grid, cudaStream_t s, const int2* cand, int ca
 
 #endif  // CCC_NARROW_TU
 
-// The rows of the other pairs of the shared sub-tests whose roots passed the filter in
-// k_ccd_narrow (its records in Weld.expand; the narrow kernel wrote the owner's row): one
-// record a thread, the rows of a warp's lanes reserved with one atomic per mesh.
+// The rows of the roots that passed the filter in k_ccd_narrow (its records in Weld.expand),
+// every pair's for a shared sub-test: one record a thread, the rows of a warp's lanes
+// reserved with one atomic per mesh.
 static constexpr int EXPAND_THREADS = 256;
 template <class T>
 __global__ void __launch_bounds__(EXPAND_THREADS)
@@ -1466,20 +1461,13 @@ k_ccd_expand(WsHeader* hdr, Weld W, Forest F, long long* __restrict__ rows, T* _
         T tv = T(0);
         if (c < n) {
             const int4 rec = W.expand[c];
-            const int qx = rec.x, qy = rec.y & SLOT_MASK, k = (rec.y >> 28) & 15;
+            const int qx = rec.x & SLOT_MASK, qy = rec.y & SLOT_MASK, k = (rec.y >> 28) & 15;
             tv = (T)__hiloint2double(rec.w, rec.z);
             const OutRegion R = out_region(F, M, qx, max_per_tri);
             m = R.m;
             po = R.po;
             cap = R.cap;
-            const int all = weld_list(W, qx, qy, k, true, ma, mb, mk);
-            for (int i = 0; i < all; ++i)
-                if (!(ma[i] == qx && mb[i] == qy && mk[i] == k)) {
-                    ma[nm] = ma[i];
-                    mb[nm] = mb[i];
-                    mk[nm] = mk[i];
-                    ++nm;
-                }
+            nm = weld_list(W, qx, qy, k, (rec.x >> 28) & 1, ma, mb, mk);
         }
         const unsigned has = __ballot_sync(FULL, nm > 0);
         if (nm > 0) {
