@@ -325,15 +325,20 @@ __device__ __forceinline__ uint32_t ccd_pair_subbox_mask(const T* __restrict__ x
             }
         }
         if constexpr (LEAF) leaf = leaf && la <= hb && ha >= lb;
-        // finite displacement, and start positions below half the largest finite value so that
-        // every difference of two of them is finite too
-        const T half_max = sizeof(T) == 4 ? T(1.7e38) : T(8.9e307);
-        rigid = rigid && fabs(dv[0]) <= half_max;
+        // the same displacement at all six vertices, finite, and start positions below half the
+        // largest finite value so that every difference of two of them is finite too (the range
+        // tests only where the displacements agree, which deforming pairs seldom do)
+        bool same = true;
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-            rigid = rigid && fabs(__ldg(a0 + 3 * c + ax)) <= half_max && fabs(__ldg(b0 + 3 * c + ax)) <= half_max;
+        for (int c = 1; c < 6; ++c) same = same && dv[c] == dv[0];
+        rigid = rigid && same;
+        if (rigid) {
+            const T half_max = sizeof(T) == 4 ? T(1.7e38) : T(8.9e307);
+            rigid = fabs(dv[0]) <= half_max;
 #pragma unroll
-        for (int c = 1; c < 6; ++c) rigid = rigid && dv[c] == dv[0];
+            for (int c = 0; c < 3; ++c)
+                rigid = rigid && fabs(__ldg(a0 + 3 * c + ax)) <= half_max && fabs(__ldg(b0 + 3 * c + ax)) <= half_max;
+        }
         // edges 01, 02, 12 and the face
         const T ealo[3] = {fmn(alo[0], alo[1]), fmn(alo[0], alo[2]), fmn(alo[1], alo[2])};
         const T eahi[3] = {fmx(ahi[0], ahi[1]), fmx(ahi[0], ahi[2]), fmx(ahi[1], ahi[2])};
