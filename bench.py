@@ -22,7 +22,8 @@ plain per-mesh path, with exact pair sets and p50 / p99 latency.
 * ``served`` — a Poisson stream of impulse-loop requests (rate 2,000/s, meshes of
   log-uniform 2e3..2e5 triangles as in the impulse workload) under a 40 GB engine budget:
   throughput (request triangles over the makespan) and p50 / p99 latency (arrival to result
-  on the host).
+  on the host).  ``served_separated``: the same stream of folds whose layers start apart
+  (``workloads.SEPARATED_FOLD``), where the loop runs until no pair collides.
 * ``e2e`` — the batched step through the public engine API from pinned host buffers
   (``engine.StepPipeline``): every step's H2D of both soups of every mesh, the graph replay,
   the rows packed on the device and one D2H copy of every row and time, with each step's
@@ -494,12 +495,14 @@ def plain_loop(r, dev, max_iter=50):
     return max_iter
 
 
-def run_served(args, dev):
+def run_served(args, dev, fold=None):
+    """The served stream through the request server, and a sample of it through the engine
+    and the plain per-request loop; fold: the fold's shape (workloads.impulse_fold_mesh)."""
     import torch
 
     from cccollisions_b200 import workloads as W
     from cccollisions_b200.serve import Request, Server, requests_from_stream
-    reqs = requests_from_stream(W.served_stream(num_requests=args.served_requests, rate=2000.0))
+    reqs = requests_from_stream(W.served_stream(num_requests=args.served_requests, rate=2000.0), fold=fold)
     srv = Server(budget_bytes=args.served_budget_gb << 30, device=dev)
     for r in reqs:
         srv._pin(r)
@@ -595,6 +598,10 @@ def main():
                 res["served"] = run_served(args, dev)
                 ss = res["served"]["same_set"]
                 res["served_over_plain"] = ss["engine"]["value"] / ss["plain"]["value"]
+                # the same stream of folds whose layers start apart, where the loop runs until
+                # no pair collides
+                from cccollisions_b200 import workloads as W
+                res["served_separated"] = {"fold": W.SEPARATED_FOLD, **run_served(args, dev, W.SEPARATED_FOLD)}
             # the headline ratios last, so that any tail of the line holds them
             res["batched_over_plain"] = res["plain"]["ms_per_step"] / res["ms_per_step"]
             rg = res["reference_gpu"]

@@ -218,11 +218,12 @@ class Server:
                 "contacts_all_iterations": int(sum(sum(r.contacts) for r in requests))}
 
 
-def requests_from_stream(stream, dtype=np.float64) -> list[Request]:
-    """Requests of workloads.served_stream entries (arrival, seed, nx, ny)."""
+def requests_from_stream(stream, dtype=np.float64, fold=None) -> list[Request]:
+    """Requests of workloads.served_stream entries (arrival, seed, nx, ny); fold: keyword
+    arguments of workloads.impulse_fold_mesh (such as workloads.SEPARATED_FOLD)."""
     from . import workloads as W
     out = []
     for i, (t, seed, nx, ny) in enumerate(stream):
-        v0, v1, vel, faces, masses = W.impulse_fold_mesh(seed, nx, ny, dtype=dtype)
+        v0, v1, vel, faces, masses = W.impulse_fold_mesh(seed, nx, ny, dtype=dtype, **(fold or {}))
         out.append(Request(v0, v1, vel, faces, masses, arrival=t, rid=i))
     return out

@@ -190,21 +190,30 @@ def batched(num_meshes: int = 64, lo: float = 1e3, hi: float = 1e5, seed0: int =
     return out
 
 
-def impulse_fold_mesh(seed: int = 0, nx: int = 256, ny: int = 256, dtype=np.float64):
-    """Indexed form of the impulse workload (jittered cloth, x > 0.5 half folded 0.005 above
-    the rest, moving 0.01 down with N(0, 0.002^2) noise) on an nx-by-ny grid scaled to the
-    grid's aspect: verts0 (V, 3), verts1 (V, 3), vel (V, 3) = verts1 - verts0, faces (F, 3)
-    int32, per-corner unit masses (F, 3)."""
+# A fold whose layers start apart (heights N(0, 0.002^2), the upper half 0.02 above) and
+# whose upper half moves 0.03 down through the lower one: every triangle of the fold collides
+# in the first check, and the impulse loop separates them in a few iterations.
+SEPARATED_FOLD = dict(noise=0.002, gap=0.02, drop=0.0, drop_noise=0.002, fold_drop=0.03)
+
+
+def impulse_fold_mesh(seed: int = 0, nx: int = 256, ny: int = 256, dtype=np.float64, noise: float = 0.01,
+                      gap: float = 0.005, drop: float = 0.01, drop_noise: float = 0.002, fold_drop: float = 0.0):
+    """Indexed form of the impulse workload (jittered cloth with heights N(0, noise^2), the
+    x > 0.5 half folded gap above the rest, everything moving drop down (the folded half
+    fold_drop more) with N(0, drop_noise^2) noise; by default a fold whose layers already
+    interpenetrate) on an nx-by-ny grid scaled to the grid's aspect: verts0 (V, 3), verts1
+    (V, 3), vel (V, 3) = verts1 - verts0, faces (F, 3) int32, per-corner unit masses (F, 3)."""
     g = rng(seed)
     sy = (ny - 1) / (nx - 1)
     verts, faces = grid(nx, ny, 0.0, 1.0, 0.0, sy)
-    verts[:, 2] = g.normal(0.0, 0.01, verts.shape[0])
+    verts[:, 2] = g.normal(0.0, noise, verts.shape[0])
     m = verts[:, 0] > 0.5
     verts[m, 0] = 1.0 - verts[m, 0]
-    verts[m, 2] += 0.005
+    verts[m, 2] += gap
     v1 = verts.copy()
-    v1[:, 2] -= 0.01
-    v1 += g.normal(0.0, 0.002, verts.shape)
+    v1[:, 2] -= drop
+    v1[m, 2] -= fold_drop
+    v1 += g.normal(0.0, drop_noise, verts.shape)
     masses = np.ones((faces.shape[0], 3), dtype=dtype)
     return (verts.astype(dtype), v1.astype(dtype), (v1 - verts).astype(dtype), faces.astype(np.int32), masses)
 

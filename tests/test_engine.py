@@ -216,6 +216,27 @@ def test_impulse_loop_matches_oracle_bit_for_bit(cuda, oracle):
         eng.close()
 
 
+def test_impulse_loop_separates_folds_like_the_oracle(cuda, oracle):
+    """Folds whose layers start apart and cross during the step: the loop ends because no pair
+    collides any more, after the oracle's number of iterations and with its positions and
+    velocities."""
+    from cccollisions_b200 import _native as N
+    from cccollisions_b200 import workloads as W
+    meshes = [W.impulse_fold_mesh(300 + i, 14 + 3 * i, 12 + 2 * i, **W.SEPARATED_FOLD) for i in range(3)]
+    with N.math_library(N.LIB_PORTABLE):
+        eng, sids = _loop_engine(meshes)
+        st = _run_loop(eng, sids)
+        assert st["status"] == 0
+        for i, (sid, m) in enumerate(zip(sids, meshes)):
+            ev1, evel, it, conv, per = oracle.impulse_loop(*m, max_iter=50)
+            assert conv and 1 <= it < 50
+            assert int(st["iterations"][i]) == it and bool(st["flags"][i] & 2)
+            view = eng.view(sid)
+            assert np.array_equal(view["verts1"].cpu().numpy(), ev1)
+            assert np.array_equal(view["vel"].cpu().numpy(), evel)
+        eng.close()
+
+
 def test_impulse_loop_same_alone_and_in_mix(cuda):
     meshes = _loop_meshes(6, seed=4)
     eng, sids = _loop_engine(meshes)

@@ -34,3 +34,13 @@ def test_collision_free_input_converges_at_once(oracle):
     ev1, evel, it, conv, per = oracle.impulse_loop(v, v1, v1 - v, f.astype(np.int32), m)
     assert it == 0 and conv and per.tolist() == [0]
     assert np.array_equal(ev1, v1)
+
+
+def test_separated_fold_converges(oracle):
+    """The fold whose layers start apart (workloads.SEPARATED_FOLD): every triangle collides in
+    the first check, and the loop separates the layers within a few iterations."""
+    from cccollisions_b200 import workloads as W
+    v0, v1, vel, faces, masses = W.impulse_fold_mesh(7, 24, 20, **W.SEPARATED_FOLD)
+    ev1, evel, it, conv, per = oracle.impulse_loop(v0, v1, vel, faces, masses, max_iter=50)
+    assert conv and 1 <= it <= 5
+    assert per[0] > faces.shape[0] and per[it] == 0
