@@ -1023,7 +1023,7 @@ k_ccd_stage_mask(const int2* __restrict__ cand, int cand_cap, WsHeader* hdr, con
     if (lane == 0 && masked) atomicAdd(&hdr->subtests, masked);
 }
 
-static __global__ void __launch_bounds__(STAGE_THREADS)
+static __global__ void __launch_bounds__(STAGE_THREADS, 8)
 k_ccd_stage_pending(int cand_cap, WsHeader* hdr, Weld W, const int4* __restrict__ pending, int4* __restrict__ live) {
     // per warp: 32 pending pairs, their classes, pending sub-tests, the prefix of their
     // counts and the sub-tests they solve; the lanes take the sub-tests 32 at a time
